@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the 3D electrostatic PIC step on B200.
+
+Workload: 256x256x512 cells over 8 cm x 8 cm x 1 m, 5e7 protons at 1 MeV
+(semi-Gaussian, 4 mm radius, 20% envelope mismatch, 5 mrad, 10 mA), FODO of
+hard-edge quads (10 cm, +-15 T/m, 50 cm period), grounded pipe r = 3.5 cm,
+periodic z; seeded synthetic beam. One step = fused gather+push+boundaries,
+fixed-point deposition, multigrid solve to a 1e-6 relative residual (warm
+started from the previous phi).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0). Under torchrun each rank runs an independent
+replica (the path does not shard; "replicas only") and the timing is the
+max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PIC steps/s, 256²×512 grid/5e7 ptcl: plain vs learned+mixed @1e-6 residual"
+WORKLOAD = "B"
+# V-cycles per warm-started solve of the FP64 form at 1e-6 relative
+# residual on this workload (the oracle runs the identical algorithm); used
+# to extrapolate the CPU reference's per-V-cycle sample to one step.
+DEFAULT_REF_VCYCLES = 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--forms", default="plain,mixed")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-vcycles", type=float, default=None)
+    ap.add_argument("--ref-sample", type=int, default=1_000_000)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        os.unlink(self.path)
+        sm = sorted(float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit())
+        smax = max((float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()),
+                   default=None)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, n in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def run_form(name, cfg, beam, steps, warmup, dev, prof):
+    import torch
+
+    from warp_b200 import _lib
+    from warp_b200.pic import ESPIC
+    precision = {"plain": "fp64", "mixed": "mixed"}[name]
+    run = ESPIC(cfg, precision=precision, tolkind="relres", mgtol=1e-6, device=dev, particles=beam)
+    run.generate()
+    s = run.solver
+    run.step(warmup)
+    stream = torch.cuda.current_stream()
+    h = s._h
+    if prof:
+        mask = (1 << _lib.PROF_SOR0) | (1 << _lib.PROF_ADVANCE) | (1 << _lib.PROF_DEPOSIT) | (1 << _lib.PROF_RESID0)
+        _lib.check(_lib.lib.wg_prof_enable(h, mask))
+    n0 = _lib.ctypes.c_int64()
+    _lib.check(_lib.lib.wg_launch_count(h, _lib.ctypes.byref(n0)))
+    vc = 0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        run.step()
+        vc += s.mgiters
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    n1 = _lib.ctypes.c_int64()
+    _lib.check(_lib.lib.wg_launch_count(h, _lib.ctypes.byref(n1)))
+    out = {"ms_per_step": ms / steps, "vcycles_per_solve": vc / steps, "launches": n1.value - n0.value,
+           "live": run.pgroup.nlive(), "relres": s.relres}
+    if prof:
+        kinds = {"sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE, "deposit": _lib.PROF_DEPOSIT,
+                 "resid0": _lib.PROF_RESID0}
+        out["kernels"] = {}
+        for k, v in kinds.items():
+            t, n, u = _lib.ctypes.c_double(), _lib.ctypes.c_int64(), _lib.ctypes.c_double()
+            _lib.check(_lib.lib.wg_prof_read(h, v, _lib.ctypes.byref(t), _lib.ctypes.byref(n), _lib.ctypes.byref(u)))
+            out["kernels"][k] = {"ms": t.value, "launches": n.value, "units": u.value}
+        _lib.check(_lib.lib.wg_prof_enable(h, 0))
+    return run, out
+
+
+def e2e_steps(run, steps):
+    """The drop-in path with host-owned particles (WARP's pgroup lives in
+    host memory): every step copies the particle arrays host->device from
+    pinned memory, advances, deposits, solves and copies them back."""
+    import torch
+    pg = run.pgroup
+    names = ("x", "y", "z", "ux", "uy", "uz", "gaminv")
+    host = {k: torch.empty(pg.np, dtype=torch.float64, pin_memory=True) for k in names}
+    for k in names:
+        host[k].copy_(getattr(pg, k))
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        for k in names:
+            getattr(pg, k).copy_(host[k], non_blocking=True)
+        run.step()
+        for k in names:
+            host[k].copy_(getattr(pg, k), non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    nbytes = 8 * pg.np * len(names)
+    return e0.elapsed_time(e1) / steps, nbytes, nbytes
+
+
+def cpu_reference_step(cfg, sample, vcycles):
+    """Oracle timing of one step on a bounded sample: deposit + gather + push
+    of `sample` particles (scaled to the full count) and one V-cycle plus one
+    residual evaluation on the full grid (scaled by `vcycles`)."""
+    import numpy as np
+
+    from oracle import oracle
+    from warp_b200 import pic
+    from warp_b200.lattice import fodo
+    from warp_b200.particles import beam_weight, semigaussian
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    dx = (cfg["xmmax"] - cfg["xmmin"]) / nx
+    dy = (cfg["ymmax"] - cfg["ymmin"]) / ny
+    dz = (cfg["zmmax"] - cfg["zmmin"]) / nz
+    mins = (cfg["xmmin"], cfg["ymmin"], cfg["zmmin"])
+    p = semigaussian(sample, seed=cfg["seed"], radius=cfg["radius"], mismatch=cfg["mismatch"],
+                     angle_rms=cfg["angle_rms"], zmin=cfg["zmmin"], zmax=cfg["zmmax"], ekin_ev=cfg["ekin_ev"])
+    w = beam_weight(cfg["current"], cfg["zmmax"] - cfg["zmmin"], cfg["npart"])
+    lat = fodo(cfg["quad_gradient"], cfg["quad_length"], cfg["period"])
+    tables = lat.tables(cfg["zmmin"], dz, nz + 1)
+    oc = oracle.Conductors(nx, ny, nz, dx, dy, dz, *mins)
+    oc.add_shape("ZCylinderOut", cfg["pipe_radius"], 100.0, 0.0, 0., 0., 0.5 * (cfg["zmmin"] + cfg["zmmax"]), 1)
+    oc.finalize()
+    phi = np.zeros((nx + 3, ny + 3, nz + 3), order="F")
+    rho = np.zeros((nx + 1, ny + 1, nz + 1), order="F")
+    from warp_b200.constants import echarge, proton_mass
+    dt = pic.timestep(cfg)
+    t0 = time.perf_counter()
+    ex, ey, ez = oracle.sete(phi, p["x"], p["y"], p["z"], dx, dy, dz, *mins)
+    oracle.push_fullv(p, ex, ey, ez, echarge, proton_mass, dt, tables, cfg["zmmin"], dz, cfg["zmmin"],
+                      cfg["zmmax"], cfg["pipe_radius"])
+    oracle.setrho(rho, p["x"], p["y"], p["z"], echarge, w * cfg["npart"] / sample, dx, dy, dz, *mins,
+                  gaminv=p["gaminv"])
+    oracle.rhobc(rho, (0, 0, 0, 0, 2, 2))
+    t_part = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.mgsolve(phi, rho, dx, dy, dz, (0, 0, 0, 0, 2, 2), conductors=oc, mgmaxiters=1, mgtol=0.0)
+    t_v = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.relresidual(phi, rho, dx, dy, dz, (0, 0, 0, 0, 2, 2), oc)
+    t_r = time.perf_counter() - t0
+    step = t_part * cfg["npart"] / sample + t_v * vcycles + t_r * (vcycles + 1)
+    desc = ("oracle (C++ FP64 restatement, 1 thread): gather+push+deposit of %d of %d particles scaled x%g, one "
+            "V-cycle and one residual on the full %dx%dx%d grid scaled to %g V-cycles per solve"
+            % (sample, cfg["npart"], cfg["npart"] / sample, nx, ny, nz, vcycles))
+    return step, desc, {"t_particles_sample": t_part, "t_vcycle": t_v, "t_residual": t_r}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    from warp_b200 import pic
+    cfg = pic.workload(args.workload)
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        vcyc = args.ref_vcycles if args.ref_vcycles is not None else DEFAULT_REF_VCYCLES
+        times = []
+        desc = ""
+        for i in range(args.warmup + args.steps):
+            st, desc, _ = cpu_reference_step(cfg, args.ref_sample, vcyc)
+            if i >= args.warmup:
+                times.append(st)
+        sec = sum(times) / len(times)
+        v = 1.0 / sec
+        line = {"metric": METRIC, "value": v, "unit": "steps/s", "impl": "reference", "n_gpus": 0,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": {"workload": "256x256x512 cells, 5e7 protons, pipe + FODO, 1e-6 relres",
+                           "flush": "inputs larger than L2"},
+                "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": "port", "sample": desc},
+                "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import torch.distributed as tdist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    dev = "cuda:%d" % local
+    if world > 1:
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
+    from warp_b200.particles import semigaussian
+    beam = semigaussian(cfg["npart"], seed=cfg["seed"] + rank, radius=cfg["radius"], mismatch=cfg["mismatch"],
+                        angle_rms=cfg["angle_rms"], zmin=cfg["zmmin"], zmax=cfg["zmmax"], ekin_ev=cfg["ekin_ev"])
+    forms = [f for f in args.forms.split(",") if f]
+    headline = forms[-1]
+    results = {}
+    clocks = None
+    head_run = None
+    for f in forms:
+        prof = f == headline
+        if world > 1:
+            tdist.barrier()
+        if prof:
+            clocks = Clocks(local)
+            clocks.start()
+        run, res = run_form(f, cfg, beam, args.steps, args.warmup, dev, prof)
+        if prof:
+            clk = clocks.stop()
+            head_run = run
+        else:
+            del run
+            torch.cuda.empty_cache()
+        results[f] = res
+    ms_head = results[headline]["ms_per_step"]
+    if world > 1:
+        t = torch.tensor([ms_head], device=dev, dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms_head = float(t.item())
+    value = world * 1000.0 / ms_head
+    e2e_ms, h2d, d2h = e2e_steps(head_run, args.e2e_steps)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    peak, peak_kind = measured_peaks()
+    kern = results[headline]["kernels"]
+    sor = kern["sor0"]
+    bytes_per_node = 6.0 if headline == "mixed" else 12.0  # one colour of a red+black sweep
+    achieved = None
+    if sor["launches"]:
+        per_launch_bytes = bytes_per_node * sor["units"] / sor["launches"]
+        achieved = per_launch_bytes / (sor["ms"] / sor["launches"] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_sor_bulk (finest level, one colour)", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "peak_kind": peak_kind, "traffic": None,
+                "bytes_per_node_per_launch": bytes_per_node}
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if headline == "plain" else "f32+f64",
+            "data": "synthetic (seeded semi-Gaussian beam)",
+            "config": {"workload": "256x256x512 cells, 5e7 protons, pipe + FODO, 1e-6 relres",
+                       "form": headline, "parallelism": "replicas" if world > 1 else "single",
+                       "flush": "inputs larger than L2 (phi 271 MB, particles 2.8 GB)"},
+            "forms": results, "gpu_launches": results[headline]["launches"],
+            "e2e": {"value": 1000.0 / e2e_ms * world, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": roofline, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        vc = results.get("plain", results[headline])["vcycles_per_solve"]
+        st, desc, parts = cpu_reference_step(cfg, args.ref_sample, vc)
+        line["cpu_baseline"] = {"value": 1.0 / st, "unit": "steps/s", "cores": 1, "kind": "port", "sample": desc,
+                                "parts_s": parts}
+    if world > 1:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

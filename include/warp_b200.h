@@ -1,0 +1,179 @@
+/*
+ * warp_b200 C ABI: B200-native 3D electrostatic PIC step of WARP.
+ *
+ * Plain C types only (no torch, no C++). Every entry point returns 0 on
+ * success or a negative WG_E* code; wg_last_error() gives the message. Grid
+ * arrays use the reference's Fortran layout (x fastest):
+ *   phi(-1:nx+1,-1:ny+1,-1:nz+1)   one guard cell (nxguardphi = 1)
+ *   rho(0:nx,0:ny,0:nz)            no guard cell  (nxguardrho = 0)
+ * Particle pointers are DEVICE pointers (SoA, float64); the Python layer
+ * (warp_b200.fieldsolver / warp_b200.multigrid) moves host arrays in and out.
+ * Work is queued on the context's stream (wg_set_stream); calls that return
+ * host results synchronize that stream.
+ *
+ * Each entry point names the reference routine it replaces (paths relative
+ * to the radiasoft/warp tree).
+ */
+#ifndef WARP_B200_H
+#define WARP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WG_OK 0
+#define WG_EINVAL (-1)       /* bad argument (shape, pointer, option) */
+#define WG_ECUDA (-2)        /* CUDA runtime error */
+#define WG_ESTATE (-3)       /* call out of order (e.g. solve before rho) */
+#define WG_EOVERFLOW (-4)    /* fixed-point charge accumulator overflow */
+#define WG_ENODEV (-5)       /* no CUDA device */
+#define WG_ENOMEM (-6)       /* device allocation failed */
+#define WG_ETOOLARGE (-7)    /* size beyond a fixed limit of the entry point */
+
+typedef struct wg_ctx wg_ctx;
+
+/* Mesh description (w3d.nx.., w3d.xmmin.., f3d.bounds; f3d.v:231-233). */
+typedef struct {
+  int nx, ny, nz;
+  double xmmin, xmmax, ymmin, ymmax, zmmin, zmmax;
+  int bounds[6]; /* 0 Dirichlet, 1 Neumann, 2 periodic: xlo,xhi,ylo,yhi,zlo,zhi */
+} wg_grid;
+
+/* Solver options (MultiGrid3D attributes, f3d.v:215-231). */
+typedef struct {
+  double mgparam;  /* SOR over-relaxation, default 1.2 */
+  double mgtol;    /* tolerance; meaning set by tolkind */
+  int mgmaxiters;  /* default 100 */
+  int mgmaxlevels; /* default 101 */
+  int downpasses;  /* default 1 */
+  int uppasses;    /* default 1 */
+  int lcndbndy;    /* subgrid conductor boundaries, default 1 */
+  int precision;   /* 0: FP64 V-cycles (mgform=1 form of the reference)
+                      1: FP32 V-cycles inside FP64 defect correction */
+  int tolkind;     /* 0: mgerror = max|dphi| in volts (reference criterion)
+                      1: relative residual max|rhs-A phi|/max|rhs| */
+} wg_solve_opts;
+
+typedef struct {
+  int mgiters;      /* V-cycles done */
+  int converged;    /* 1 if the tolerance was met before mgmaxiters */
+  double mgerror;   /* last max|dphi| (volts) */
+  double relres;    /* last relative residual (when computed, else -1) */
+} wg_solve_stats;
+
+/* One particle species, device SoA arrays of length np (top.pgroup). A lost
+ * particle has gaminv == 0 (stckxy3d convention, w3d.F:11520-11535). */
+typedef struct {
+  double *x, *y, *z, *ux, *uy, *uz, *gaminv;
+  int64_t np;
+  double q, m, w; /* charge, mass, macroparticle weight (sq, sm, sw) */
+} wg_particles;
+
+/* Parameters of one fullv particle advance (padvnc3d, w3d.F:1862-1987). */
+typedef struct {
+  double dt;
+  double prwall, prwallx, prwally; /* round absorbing aperture (top.prwall) */
+  int use_lattice;                 /* apply the hard-edge quad tables */
+} wg_push_params;
+
+/* ---- context ----------------------------------------------------------- */
+
+/* MultiGrid3D.__init__ + allocatedataarrays (scripts/multigrid.py:77,
+ * scripts/fieldsolver.py:1622-1695): allocates every MG level on the current
+ * CUDA device. */
+int wg_create(const wg_grid* grid, wg_ctx** out);
+int wg_destroy(wg_ctx* ctx);
+/* Work is queued on this cudaStream_t (NULL = the legacy default stream). */
+int wg_set_stream(wg_ctx* ctx, void* cuda_stream);
+const char* wg_last_error(void);
+/* getmglevels (f3d_mgrid.F:3654-3845): level sizes and cell sizes. */
+int wg_level_info(wg_ctx* ctx, int* nlevels, int* dims, double* deltas, int maxlevels);
+/* Device pointers of the solver's phi and rho (solver.phi / solver.rho,
+ * Fortran layout above). */
+int wg_arrays(wg_ctx* ctx, double** phi, double** rho);
+
+/* ---- conductors (installconductor, scripts/multigrid.py:743-783) ---------- */
+
+/* Adds a shape on every MG level via grid-line intercepts
+ * (generateconductors.py:2750 getdatanew + f3d_conductors.F:12
+ * conductordelfromintercepts). kind: 0 ZCylinderOut (generateconductors.py:3494),
+ * 1 ZCylinder (:3305), 2 Sphere (:4009). dfill defaults to 2. */
+int wg_conductors_add_shape(wg_ctx* ctx, int kind, double radius, double length, double voltage,
+                            double xcent, double ycent, double zcent, int condid, double dfill);
+/* Adds raw ConductorType points (f3d.v:105-164). kind 0: interior
+ * (indx[3n], volt[n], ilevel[n]); kind 1: subgrid (indx[3n], dels[6n] in the
+ * order mx,px,my,py,mz,pz, volt[6n], ilevel[n]). Host pointers. */
+int wg_conductors_add_points(wg_ctx* ctx, int kind, int64_t n, const int32_t* indx, const double* dels,
+                             const double* volt, const int32_t* ilevel);
+/* checkconductors (f3d_mgrid.F:3964-4050): clip, dedupe, sort by level, and
+ * upload to the device. */
+int wg_conductors_finalize(wg_ctx* ctx);
+int wg_conductors_clear(wg_ctx* ctx);
+/* out[0] interior, out[1] even subgrid, out[2] odd subgrid point counts. */
+int wg_conductors_counts(wg_ctx* ctx, int64_t* out);
+/* Host copy of the finalized lists; which: 0 interior, 1 even, 2 odd. */
+int wg_conductors_export(wg_ctx* ctx, int which, int32_t* indx, double* dels, double* volt, int32_t* ilevel);
+
+/* ---- field solve ---------------------------------------------------------- */
+
+/* multigrid3dsolve (f3d_mgrid.F:83-500), called through
+ * MultiGrid3D.dosolve (scripts/multigrid.py:846-917). phi is the warm start
+ * and the result; rho is left unchanged. */
+int wg_solve(wg_ctx* ctx, const wg_solve_opts* opts, wg_solve_stats* stats);
+/* Relative residual of the current phi (same definition as tolkind 1). */
+int wg_relresidual(wg_ctx* ctx, double mgparam, double* out);
+
+/* ---- particles -------------------------------------------------------------- */
+
+/* setrho3d -> setrho3ddirect1 (w3d.F:7199, 7757-7960), via
+ * MultiGrid3D.setsourcep (multigrid.py:492-511). Charge is accumulated in a
+ * 64-bit fixed-point grid, so rho is bit-identical from run to run.
+ * zero_first clears rho first (loadrho3d zeroes rho before depositing). */
+int wg_deposit(wg_ctx* ctx, const wg_particles* p, int zero_first);
+/* applyrhoboundaryconditions3d (w3d.F:2660-2750) on rho. */
+int wg_finalize_rho(wg_ctx* ctx);
+/* sete3d -> sete_from_phi_linear3d (w3d.F:3656, 3963-4108), via
+ * MultiGrid3D.fetchfieldfrompositions (multigrid.py:521-558). E is ADDED to
+ * ex, ey, ez (device arrays). */
+int wg_fetch_e(wg_ctx* ctx, const double* x, const double* y, const double* z, double* ex, double* ey,
+               double* ez, int64_t np);
+/* Hard-edge quadrupole tables per lattice cell, as set by setlattzt
+ * (top_lattice.F:1852-2030) and read by applyquad (top_lattice.F:2985-3120).
+ * Host arrays of length nzl+1. */
+int wg_set_lattice(wg_ctx* ctx, const double* czs, const double* cze, const double* cdb, int nzl,
+                   double zlmin, double dzl);
+/* One fused fullv step of padvnc3d (w3d.F:1862-1987) followed by
+ * particleboundaries3d (w3d.F:11292): gather E (sete_from_phi_linear3d),
+ * quad B (applyquad), epush3d/bpush3d(ibpush=1)/epush3d/xpush3d
+ * (w3d.F:2752,2834,3070), periz (top.F:4015) and the round-pipe absorber
+ * (stckxy3d, w3d.F:11473). */
+int wg_advance(wg_ctx* ctx, const wg_particles* p, const wg_push_params* prm);
+/* getzmmnt global moments (top.F:521-1444): out[0] live count, 1 xbar,
+ * 2 ybar, 3 xrms, 4 yrms, 5 epsx, 6 epsy (x' = ux/uz), 7 reserved. FP64,
+ * deterministic order. */
+int wg_moments(wg_ctx* ctx, const wg_particles* p, double* out);
+
+/* ---- instrumentation (no reference counterpart: replaces the wall-clock
+ * sub-timers lf3dtimesubs / lw3dtimesubs, f3d.v:1308, w3d.v:1396) -------- */
+
+#define WG_PROF_SOR0 0     /* SOR half pass on the finest level (units: nodes) */
+#define WG_PROF_DEPOSIT 1  /* charge deposition (units: particles) */
+#define WG_PROF_ADVANCE 2  /* fused gather + push (units: particles) */
+#define WG_PROF_RESID0 3   /* residual on the finest level (units: nodes) */
+
+/* Starts CUDA-event timing of the kernel kinds in `mask` (bits 1<<WG_PROF_*),
+ * clearing earlier records; mask 0 stops it. */
+int wg_prof_enable(wg_ctx* ctx, int mask);
+/* Sums the device time (ms), launch count and algorithmic units of one
+ * kind recorded since wg_prof_enable. Synchronizes the stream. */
+int wg_prof_read(wg_ctx* ctx, int kind, double* total_ms, int64_t* launches, double* units);
+/* Number of kernels this context has launched since it was created. */
+int wg_launch_count(wg_ctx* ctx, int64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARP_B200_H */

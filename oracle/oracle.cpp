@@ -1186,11 +1186,19 @@ void or_quad_table(int nquad, const double* zs, const double* ze, const double* 
     double offset = std::floor((zz - zlatstrt) / zlatperi) * zlatperi + zlatstrt;
     double zloc = zz - offset;
     int best = 0;
-    for (int k = 0; k < nquad; ++k) {
-      double left = (k == 0) ? 0.5 * (zs[0] + ze[nquad - 1] - zlatperi) : 0.5 * (zs[k] + ze[k - 1]);
-      double right = (k == nquad - 1) ? 0.5 * (ze[k] + zs[0] + zlatperi) : 0.5 * (ze[k] + zs[k + 1]);
-      if (zloc >= left && zloc < right) { best = k; break; }
-      if (k == 0 && zloc >= left + zlatperi) { best = 0; offset += zlatperi; break; }
+    double left0 = 0.5 * (zs[0] + ze[nquad - 1] - zlatperi);
+    if (zloc < left0) {
+      best = nquad - 1;
+      offset -= zlatperi;
+    } else if (zloc >= left0 + zlatperi) {
+      best = 0;
+      offset += zlatperi;
+    } else {
+      for (int k = 0; k < nquad; ++k) {
+        double left = (k == 0) ? left0 : 0.5 * (zs[k] + ze[k - 1]);
+        double right = (k == nquad - 1) ? 0.5 * (ze[k] + zs[0] + zlatperi) : 0.5 * (ze[k] + zs[k + 1]);
+        if (zloc >= left && zloc < right) { best = k; break; }
+      }
     }
     czs[iz] = zs[best] + offset;
     cze[iz] = ze[best] + offset;

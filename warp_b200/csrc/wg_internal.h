@@ -1,0 +1,135 @@
+// Internal declarations shared by the warp_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/warp_b200.h"
+
+namespace wg {
+
+void set_error(const std::string& msg);
+
+#define WG_TRY_CUDA(expr)                                                   \
+  do {                                                                      \
+    cudaError_t e_ = (expr);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      ::wg::set_error(std::string(#expr) + ": " + cudaGetErrorString(e_));  \
+      return WG_ECUDA;                                                      \
+    }                                                                       \
+  } while (0)
+
+#define WG_TRY(expr)            \
+  do {                          \
+    int r_ = (expr);            \
+    if (r_ != WG_OK) return r_; \
+  } while (0)
+
+// Host-side conductor lists (ConductorType, f3d.v:105-164), all levels.
+struct HostConductors {
+  std::vector<int32_t> int_indx;  // 3 per point
+  std::vector<double> int_volt;
+  std::vector<int32_t> int_level;
+  std::vector<int32_t> sub_indx;  // 3 per point
+  std::vector<double> sub_dels;   // 6 per point
+  std::vector<double> sub_volt;   // 6 per point
+  std::vector<int32_t> sub_level;
+  // after finalize: points sorted by level; even and odd separated
+  std::vector<int32_t> istart_int, istart_even, istart_odd;
+  std::vector<int32_t> even_indx, odd_indx;
+  std::vector<double> even_dels, odd_dels, even_volt, odd_volt;
+  std::vector<int32_t> even_level, odd_level;
+  bool finalized = false;
+};
+
+struct LevelDims {
+  int nx, ny, nz;
+  double dx, dy, dz;
+};
+
+// Device conductor data of one level (one parity for subgrid lists).
+struct DevSubgrid {
+  int n = 0;
+  int32_t* ijk = nullptr;   // 3 per point
+  double* dels = nullptr;   // 6 per point
+  double* volt = nullptr;   // 6 per point
+  double* prev = nullptr;   // prevphi (FP64 V-cycles)
+  float* prevf = nullptr;   // prevphi (FP32 V-cycles)
+};
+
+struct Level {
+  LevelDims d;
+  size_t np = 0;  // (nx+3)(ny+3)(nz+3)
+  size_t nr = 0;  // (nx+1)(ny+1)(nz+1)
+  double* phi = nullptr;
+  double* rhs = nullptr;
+  double* res = nullptr;
+  float* phif = nullptr;
+  float* rhsf = nullptr;
+  float* resf = nullptr;
+  int n_int = 0;
+  int32_t* int_ijk = nullptr;
+  double* int_volt = nullptr;
+  DevSubgrid sub[2];   // 0 even, 1 odd
+  uint32_t* mask = nullptr;  // 1 bit per node: conductor (interior or subgrid) node
+  bool has_neumann_sub = false;
+};
+
+std::vector<LevelDims> mglevels(int nx, int ny, int nz, double dx, double dy, double dz);
+
+// Conductor generation and checking (wg_conductors.cpp).
+int add_shape(HostConductors& C, const std::vector<LevelDims>& lv, double xmmin, double ymmin, double zmmin,
+              int kind, double radius, double length, double voltage, double xcent, double ycent, double zcent,
+              int condid, double dfill);
+int finalize_conductors(HostConductors& C, const std::vector<LevelDims>& lv);
+
+}  // namespace wg
+
+struct wg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  wg_grid grid;
+  double dx, dy, dz;
+  std::vector<wg::Level> lv;
+  wg::HostConductors cond;
+  // level-0 work arrays
+  double* phisave = nullptr;          // copy of phi at the start of a V-cycle
+  double* rho = nullptr;              // user-visible rho (Fortran layout)
+  unsigned long long* racc = nullptr; // fixed-point deposit accumulator
+  // reductions: [0] max|dphi| bits, [1] max|res| bits, [2] max|rhs| bits, [3] flags
+  unsigned long long* dred = nullptr;
+  unsigned long long* hred = nullptr;  // pinned host copy
+  double* dmom = nullptr;              // moment partial sums
+  int mom_blocks = 0;
+  // lattice tables
+  double* czs = nullptr;
+  double* cze = nullptr;
+  double* cdb = nullptr;
+  int nzl = -1;
+  double zlmin = 0., dzl = 1.;
+  bool have_fp32 = false;
+  // kernels launched by this context (cumulative)
+  long long nlaunch = 0;
+  // CUDA-event timing of selected kernel kinds (WG_PROF_* bits)
+  int prof_mask = 0;
+  std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
+  std::vector<int> prof_kind;
+  std::vector<double> prof_units;
+  size_t prof_used = 0;
+
+  // Records a start event for a launch of `kind`; returns the pair index or -1.
+  int prof_begin(int kind, double units) {
+    if (!(prof_mask & (1 << kind)) || prof_used >= prof_kind.size()) return -1;
+    size_t i = prof_used++;
+    prof_kind[i] = kind;
+    prof_units[i] = units;
+    cudaEventRecord(prof_ev[2 * i], stream);
+    return (int)i;
+  }
+  void prof_end(int i) {
+    if (i >= 0) cudaEventRecord(prof_ev[2 * (size_t)i + 1], stream);
+  }
+};

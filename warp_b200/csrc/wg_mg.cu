@@ -1,0 +1,794 @@
+// Multigrid Poisson solver with subgrid conductors on one B200.
+//
+// Device kernels for the phases of multigrid3dsolve (pywarp90/f3d_mgrid.F:83-500):
+// red-black SOR half passes, subgrid conductor stencil, residual, restriction,
+// prolongation and guard-plane boundary conditions, for FP64 and FP32 levels,
+// plus the host-side V-cycle driver. This translation unit is compiled with
+// --fmad=false and evaluates every expression in the reference's operand
+// order, so with identical inputs the FP64 path reproduces the CPU oracle
+// bit for bit.
+//
+// Layout: each level keeps phi and res as (nx+3)(ny+3)(nz+3) arrays with one
+// guard cell and rhs as (nx+1)(ny+1)(nz+1), x fastest (the reference's
+// Fortran layout), so the user-visible solver.phi needs no repacking.
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "wg_internal.h"
+
+namespace wg {
+
+namespace {
+
+constexpr double kEps0 = 1. / (4. * 3.14159265358979323 * 1.e-7 * 2.99792458e+8 * 2.99792458e+8);
+
+struct Bnd {
+  int b[6];
+};
+
+__host__ __device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
+  return (size_t)(ix + 1) + (size_t)(nx + 3) * ((size_t)(iy + 1) + (size_t)(ny + 3) * (size_t)(iz + 1));
+}
+__host__ __device__ inline size_t rix(int nx, int ny, int ix, int iy, int iz) {
+  return (size_t)ix + (size_t)(nx + 1) * ((size_t)iy + (size_t)(ny + 1) * (size_t)iz);
+}
+
+__device__ inline void atomic_max_nonneg(unsigned long long* addr, double v) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+__device__ inline double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// Block-wide max folded into *addr (all threads must call).
+__device__ inline void block_max_to(unsigned long long* addr, double v) {
+  __shared__ double sm[32];
+  v = warp_max(v);
+  int lane = threadIdx.x & 31, wid = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+  int nw = (blockDim.x * blockDim.y + 31) >> 5;
+  if (lane == 0) sm[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double w = (lane < nw) ? sm[lane] : 0.;
+    w = warp_max(w);
+    if (lane == 0 && w > 0.) atomic_max_nonneg(addr, w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// applyboundaryconditions3d (f3d_mgrid.F:3847-3955), ncomp = 1, one guard.
+// The x phase, then the y phase over all x (guards included), then the z
+// phase over all x and y, exactly as the reference orders them.
+template <typename T>
+__global__ void k_bc_xy(T* __restrict__ u, int nx, int ny, Bnd B, int lwithdirichlet) {
+  const int iz = blockIdx.x;
+  const size_t sy = nx + 3;
+  const size_t base = (size_t)(ny + 3) * sy * (size_t)(iz + 1);
+  for (int iy = threadIdx.x; iy <= ny; iy += blockDim.x) {
+    T* r = u + base + sy * (iy + 1) + 1;  // r[ix] = u(ix,iy,iz)
+    if (lwithdirichlet) {
+      if (B.b[0] == 0) r[-1] = (T)2. * r[0] - r[1];
+      if (B.b[1] == 0) r[nx + 1] = (T)2. * r[nx] - r[nx - 1];
+    }
+    if (B.b[0] == 1) r[-1] = r[1];
+    if (B.b[1] == 1) r[nx + 1] = r[nx - 1];
+    if (B.b[0] == 2 && B.b[1] == 2) {
+      r[-1] = r[nx - 1];
+      r[nx] = r[0];
+      r[nx + 1] = r[1];
+    }
+  }
+  __syncthreads();
+  for (int ix = -1 + (int)threadIdx.x; ix <= nx + 1; ix += blockDim.x) {
+    T* c = u + base + (ix + 1) + sy;  // c[iy*sy] = u(ix,iy,iz)
+    auto C = [&](int iy) -> T& { return c[(ptrdiff_t)iy * (ptrdiff_t)sy]; };
+    if (lwithdirichlet) {
+      if (B.b[2] == 0) C(-1) = (T)2. * C(0) - C(1);
+      if (B.b[3] == 0) C(ny + 1) = (T)2. * C(ny) - C(ny - 1);
+    }
+    if (B.b[2] == 1) C(-1) = C(1);
+    if (B.b[3] == 1) C(ny + 1) = C(ny - 1);
+    if (B.b[2] == 2 && B.b[3] == 2) {
+      C(-1) = C(ny - 1);
+      C(ny) = C(0);
+      C(ny + 1) = C(1);
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_bc_z(T* __restrict__ u, int nx, int ny, int nz, Bnd B, int lwithdirichlet) {
+  const size_t nxy = (size_t)(nx + 3) * (ny + 3);
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nxy) return;
+  T* c = u + t + nxy;  // c[iz*nxy] = u(.,.,iz)
+  auto C = [&](int iz) -> T& { return c[(ptrdiff_t)iz * (ptrdiff_t)nxy]; };
+  if (lwithdirichlet) {
+    if (B.b[4] == 0) C(-1) = (T)2. * C(0) - C(1);
+    if (B.b[5] == 0) C(nz + 1) = (T)2. * C(nz) - C(nz - 1);
+  }
+  if (B.b[4] == 1) C(-1) = C(1);
+  if (B.b[5] == 1) C(nz + 1) = C(nz - 1);
+  if (B.b[4] == 2 && B.b[5] == 2) {
+    C(-1) = C(nz - 1);
+    C(nz) = C(0);
+    C(nz + 1) = C(1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sorhalfpass3d bulk loop (f3d_mgrid.F:2229-2243): one colour, in place.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny,
+                                                  int ixmin, int ixmax, int iymin, int iymax, int izmin, int parity,
+                                                  T cx, T cy, T cz, T spm1) {
+  const int iz = izmin + blockIdx.z;
+  const int iy = iymin + blockIdx.y * blockDim.y + threadIdx.y;
+  if (iy > iymax) return;
+  const int ix = ixmin + ((ixmin + iy + iz + parity) & 1) + 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (ix > ixmax) return;
+  const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
+  const size_t p = pix(nx, ny, ix, iy, iz);
+  phi[p] = rhs[rix(nx, ny, ix, iy, iz)] + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy +
+           (phi[p - sz] + phi[p + sz]) * cz + spm1 * phi[p];
+}
+
+// Saves phi at the subgrid points of one colour (prevphi, f3d_mgrid.F:2206-2226).
+template <typename T>
+__global__ void k_save_prev(const T* __restrict__ phi, int nx, int ny, const int32_t* __restrict__ ijk, int n,
+                            T* __restrict__ prev) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  prev[i] = phi[pix(nx, ny, ijk[3 * i], ijk[3 * i + 1], ijk[3 * i + 2])];
+}
+
+// handlesubgrid2 (f3d_mgrid.F:2628-2764).
+template <typename T>
+__device__ inline void handlesubgrid2(int im, int ip, T& pm, T& pp, T dsqicos, const double* dels, const double* volt,
+                                      T voltfac, T& denom, T& ppp) {
+  const T dm = (T)dels[im], dp = (T)dels[ip];
+  const T one = (T)1., two = (T)2., half = (T)0.5, zero = (T)0.;
+  const T nearone = (T)(1. - 1.e-9);
+  if (zero < dm && dm < one && zero < dp && dp < one) {
+    pm = voltfac * (T)volt[im] * two / (dm * (dp + dm));
+    pp = voltfac * (T)volt[ip] * two / (dp * (dp + dm));
+    denom = denom + two * (one - dp * dm) / (dp * dm) * dsqicos;
+    ppp = fmin(ppp, dm);
+    ppp = fmin(ppp, dp);
+  } else if (zero >= dm && dm > -one && zero >= dp && dp > -one) {
+    pm = zero;
+    pp = zero;
+    denom = denom - two * dsqicos;
+    ppp = (fabs(dm) > zero) ? (T)fmin(ppp, (T)fabs(dm)) : (T)fmin(ppp, nearone);
+    ppp = (fabs(dp) > zero) ? (T)fmin(ppp, (T)fabs(dp)) : (T)fmin(ppp, nearone);
+  } else if (zero < dm && dm < one && zero >= dp && dp > -one) {
+    const T adel = fabs(dp);
+    pm = voltfac * (T)volt[im] / (dm * (adel + half * dm));
+    pp = zero;
+    denom = denom + (one - two * dm * adel - dm) / (dm * (adel + half * dm)) * dsqicos;
+    ppp = fmin(ppp, dm);
+    ppp = (adel > zero) ? (T)fmin(ppp, adel) : (T)fmin(ppp, nearone);
+  } else if (zero >= dm && dm > -one && zero < dp && dp < one) {
+    const T adel = fabs(dm);
+    pm = zero;
+    pp = voltfac * (T)volt[ip] / (dp * (adel + half * dp));
+    denom = denom + (one - two * dp * adel - dp) / (dp * (adel + half * dp)) * dsqicos;
+    ppp = (adel > zero) ? (T)fmin(ppp, adel) : (T)fmin(ppp, nearone);
+    ppp = fmin(ppp, dp);
+  } else {
+    if (zero < dm && dm < one) {
+      pm = voltfac * (T)volt[im] * two / (dm * (one + dm));
+      pp = pp * (two / (one + dm));
+      denom = denom + two * (one - dm) / dm * dsqicos;
+      ppp = fmin(ppp, dm);
+    } else if (zero >= dm && dm > -one) {
+      const T adel = fabs(dm);
+      pm = zero;
+      pp = pp / (half + adel);
+      denom = denom - two * adel / (adel + half) * dsqicos;
+      ppp = (adel > zero) ? (T)fmin(ppp, adel) : (T)fmin(ppp, nearone);
+    }
+    if (zero < dp && dp < one) {
+      pp = voltfac * (T)volt[ip] * two / (dp * (one + dp));
+      pm = pm * (two / (one + dp));
+      denom = denom + two * (one - dp) / dp * dsqicos;
+      ppp = fmin(ppp, dp);
+    } else if (zero >= dp && dp > -one) {
+      const T adel = fabs(dp);
+      pp = zero;
+      pm = pm / (half + adel);
+      denom = denom - two * adel / (adel + half) * dsqicos;
+      ppp = (adel > zero) ? (T)fmin(ppp, adel) : (T)fmin(ppp, nearone);
+    }
+  }
+}
+
+struct SorCoef {
+  double cx, cy, cz, spm1, mgparam;
+};
+
+// condbndymg (icndbndy = 2, f3d_mgrid.F:2874-2978) for one colour, then
+// cond_potmg (f3d_mgrid.F:2426-2470) for the interior points. The two sets
+// are disjoint and only read the other colour, so one launch does both.
+template <typename T>
+__global__ void k_special_sor(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny, int nz,
+                              const int32_t* __restrict__ sijk, const double* __restrict__ sdels,
+                              const double* __restrict__ svolt, const T* __restrict__ prev, int nsub,
+                              const int32_t* __restrict__ iijk, const double* __restrict__ ivolt, int nint, Bnd B,
+                              SorCoef c, int voltfac_on, int usev) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nsub) {
+    const int ix = sijk[3 * i], iy = sijk[3 * i + 1], iz = sijk[3 * i + 2];
+    if (ix == 0 && B.b[0] < 1) return;
+    if (ix == nx && B.b[1] < 1) return;
+    if (iy == 0 && B.b[2] < 1) return;
+    if (iy == ny && B.b[3] < 1) return;
+    if (iz == 0 && B.b[4] < 1) return;
+    if (iz == nz && B.b[5] < 1) return;
+    const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
+    const size_t p = pix(nx, ny, ix, iy, iz);
+    T pxm = phi[p - 1], pxp = phi[p + 1], pym = phi[p - sy], pyp = phi[p + sy], pzm = phi[p - sz], pzp = phi[p + sz];
+    const T dxsqic = (T)c.cx, dysqic = (T)c.cy, dzsqic = (T)c.cz;
+    const T dxsqicos = (T)(c.cx / c.mgparam), dysqicos = (T)(c.cy / c.mgparam), dzsqicos = (T)(c.cz / c.mgparam);
+    const T voltfac = voltfac_on ? (T)1. : (T)0.;
+    T denom = (T)1., ppp = (T)1.;
+    const double* d = sdels + 6 * (size_t)i;
+    const double* v = svolt + 6 * (size_t)i;
+    handlesubgrid2<T>(0, 1, pxm, pxp, dxsqicos, d, v, voltfac, denom, ppp);
+    handlesubgrid2<T>(2, 3, pym, pyp, dysqicos, d, v, voltfac, denom, ppp);
+    handlesubgrid2<T>(4, 5, pzm, pzp, dzsqicos, d, v, voltfac, denom, ppp);
+    if (ppp < (T)1.) {
+      phi[p] = (rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic) /
+                   denom +
+               (T)c.spm1 * prev[i];
+    } else {
+      // no special direction: the bulk update the reference would have kept
+      phi[p] = rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic +
+               (T)c.spm1 * prev[i];
+    }
+    return;
+  }
+  i -= nsub;
+  if (i < nint) phi[pix(nx, ny, iijk[3 * i], iijk[3 * i + 1], iijk[3 * i + 2])] = usev ? (T)ivolt[i] : (T)0.;
+}
+
+// cond_potmg alone (start of sorpass3d and the mgform=2 initial phi).
+template <typename T>
+__global__ void k_interior(T* __restrict__ phi, int nx, int ny, const int32_t* __restrict__ iijk,
+                           const double* __restrict__ ivolt, int nint, int usev) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nint) phi[pix(nx, ny, iijk[3 * i], iijk[3 * i + 1], iijk[3 * i + 2])] = usev ? (T)ivolt[i] : (T)0.;
+}
+
+// condbndymgint (f3d_mgrid.F:2982-3092): Neumann subgrid neighbours take the
+// point's value. Points of both colours in one launch.
+template <typename T>
+__global__ void k_condbndymgint(T* __restrict__ phi, int nx, int ny, int nz, const int32_t* __restrict__ ijk,
+                                const double* __restrict__ dels, int n, Bnd B) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int ix = ijk[3 * i], iy = ijk[3 * i + 1], iz = ijk[3 * i + 2];
+  const double* d = dels + 6 * (size_t)i;
+  const T p0 = phi[pix(nx, ny, ix, iy, iz)];
+  if (!((ix - 1 == 0 && B.b[0] == 0) || (ix + 1 == nx && B.b[1] == 0) || (ix == 0 && B.b[0] < 1) ||
+        (ix == nx && B.b[1] < 1))) {
+    if (0. >= d[0] && d[0] > -1.) phi[pix(nx, ny, ix - 1, iy, iz)] = p0;
+    if (0. >= d[1] && d[1] > -1.) phi[pix(nx, ny, ix + 1, iy, iz)] = p0;
+  }
+  if (!((iy - 1 == 0 && B.b[2] == 0) || (iy + 1 == ny && B.b[3] == 0) || (iy == 0 && B.b[2] < 1) ||
+        (iy == ny && B.b[3] < 1))) {
+    if (0. >= d[2] && d[2] > -1.) phi[pix(nx, ny, ix, iy - 1, iz)] = p0;
+    if (0. >= d[3] && d[3] > -1.) phi[pix(nx, ny, ix, iy + 1, iz)] = p0;
+  }
+  if (!((iz - 1 == 0 && B.b[4] == 0) || (iz + 1 == nz && B.b[5] == 0) || (iz == 0 && B.b[4] < 1) ||
+        (iz == nz && B.b[5] < 1))) {
+    if (0. >= d[4] && d[4] > -1.) phi[pix(nx, ny, ix, iy, iz - 1)] = p0;
+    if (0. >= d[5] && d[5] > -1.) phi[pix(nx, ny, ix, iy, iz + 1)] = p0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// residual3d bulk part (f3d_mgrid.F:3519-3586).
+//   MODE 0: writes the padded res array (0 outside the updated range)
+//   MODE 1: no store, only the max over non-special nodes (norm)
+//   MODE 2: writes the unpadded FP32 rhs of the next correction solve
+// The max skips nodes flagged in `mask` (conductor nodes), which the special
+// kernel handles.
+template <typename T, int MODE, typename TO>
+__global__ void __launch_bounds__(256) k_residual(const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                  TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
+                                                  int ixmax, int iymin, int iymax, int izmin, int izmax, T cx, T cy,
+                                                  T cz, T mgparam, const uint32_t* __restrict__ mask,
+                                                  unsigned long long* maxout) {
+  // MODE 0 covers the padded array, the others the node array
+  const int g = (MODE == 0) ? 1 : 0;
+  const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x) - g;
+  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y) - g;
+  const int iz = (int)blockIdx.z - g;
+  double m = 0.;
+  bool live = ix <= nx + g && iy <= ny + g;
+  if (live) {
+    T r = (T)0.;
+    bool inrange = ix >= ixmin && ix <= ixmax && iy >= iymin && iy <= iymax && iz >= izmin && iz <= izmax;
+    if (inrange) {
+      const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
+      const size_t p = pix(nx, ny, ix, iy, iz);
+      r = rhs[rix(nx, ny, ix, iy, iz)] + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy +
+          (phi[p - sz] + phi[p + sz]) * cz - phi[p] * mgparam;
+      if (maxout) {
+        size_t ri = rix(nx, ny, ix, iy, iz);
+        bool special = mask && ((mask[ri >> 5] >> (ri & 31)) & 1u);
+        if (!special) m = fabs((double)r);
+      }
+    }
+    if (MODE == 0) out[pix(nx, ny, ix, iy, iz)] = (TO)r;
+    if (MODE == 2) out[rix(nx, ny, ix, iy, iz)] = (TO)r;
+  }
+  if (maxout) block_max_to(maxout, m);
+}
+
+// cond_potmgres (interior -> 0, f3d_mgrid.F:2472-2500) and condbndyres
+// (icndbndy = 2, f3d_mgrid.F:3240-3362) for both colours.
+template <typename T, int MODE, typename TO>
+__global__ void k_special_res(const T* __restrict__ phi, const T* __restrict__ rhs, TO* __restrict__ out, int nx,
+                              int ny, int nz, const int32_t* __restrict__ ijk0, const double* __restrict__ dels0,
+                              const double* __restrict__ volt0, int n0, const int32_t* __restrict__ ijk1,
+                              const double* __restrict__ dels1, const double* __restrict__ volt1, int n1,
+                              const int32_t* __restrict__ iijk, int nint, Bnd B, double dxsqi, double dysqi,
+                              double dzsqi, double mgparam_d, int voltfac_on, int mgform2init,
+                              unsigned long long* maxout) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.;
+  auto store = [&](int ix, int iy, int iz, T v) {
+    if (MODE == 0) out[pix(nx, ny, ix, iy, iz)] = (TO)v;
+    if (MODE == 2 && ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz)
+      out[rix(nx, ny, ix, iy, iz)] = (TO)v;
+  };
+  if (i < nint) {
+    store(iijk[3 * i], iijk[3 * i + 1], iijk[3 * i + 2], (T)0.);
+  } else if (i < nint + n0 + n1) {
+    int k = i - nint;
+    const int32_t* ijk = (k < n0) ? ijk0 : ijk1;
+    const double* dd = (k < n0) ? dels0 : dels1;
+    const double* vv = (k < n0) ? volt0 : volt1;
+    if (k >= n0) k -= n0;
+    const int ix = ijk[3 * k], iy = ijk[3 * k + 1], iz = ijk[3 * k + 2];
+    bool skip = (ix == 0 && B.b[0] == 0) || (ix == nx && B.b[1] == 0) || (iy == 0 && B.b[2] == 0) ||
+                (iy == ny && B.b[3] == 0) || (iz == 0 && B.b[4] == 0) || (iz == nz && B.b[5] == 0);
+    if (!skip) {
+      const double cst = 0.5 / (dxsqi + dysqi + dzsqi);
+      const T dxsqic = (T)(dxsqi * cst), dysqic = (T)(dysqi * cst), dzsqic = (T)(dzsqi * cst);
+      const T dxsqics = (T)(mgparam_d * dxsqi * cst), dysqics = (T)(mgparam_d * dysqi * cst),
+              dzsqics = (T)(mgparam_d * dzsqi * cst);
+      const T mgparam = (T)mgparam_d;
+      const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
+      const size_t p = pix(nx, ny, ix, iy, iz);
+      T pxm = phi[p - 1], pxp = phi[p + 1], pym = phi[p - sy], pyp = phi[p + sy], pzm = phi[p - sz],
+        pzp = phi[p + sz];
+      T denom = (T)1., ppp = (T)1.;
+      const T voltfac = voltfac_on ? (T)1. : (T)0.;
+      const double* d = dd + 6 * (size_t)k;
+      const double* v = vv + 6 * (size_t)k;
+      handlesubgrid2<T>(0, 1, pxm, pxp, dxsqic, d, v, voltfac, denom, ppp);
+      handlesubgrid2<T>(2, 3, pym, pyp, dysqic, d, v, voltfac, denom, ppp);
+      handlesubgrid2<T>(4, 5, pzm, pzp, dzsqic, d, v, voltfac, denom, ppp);
+      if (ppp < (T)1.) {
+        if (mgform2init) ppp = (T)1.;
+        T r = ppp * (rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqics + (pym + pyp) * dysqics +
+                     (pzm + pzp) * dzsqics - phi[p] * mgparam * denom);
+        store(ix, iy, iz, r);
+        m = fabs((double)r);
+        if (0. >= d[0] && d[0] >= -1.) store(ix - 1, iy, iz, (T)0.);
+        if (0. >= d[1] && d[1] >= -1.) store(ix + 1, iy, iz, (T)0.);
+        if (0. >= d[2] && d[2] >= -1.) store(ix, iy - 1, iz, (T)0.);
+        if (0. >= d[3] && d[3] >= -1.) store(ix, iy + 1, iz, (T)0.);
+        if (0. >= d[4] && d[4] >= -1.) store(ix, iy, iz - 1, (T)0.);
+        if (0. >= d[5] && d[5] >= -1.) store(ix, iy, iz + 1, (T)0.);
+      } else {
+        // the bulk value stays; it was left out of the bulk max
+        T r = rhs[rix(nx, ny, ix, iy, iz)] + (phi[p - 1] + phi[p + 1]) * dxsqics +
+              (phi[p - sy] + phi[p + sy]) * dysqics + (phi[p - sz] + phi[p + sz]) * dzsqics - phi[p] * mgparam;
+        m = fabs((double)r);
+      }
+    }
+  }
+  if (maxout) block_max_to(maxout, m);
+}
+
+// restrict3d (f3d_mgrid.F:1593-1775), serial: one thread per coarse node,
+// summing the tent-weighted fine residual in the reference's loop order.
+template <typename T>
+__global__ void k_restrict(const T* __restrict__ res, T* __restrict__ rhoc, int nx, int ny, int nz, int nxc, int nyc,
+                           int nzc, int ixcmin, int ixcmax, int iycmin, int iycmax, int izcmin, int izcmax, double dxi,
+                           double dyi, double dzi, double ff) {
+  const int ixc = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iyc = blockIdx.y * blockDim.y + threadIdx.y;
+  const int izc = blockIdx.z;
+  if (ixc > nxc || iyc > nyc) return;
+  const size_t o = rix(nxc, nyc, ixc, iyc, izc);
+  if (ixc < ixcmin || ixc > ixcmax || iyc < iycmin || iyc > iycmax || izc < izcmin || izc > izcmax) {
+    rhoc[o] = (T)0.;
+    return;
+  }
+  auto lim = [](int ic, int n, int nc, int& lo, int& hi) {
+    lo = ((ic - 1) * n + 4 * nc) / nc - 3;
+    hi = ((ic + 1) * n - 1) / nc;
+    lo = max(lo, -1);
+    hi = min(hi, n + 1);
+  };
+  int ixmin, ixmax, iymin, iymax, izmin, izmax;
+  lim(ixc, nx, nxc, ixmin, ixmax);
+  lim(iyc, ny, nyc, iymin, iymax);
+  lim(izc, nz, nzc, izmin, izmax);
+  T r = (T)0., w = (T)0.;
+  for (int iz = izmin; iz <= izmax; ++iz) {
+    const T wz = (T)(1. - fabs(izc - (iz + 0.) * dzi));
+    for (int iy = iymin; iy <= iymax; ++iy) {
+      const T wy = (T)(1. - fabs(iyc - (iy + 0.) * dyi));
+      for (int ix = ixmin; ix <= ixmax; ++ix) {
+        const T wx = (T)(1. - fabs(ixc - (ix + 0.) * dxi));
+        r = r + wx * wy * wz * res[pix(nx, ny, ix, iy, iz)];
+        w = w + wx * wy * wz;
+      }
+    }
+  }
+  if (w > (T)0.) {
+    r = r / w;
+    rhoc[o] = r * (T)ff;
+  } else {
+    rhoc[o] = (T)0.;
+  }
+}
+
+// expand3d (f3d_mgrid.F:1777-1947): trilinear prolongation added to phi.
+template <typename T>
+__global__ void k_expand(T* __restrict__ phi, const T* __restrict__ pc, int nx, int ny, int nxc, int nyc, int nzc,
+                         int nz, int ixmin, int ixmax, int iymin, int iymax, int izmin) {
+  const int ix = ixmin + blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = iymin + blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = izmin + blockIdx.z;
+  if (ix > ixmax || iy > iymax) return;
+  const int jz = (iz * nzc) / nz, jy = (iy * nyc) / ny, jx = (ix * nxc) / nx;
+  const T wz = (T)(1. * (iz * nzc) / nz - jz), wy = (T)(1. * (iy * nyc) / ny - jy), wx = (T)(1. * (ix * nxc) / nx - jx);
+  const T one = (T)1.;
+  T& p = phi[pix(nx, ny, ix, iy, iz)];
+  p = p + (one - wx) * (one - wy) * (one - wz) * pc[pix(nxc, nyc, jx, jy, jz)] +
+      wx * (one - wy) * (one - wz) * pc[pix(nxc, nyc, jx + 1, jy, jz)] +
+      (one - wx) * wy * (one - wz) * pc[pix(nxc, nyc, jx, jy + 1, jz)] +
+      wx * wy * (one - wz) * pc[pix(nxc, nyc, jx + 1, jy + 1, jz)] +
+      (one - wx) * (one - wy) * wz * pc[pix(nxc, nyc, jx, jy, jz + 1)] +
+      wx * (one - wy) * wz * pc[pix(nxc, nyc, jx + 1, jy, jz + 1)] +
+      (one - wx) * wy * wz * pc[pix(nxc, nyc, jx, jy + 1, jz + 1)] +
+      wx * wy * wz * pc[pix(nxc, nyc, jx + 1, jy + 1, jz + 1)];
+}
+
+// mgerror = max|phisave - phi| over nodes 0..n (f3d_mgrid.F:383-391).
+__global__ void k_maxdiff(const double* __restrict__ a, const double* __restrict__ b, int nx, int ny,
+                          unsigned long long* maxout) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  double m = 0.;
+  if (ix <= nx && iy <= ny) {
+    size_t p = pix(nx, ny, ix, iy, iz);
+    m = fabs(a[p] - b[p]);
+  }
+  block_max_to(maxout, m);
+}
+
+// rhs = rho * reps0c (f3d_mgrid.F:223) and max|rhs|.
+__global__ void k_scale_rhs(const double* __restrict__ rho, double* __restrict__ rhs, size_t n, double s,
+                            unsigned long long* maxout) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.;
+  if (i < n) {
+    double v = rho[i] * s;
+    rhs[i] = v;
+    m = fabs(v);
+  }
+  block_max_to(maxout, m);
+}
+
+// Residual-correction update phi = e + phisave (f3d_mgrid.F:355-358) with
+// e from an FP32 V-cycle; max|dphi| over nodes 0..n.
+__global__ void k_add_corr(double* __restrict__ phi, const float* __restrict__ e, int nx, int ny, int nz,
+                           unsigned long long* maxout) {
+  const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 1;
+  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
+  const int iz = (int)blockIdx.z - 1;
+  double m = 0.;
+  if (ix <= nx + 1 && iy <= ny + 1) {
+    size_t p = pix(nx, ny, ix, iy, iz);
+    double old = phi[p];
+    double nw = (double)e[p] + old;
+    phi[p] = nw;
+    if (ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz) m = fabs(old - nw);
+  }
+  block_max_to(maxout, m);
+}
+
+inline unsigned cdiv(size_t a, unsigned b) { return (unsigned)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// Host driver
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Arr;
+template <>
+struct Arr<double> {
+  static double* phi(Level& L) { return L.phi; }
+  static double* rhs(Level& L) { return L.rhs; }
+  static double* res(Level& L) { return L.res; }
+  static double* prev(DevSubgrid& S) { return S.prev; }
+};
+template <>
+struct Arr<float> {
+  static float* phi(Level& L) { return L.phif; }
+  static float* rhs(Level& L) { return L.rhsf; }
+  static float* res(Level& L) { return L.resf; }
+  static float* prev(DevSubgrid& S) { return S.prevf; }
+};
+
+struct Ranges {
+  int ixmin, ixmax, iymin, iymax, izmin, izmax;
+};
+// Loop limits: `le` = limits of sorhalfpass3d (bound <= 0 excludes the edge),
+// else those of residual3d/expand3d/restrict3d (bound == 0 excludes it).
+Ranges ranges(const LevelDims& d, const int* b, bool le) {
+  Ranges r{0, d.nx, 0, d.ny, 0, d.nz};
+  auto dir = [&](int v) { return le ? v <= 0 : v == 0; };
+  if (dir(b[0])) r.ixmin = 1;
+  if (dir(b[1])) r.ixmax = d.nx - 1;
+  if (dir(b[2])) r.iymin = 1;
+  if (dir(b[3])) r.iymax = d.ny - 1;
+  if (dir(b[4])) r.izmin = 1;
+  if (dir(b[5])) r.izmax = d.nz - 1;
+  return r;
+}
+
+struct Solver {
+  wg_ctx* c;
+  const wg_solve_opts* o;
+  Bnd B;
+  cudaStream_t s;
+
+  template <typename T>
+  void bc(Level& L, T* u, bool lwithdirichlet) {
+    const int* b = B.b;
+    bool xy = lwithdirichlet || b[0] >= 1 || b[1] >= 1 || b[2] >= 1 || b[3] >= 1;
+    bool z = lwithdirichlet || b[4] >= 1 || b[5] >= 1;
+    if (xy) { ++c->nlaunch; k_bc_xy<T><<<L.d.nz + 1, 256, 0, s>>>(u, L.d.nx, L.d.ny, B, (int)lwithdirichlet); }
+    if (z) {
+      size_t nxy = (size_t)(L.d.nx + 3) * (L.d.ny + 3);
+      { ++c->nlaunch; k_bc_z<T><<<cdiv(nxy, 256), 256, 0, s>>>(u, L.d.nx, L.d.ny, L.d.nz, B, (int)lwithdirichlet); }
+    }
+  }
+
+  SorCoef coef(const LevelDims& d) const {
+    double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
+    double cst = o->mgparam * 0.5 / (dxsqi + dysqi + dzsqi);
+    return SorCoef{dxsqi * cst, dysqi * cst, dzsqi * cst, 1. - o->mgparam, o->mgparam};
+  }
+
+  template <typename T>
+  void neumann_int(Level& L, T* phi) {
+    if (!L.has_neumann_sub) return;
+    for (int par = 0; par < 2; ++par) {
+      DevSubgrid& S = L.sub[par];
+      if (S.n)
+        { ++c->nlaunch; k_condbndymgint<T><<<cdiv(S.n, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, S.ijk, S.dels, S.n, B); }
+    }
+  }
+
+  // sorpass3d (f3d_mgrid.F:1949-2093)
+  template <typename T>
+  void sorpass(int l, bool usev) {
+    Level& L = c->lv[l];
+    T* phi = Arr<T>::phi(L);
+    const T* rhs = Arr<T>::rhs(L);
+    if (L.n_int) { ++c->nlaunch; k_interior<T><<<cdiv(L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev); }
+    neumann_int<T>(L, phi);
+    const Ranges R = ranges(L.d, B.b, true);
+    const SorCoef k = coef(L.d);
+    const int nyr = R.iymax - R.iymin + 1, nzr = R.izmax - R.izmin + 1;
+    const int nhalf = (R.ixmax - R.ixmin) / 2 + 1;
+    for (int parity = 0; parity < 2; ++parity) {
+      DevSubgrid& S = L.sub[parity];
+      int nsub = o->lcndbndy ? S.n : 0;
+      if (nsub) { ++c->nlaunch; k_save_prev<T><<<cdiv(nsub, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, S.ijk, nsub, Arr<T>::prev(S)); }
+      if (nyr > 0 && nzr > 0 && nhalf > 0) {
+        dim3 blk(32, 8), grd(cdiv(nhalf, 32), cdiv(nyr, 8), nzr);
+        { ++c->nlaunch; int pe = (l == 0) ? c->prof_begin(WG_PROF_SOR0, (double)L.nr) : -1; k_sor_bulk<T><<<grd, blk, 0, s>>>(phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin,
+                                          parity, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1); c->prof_end(pe); }
+      }
+      if (nsub + L.n_int)
+        { ++c->nlaunch; k_special_sor<T><<<cdiv(nsub + L.n_int, 128), 128, 0, s>>>(
+            phi, rhs, L.d.nx, L.d.ny, L.d.nz, S.ijk, S.dels, S.volt, Arr<T>::prev(S), nsub, L.int_ijk, L.int_volt,
+            L.n_int, B, k, (int)usev, (int)usev); }
+      neumann_int<T>(L, phi);
+      bc<T>(L, phi, false);
+    }
+  }
+
+  // residual3d into the padded res array of level l (MODE 0), or a norm only
+  // (MODE 1), or into the FP32 rhs of level 0 (MODE 2).
+  template <typename T, int MODE, typename TO>
+  void residual(int l, const T* phi, const T* rhs, TO* out, bool mgform2init, bool voltfac_on,
+                unsigned long long* maxout) {
+    Level& L = c->lv[l];
+    const Ranges R = ranges(L.d, B.b, false);
+    double dxsqi = 1. / (L.d.dx * L.d.dx), dysqi = 1. / (L.d.dy * L.d.dy), dzsqi = 1. / (L.d.dz * L.d.dz);
+    double cst = 0.5 / (dxsqi + dysqi + dzsqi);
+    const int g = (MODE == 0) ? 1 : 0;
+    dim3 blk(32, 8), grd(cdiv(L.d.nx + 1 + 2 * g, 32), cdiv(L.d.ny + 1 + 2 * g, 8), L.d.nz + 1 + 2 * g);
+    { ++c->nlaunch; int pe = (l == 0) ? c->prof_begin(WG_PROF_RESID0, (double)L.nr) : -1; k_residual<T, MODE, TO><<<grd, blk, 0, s>>>(phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
+                                                R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
+                                                (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst),
+                                                (T)o->mgparam, L.mask, maxout); c->prof_end(pe); }
+    int nsub = o->lcndbndy ? (L.sub[0].n + L.sub[1].n) : 0;
+    int n0 = o->lcndbndy ? L.sub[0].n : 0, n1 = o->lcndbndy ? L.sub[1].n : 0;
+    if (nsub + L.n_int)
+      { ++c->nlaunch; k_special_res<T, MODE, TO><<<cdiv(nsub + L.n_int, 128), 128, 0, s>>>(
+          phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, L.sub[0].ijk, L.sub[0].dels, L.sub[0].volt, n0, L.sub[1].ijk,
+          L.sub[1].dels, L.sub[1].volt, n1, L.int_ijk, L.n_int, B, dxsqi, dysqi, dzsqi, o->mgparam, (int)voltfac_on,
+          (int)mgform2init, maxout); }
+    if (MODE == 0) bc<TO>(L, (TO*)out, false);
+  }
+
+  // vcycle (f3d_mgrid.F:1101-1591)
+  template <typename T>
+  void vcycle(int l, bool usev) {
+    Level& L = c->lv[l];
+    for (int i = 0; i < o->downpasses; ++i) sorpass<T>(l, usev);
+    const LevelDims& d = L.d;
+    if (d.nx >= 4 && d.ny >= 4 && d.nz >= 4 && l < o->mgmaxlevels && l + 1 < (int)c->lv.size()) {
+      residual<T, 0, T>(l, Arr<T>::phi(L), Arr<T>::rhs(L), Arr<T>::res(L), false, usev, nullptr);
+      Level& Lc = c->lv[l + 1];
+      const LevelDims& dc = Lc.d;
+      double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
+      double dxcsqi = 1. / (dc.dx * dc.dx), dycsqi = 1. / (dc.dy * dc.dy), dzcsqi = 1. / (dc.dz * dc.dz);
+      double ff = (dxsqi + dysqi + dzsqi) / (dxcsqi + dycsqi + dzcsqi);
+      Ranges Rc = ranges(dc, B.b, false);
+      dim3 blk(32, 8), grd(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), dc.nz + 1);
+      { ++c->nlaunch; k_restrict<T><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, d.nz, dc.nx, dc.ny, dc.nz,
+                                        Rc.ixmin, Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
+                                        1. * dc.nx / d.nx, 1. * dc.ny / d.ny, 1. * dc.nz / d.nz, ff); }
+      cudaMemsetAsync(Arr<T>::phi(Lc), 0, Lc.np * sizeof(T), s);
+      vcycle<T>(l + 1, false);
+      Ranges R = ranges(d, B.b, false);
+      dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), R.izmax - R.izmin + 1);
+      if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin)
+        { ++c->nlaunch; k_expand<T><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny, dc.nz, d.nz,
+                                         R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin); }
+      bc<T>(L, Arr<T>::phi(L), false);
+    }
+    for (int i = 0; i < o->uppasses; ++i) sorpass<T>(l, usev);
+  }
+
+  int fetch_red(double* out, int n) {
+    WG_TRY_CUDA(cudaMemcpyAsync(c->hred, c->dred, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    WG_TRY_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; ++i) {
+      unsigned long long v = c->hred[i];
+      double dv;
+      memcpy(&dv, &v, sizeof(double));
+      out[i] = dv;
+    }
+    return WG_OK;
+  }
+};
+
+}  // namespace
+
+int ensure_fp32(wg_ctx* c);
+
+int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
+  if (!o || !st) { set_error("wg_solve: null options or stats"); return WG_EINVAL; }
+  if (!(o->mgparam > 0. && o->mgparam < 2.) || o->mgmaxiters < 0 || o->downpasses < 0 || o->uppasses < 0 ||
+      (o->precision != 0 && o->precision != 1) || (o->tolkind != 0 && o->tolkind != 1)) {
+    set_error("wg_solve: invalid options");
+    return WG_EINVAL;
+  }
+  if (o->precision == 1) WG_TRY(ensure_fp32(c));
+  Solver S{c, o, {}, c->stream};
+  for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
+  cudaStream_t s = c->stream;
+  Level& L0 = c->lv[0];
+  const LevelDims& d = L0.d;
+  double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
+  double reps0c = o->mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
+  unsigned long long* red = c->dred;
+  WG_TRY_CUDA(cudaMemsetAsync(red, 0, 4 * sizeof(unsigned long long), s));
+  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, red + 2); }
+  S.bc<double>(L0, L0.phi, false);
+  dim3 blk(32, 8), grdn(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1);
+  dim3 grdp(cdiv(d.nx + 3, 32), cdiv(d.ny + 3, 8), d.nz + 3);
+  int it = 0;
+  double err = 2. * o->mgtol + 1., relres = -1.;
+  bool conv = false;
+  double rv[4];
+  if (o->precision == 0) {
+    for (;;) {
+      if (o->tolkind == 1) {
+        WG_TRY_CUDA(cudaMemsetAsync(red + 1, 0, sizeof(unsigned long long), s));
+        S.residual<double, 1, double>(0, L0.phi, L0.rhs, nullptr, true, true, red + 1);
+        WG_TRY(S.fetch_red(rv, 3));
+        relres = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
+        if (relres <= o->mgtol) { conv = true; break; }
+      }
+      if (it >= o->mgmaxiters) break;
+      if (o->tolkind == 0)
+        WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      S.vcycle<double>(0, true);
+      it += 1;
+      if (o->tolkind == 0) {
+        WG_TRY_CUDA(cudaMemsetAsync(red, 0, sizeof(unsigned long long), s));
+        { ++c->nlaunch; k_maxdiff<<<grdn, blk, 0, s>>>(c->phisave, L0.phi, d.nx, d.ny, red); }
+        WG_TRY(S.fetch_red(rv, 1));
+        err = rv[0];
+        if (!(err > o->mgtol)) { conv = true; break; }
+      }
+    }
+  } else {
+    for (;;) {
+      // residual of the FP64 solution with actual voltages (mgform = 2 set-up)
+      if (L0.n_int)
+        { ++c->nlaunch; k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(L0.phi, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1); }
+      S.neumann_int<double>(L0, L0.phi);
+      WG_TRY_CUDA(cudaMemsetAsync(red + 1, 0, sizeof(unsigned long long), s));
+      S.residual<double, 2, float>(0, L0.phi, L0.rhs, L0.rhsf, true, true, red + 1);
+      if (o->tolkind == 1 || it >= o->mgmaxiters) {
+        WG_TRY(S.fetch_red(rv, 3));
+        relres = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
+        if (o->tolkind == 1 && relres <= o->mgtol) { conv = true; break; }
+      }
+      if (it >= o->mgmaxiters) break;
+      WG_TRY_CUDA(cudaMemsetAsync(L0.phif, 0, L0.np * sizeof(float), s));
+      S.vcycle<float>(0, false);
+      WG_TRY_CUDA(cudaMemsetAsync(red, 0, sizeof(unsigned long long), s));
+      { ++c->nlaunch; k_add_corr<<<grdp, blk, 0, s>>>(L0.phi, L0.phif, d.nx, d.ny, d.nz, red); }
+      S.bc<double>(L0, L0.phi, false);
+      it += 1;
+      if (o->tolkind == 0) {
+        WG_TRY(S.fetch_red(rv, 1));
+        err = rv[0];
+        if (!(err > o->mgtol)) { conv = true; break; }
+      }
+    }
+  }
+  S.bc<double>(L0, L0.phi, true);
+  WG_TRY_CUDA(cudaGetLastError());
+  WG_TRY_CUDA(cudaStreamSynchronize(s));
+  st->mgiters = it;
+  st->converged = conv ? 1 : 0;
+  st->mgerror = (o->tolkind == 0) ? err : -1.;
+  st->relres = relres;
+  return WG_OK;
+}
+
+int relresidual(wg_ctx* c, double mgparam, double* out) {
+  wg_solve_opts o{mgparam, 0., 0, 101, 1, 1, 1, 0, 1};
+  Solver S{c, &o, {}, c->stream};
+  for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
+  cudaStream_t s = c->stream;
+  Level& L0 = c->lv[0];
+  const LevelDims& d = L0.d;
+  double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
+  double reps0c = mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
+  WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
+  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, c->dred + 2); }
+  // residual of a copy with the conductor voltages imposed, as the solver sees it
+  WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (L0.n_int)
+    { ++c->nlaunch; k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1); }
+  S.residual<double, 1, double>(0, c->phisave, L0.rhs, nullptr, true, true, c->dred + 1);
+  double rv[4];
+  WG_TRY(S.fetch_red(rv, 3));
+  *out = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
+  return WG_OK;
+}
+
+}  // namespace wg

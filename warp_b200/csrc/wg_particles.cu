@@ -1,0 +1,440 @@
+// Particle kernels: fixed-point CIC deposition, field gather, the fused
+// gather + quad + Boris leapfrog push + boundaries kernel, and moments.
+//
+// Compiled with --fmad=false: gather and push evaluate the reference's
+// expressions in its operand order, so with identical phi and particles the
+// results match the CPU oracle bit for bit. Deposition accumulates
+// round(weight * 2^46) in 64-bit integers, so rho does not depend on the
+// order of the atomic adds (bit-identical run to run); it differs from an
+// FP64 running sum only by the rounding of each weight to 2^-46.
+
+#include <cmath>
+
+#include "wg_internal.h"
+
+namespace wg {
+
+// 2^46: one particle's full CIC weight (1.0) in accumulator units. The
+// convert kernel reports WG_EOVERFLOW once a node reaches 2^62, i.e. 65536
+// full particle weights on one node (the unsigned sum wraps only at 2^64).
+constexpr double kFixScale = 70368744177664.0;  // 2^46
+constexpr double kFixInv = 1.0 / 70368744177664.0;
+
+struct GridP {
+  int nx, ny, nz;
+  double dx, dy, dz, xmmin, ymmin, zmmin, zgrid;
+};
+
+namespace {
+
+__device__ inline void cellfrac(double s, int n, int& i, double& f) {
+  i = (int)s;
+  if (i > n - 1) i = n - 1;
+  if (i < 0) i = 0;
+  f = s - i;
+}
+
+__device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
+  return (size_t)(ix + 1) + (size_t)(nx + 3) * ((size_t)(iy + 1) + (size_t)(ny + 3) * (size_t)(iz + 1));
+}
+
+// setrho3ddirect1 (w3d.F:7757-7960): 8 CIC weights per particle, summed per
+// cell within a warp (runs of equal cell index, as sorted particles give),
+// one 64-bit atomic per node per run.
+__global__ void __launch_bounds__(256) k_deposit(const double* __restrict__ xp, const double* __restrict__ yp,
+                                                 const double* __restrict__ zp, const double* __restrict__ gaminv,
+                                                 int64_t np, GridP g, unsigned long long* __restrict__ acc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int key = -1;
+  unsigned long long w[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) w[k] = 0ull;
+  if (i < np && gaminv[i] != 0.) {
+    const double dxi = 1. / g.dx, dyi = 1. / g.dy, dzi = 1. / g.dz;
+    int ii, jj, kk;
+    double u1, v1, w1;
+    cellfrac((xp[i] - g.xmmin) * dxi, g.nx, ii, u1);
+    cellfrac((yp[i] - g.ymmin) * dyi, g.ny, jj, v1);
+    cellfrac((zp[i] - g.zgrid - g.zmmin) * dzi, g.nz, kk, w1);
+    const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+    key = ii + (g.nx + 1) * (jj + (g.ny + 1) * kk);
+    w[0] = (unsigned long long)llrint(u0 * v0 * w0 * kFixScale);
+    w[1] = (unsigned long long)llrint(u1 * v0 * w0 * kFixScale);
+    w[2] = (unsigned long long)llrint(u0 * v1 * w0 * kFixScale);
+    w[3] = (unsigned long long)llrint(u1 * v1 * w0 * kFixScale);
+    w[4] = (unsigned long long)llrint(u0 * v0 * w1 * kFixScale);
+    w[5] = (unsigned long long)llrint(u1 * v0 * w1 * kFixScale);
+    w[6] = (unsigned long long)llrint(u0 * v1 * w1 * kFixScale);
+    w[7] = (unsigned long long)llrint(u1 * v1 * w1 * kFixScale);
+  }
+  // segmented suffix sums over runs of equal key within the warp
+  const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+  const bool tail = (lane == 31) || (knext != key);
+  const unsigned tails = __ballot_sync(0xffffffffu, tail);
+  const int seg_end = __ffs(tails & (0xffffffffu << lane)) - 1;
+  const int kprev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool head = (lane == 0) || (kprev != key);
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      unsigned long long t = __shfl_down_sync(0xffffffffu, w[k], off);
+      if (lane + off <= seg_end) w[k] += t;
+    }
+  }
+  if (head && key >= 0) {
+    const int sx = 1, sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+    unsigned long long* a = acc + key;
+    atomicAdd(a, w[0]);
+    atomicAdd(a + sx, w[1]);
+    atomicAdd(a + sy, w[2]);
+    atomicAdd(a + sx + sy, w[3]);
+    atomicAdd(a + sz, w[4]);
+    atomicAdd(a + sx + sz, w[5]);
+    atomicAdd(a + sy + sz, w[6]);
+    atomicAdd(a + sx + sy + sz, w[7]);
+  }
+}
+
+// rho (+)= acc * g * 2^-46; flags accumulator values at or above 2^62.
+__global__ void k_fix_to_rho(const unsigned long long* __restrict__ acc, double* __restrict__ rho, size_t n,
+                             double scale, int add, unsigned long long* flag) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long a = acc[i];
+  if (a >> 62) atomicOr(flag, 1ull);
+  double v = (double)a * scale;
+  rho[i] = add ? rho[i] + v : v;
+}
+
+// applyrhoboundaryconditions3d (w3d.F:2660-2750), serial, no rho guard:
+// one thread per line perpendicular to the face, phases x, y, z in order.
+__global__ void k_rhobc(double* __restrict__ rho, int nx, int ny, int nz, int axis, int blo, int bhi) {
+  const size_t sx = 1, sy = nx + 1, sz = (size_t)(nx + 1) * (ny + 1);
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t stride, base;
+  int n;
+  if (axis == 0) {
+    if (t >= (size_t)(ny + 1) * (nz + 1)) return;
+    base = (t % (ny + 1)) * sy + (t / (ny + 1)) * sz;
+    stride = sx;
+    n = nx;
+  } else if (axis == 1) {
+    if (t >= (size_t)(nx + 1) * (nz + 1)) return;
+    base = (t % (nx + 1)) * sx + (t / (nx + 1)) * sz;
+    stride = sy;
+    n = ny;
+  } else {
+    if (t >= (size_t)(nx + 1) * (ny + 1)) return;
+    base = (t % (nx + 1)) * sx + (t / (nx + 1)) * sy;
+    stride = sz;
+    n = nz;
+  }
+  double* lo = rho + base;
+  double* hi = rho + base + (size_t)n * stride;
+  if (blo == 1) *lo = *lo + *lo;
+  if (bhi == 1) *hi = *hi + *hi;
+  if (blo == 2 || bhi == 2) {
+    *lo = *lo + *hi;
+    *hi = *lo;
+  }
+}
+
+// sete_from_phi_linear3d (w3d.F:3963-4108), no symmetry: E from centred
+// differences of phi at the 8 cell nodes, trilinearly weighted.
+__device__ inline void gather_e(const double* __restrict__ phi, const GridP& g, double x, double y, double z,
+                                double& ext, double& eyt, double& ezt) {
+  const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
+  const double dxi = 1. / g.dx, dyi = 1. / g.dy, dzi = 1. / g.dz;
+  int i, j, k;
+  double u1, v1, w1;
+  cellfrac((x - g.xmmin) * dxi, g.nx, i, u1);
+  cellfrac((y - g.ymmin) * dyi, g.ny, j, v1);
+  cellfrac((z - g.zgrid - g.zmmin) * dzi, g.nz, k, w1);
+  const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+  const int nx = g.nx, ny = g.ny;
+  auto P = [&](int a, int b, int c) { return __ldg(phi + pix(nx, ny, a, b, c)); };
+  ext = tdxi * (u0 * v0 * w0 * (P(i - 1, j, k) - P(i + 1, j, k)) + u1 * v0 * w0 * (P(i, j, k) - P(i + 2, j, k)) +
+                u0 * v1 * w0 * (P(i - 1, j + 1, k) - P(i + 1, j + 1, k)) +
+                u1 * v1 * w0 * (P(i, j + 1, k) - P(i + 2, j + 1, k)) +
+                u0 * v0 * w1 * (P(i - 1, j, k + 1) - P(i + 1, j, k + 1)) +
+                u1 * v0 * w1 * (P(i, j, k + 1) - P(i + 2, j, k + 1)) +
+                u0 * v1 * w1 * (P(i - 1, j + 1, k + 1) - P(i + 1, j + 1, k + 1)) +
+                u1 * v1 * w1 * (P(i, j + 1, k + 1) - P(i + 2, j + 1, k + 1)));
+  eyt = tdyi * (u0 * v0 * w0 * (P(i, j - 1, k) - P(i, j + 1, k)) + u1 * v0 * w0 * (P(i + 1, j - 1, k) - P(i + 1, j + 1, k)) +
+                u0 * v1 * w0 * (P(i, j, k) - P(i, j + 2, k)) + u1 * v1 * w0 * (P(i + 1, j, k) - P(i + 1, j + 2, k)) +
+                u0 * v0 * w1 * (P(i, j - 1, k + 1) - P(i, j + 1, k + 1)) +
+                u1 * v0 * w1 * (P(i + 1, j - 1, k + 1) - P(i + 1, j + 1, k + 1)) +
+                u0 * v1 * w1 * (P(i, j, k + 1) - P(i, j + 2, k + 1)) +
+                u1 * v1 * w1 * (P(i + 1, j, k + 1) - P(i + 1, j + 2, k + 1)));
+  ezt = tdzi * (u0 * v0 * w0 * (P(i, j, k - 1) - P(i, j, k + 1)) + u1 * v0 * w0 * (P(i + 1, j, k - 1) - P(i + 1, j, k + 1)) +
+                u0 * v1 * w0 * (P(i, j + 1, k - 1) - P(i, j + 1, k + 1)) +
+                u1 * v1 * w0 * (P(i + 1, j + 1, k - 1) - P(i + 1, j + 1, k + 1)) +
+                u0 * v0 * w1 * (P(i, j, k) - P(i, j, k + 2)) + u1 * v0 * w1 * (P(i + 1, j, k) - P(i + 1, j, k + 2)) +
+                u0 * v1 * w1 * (P(i, j + 1, k) - P(i, j + 1, k + 2)) +
+                u1 * v1 * w1 * (P(i + 1, j + 1, k) - P(i + 1, j + 1, k + 2)));
+}
+
+__global__ void k_fetch_e(const double* __restrict__ phi, GridP g, const double* __restrict__ xp,
+                          const double* __restrict__ yp, const double* __restrict__ zp, double* __restrict__ ex,
+                          double* __restrict__ ey, double* __restrict__ ez, int64_t np) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  double a, b, c;
+  gather_e(phi, g, xp[i], yp[i], zp[i], a, b, c);
+  ex[i] = ex[i] + a;
+  ey[i] = ey[i] + b;
+  ez[i] = ez[i] + c;
+}
+
+struct PushP {
+  double q, m, dt;
+  double zmmin, zmmax;
+  double prwall, prwallx, prwally;
+  const double* czs;
+  const double* cze;
+  const double* cdb;
+  int nzl;
+  double zlmin, dzl;
+};
+
+// padvnc3d fullv + particleboundaries3d for one particle per thread.
+__global__ void __launch_bounds__(256) k_advance(const double* __restrict__ phi, GridP g, PushP P,
+                                                 double* __restrict__ xp, double* __restrict__ yp,
+                                                 double* __restrict__ zp, double* __restrict__ uxp,
+                                                 double* __restrict__ uyp, double* __restrict__ uzp,
+                                                 double* __restrict__ gaminv, int64_t np) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  double gi = gaminv[i];
+  if (gi == 0.) return;
+  double x = xp[i], y = yp[i], z = zp[i], ux = uxp[i], uy = uyp[i], uz = uzp[i];
+  double ex, ey, ez;
+  gather_e(phi, g, x, y, z, ex, ey, ez);
+  // fetche3d zeroes E before the gather (w3d.F:11015): E = 0 + gathered
+  ex = 0. + ex;
+  ey = 0. + ey;
+  ez = 0. + ez;
+  double bx = 0., by = 0., bz = 0.;
+  const double halfdt = 0.5 * P.dt, dtl = -halfdt, dtr = halfdt;
+  if (P.czs) {
+    // applyquad (top_lattice.F:2985-3120), one overlap level
+    const double vz = uz * gi;
+    const double a = vz * (dtr - dtl);
+    const double dzi = fabs(1. / copysign(fabs(a) + 1.0e-36, a));
+    int iz = (int)fmax(0., (z - P.zlmin) * (1. / P.dzl) + 0.5);
+    if (iz > P.nzl) iz = P.nzl;
+    const double zs = __ldg(P.czs + iz), ze = __ldg(P.cze + iz);
+    const double z1 = z + vz * dtl, z2 = z + vz * dtr;
+    const double zl = fmin(z1, z2);
+    const double fl = (zl >= zs && zl < ze) ? 1. : 0.;
+    const double zr = fmax(z1, z2);
+    const double fr = (zr >= zs && zr < ze) ? 1. : 0.;
+    double frac = fl;
+    if (fl > fr) frac = (ze - zl) * dzi;
+    if (fr > fl) frac = (zr - zs) * dzi;
+    if (frac > 0.) {
+      const double db = __ldg(P.cdb + iz);
+      bx = bx + db * frac * y;
+      by = by + db * frac * x;
+    }
+  }
+  // epush3d (half step), bpush3d (ibpush = 1), epush3d (half step)
+  const double cst = P.q * halfdt / P.m;
+  ux = ux + ex * cst;
+  uy = uy + ey * cst;
+  uz = uz + ez * cst;
+  const double cb = P.q * P.dt * 0.5 / P.m;
+  const double tx = gi * bx * cb, ty = gi * by * cb, tz = gi * bz * cb;
+  const double tsqi = 2. / (1. + tx * tx + ty * ty + tz * tz);
+  const double sx = tx * tsqi, sy = ty * tsqi, sz = tz * tsqi;
+  const double uxppr = ux + uy * tz - uz * ty;
+  const double uyppr = uy + uz * tx - ux * tz;
+  const double uzppr = uz + ux * ty - uy * tx;
+  ux = ux + uyppr * sz - uzppr * sy;
+  uy = uy + uzppr * sx - uxppr * sz;
+  uz = uz + uxppr * sy - uyppr * sx;
+  ux = ux + ex * cst;
+  uy = uy + ey * cst;
+  uz = uz + ez * cst;
+  // xpush3d
+  x = x + ux * gi * P.dt;
+  y = y + uy * gi * P.dt;
+  z = z + uz * gi * P.dt;
+  // periz (top.F:4015-4035)
+  const double syslen = P.zmmax - P.zmmin, sysleni = 1. / syslen;
+  if (z < P.zmmin) z = z + syslen * (int)((P.zmmax - z) * sysleni);
+  if (z > P.zmmax) z = z - syslen * (int)((z - P.zmmin) * sysleni);
+  // stckxy3d round aperture
+  const double rx = x - P.prwallx, ry = y - P.prwally;
+  if (rx * rx + ry * ry >= P.prwall * P.prwall) gaminv[i] = 0.;
+  xp[i] = x;
+  yp[i] = y;
+  zp[i] = z;
+  uxp[i] = ux;
+  uyp[i] = uy;
+  uzp[i] = uz;
+}
+
+constexpr int kMomN = 11;
+
+// Per-block partial sums of the moments of live particles (getzmmnt,
+// top.F:690-721 with x' = ux/(uz+SMALLPOS)); fixed reduction tree per block.
+__global__ void k_moments(const double* __restrict__ xp, const double* __restrict__ yp,
+                          const double* __restrict__ uxp, const double* __restrict__ uyp,
+                          const double* __restrict__ uzp, const double* __restrict__ gaminv, int64_t np,
+                          double* __restrict__ part) {
+  __shared__ double sm[kMomN][256];
+  double s[kMomN];
+#pragma unroll
+  for (int k = 0; k < kMomN; ++k) s[k] = 0.;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+    if (gaminv[i] == 0.) continue;
+    const double vzi = 1. / (uzp[i] + 1.0e-36);
+    const double x = xp[i], y = yp[i], xpr = uxp[i] * vzi, ypr = uyp[i] * vzi;
+    s[0] += 1.;
+    s[1] += x;
+    s[2] += y;
+    s[3] += xpr;
+    s[4] += ypr;
+    s[5] += x * x;
+    s[6] += y * y;
+    s[7] += xpr * xpr;
+    s[8] += ypr * ypr;
+    s[9] += x * xpr;
+    s[10] += y * ypr;
+  }
+#pragma unroll
+  for (int k = 0; k < kMomN; ++k) sm[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int k = 0; k < kMomN; ++k) sm[k][threadIdx.x] += sm[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kMomN; ++k) part[(size_t)blockIdx.x * kMomN + k] = sm[k][0];
+}
+
+__global__ void k_moments_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s[kMomN];
+  for (int k = 0; k < kMomN; ++k) s[k] = 0.;
+  for (int b = 0; b < nb; ++b)
+    for (int k = 0; k < kMomN; ++k) s[k] += part[(size_t)b * kMomN + k];
+  const double n = s[0] > 0. ? s[0] : 1.;
+  const double xb = s[1] / n, yb = s[2] / n, xpb = s[3] / n, ypb = s[4] / n;
+  const double dxsq = s[5] / n - xb * xb, dysq = s[6] / n - yb * yb;
+  const double dxpsq = s[7] / n - xpb * xpb, dypsq = s[8] / n - ypb * ypb;
+  const double dxxp = s[9] / n - xb * xpb, dyyp = s[10] / n - yb * ypb;
+  out[0] = s[0];
+  out[1] = xb;
+  out[2] = yb;
+  out[3] = sqrt(fmax(0., dxsq));
+  out[4] = sqrt(fmax(0., dysq));
+  out[5] = 4. * sqrt(fmax(0., dxsq * dxpsq - dxxp * dxxp));
+  out[6] = 4. * sqrt(fmax(0., dysq * dypsq - dyyp * dyyp));
+  out[7] = 0.;
+}
+
+inline unsigned cdiv64(int64_t a, unsigned b) { return (unsigned)((a + b - 1) / b); }
+
+GridP gridp(const wg_ctx* c) {
+  return GridP{c->grid.nx, c->grid.ny, c->grid.nz, c->dx, c->dy, c->dz, c->grid.xmmin, c->grid.ymmin,
+               c->grid.zmmin, 0.};
+}
+
+}  // namespace
+
+int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
+  if (!p || (p->np > 0 && (!p->x || !p->y || !p->z || !p->gaminv)) || p->np < 0) {
+    set_error("wg_deposit: null particle arrays");
+    return WG_EINVAL;
+  }
+  Level& L0 = c->lv[0];
+  cudaStream_t s = c->stream;
+  WG_TRY_CUDA(cudaMemsetAsync(c->racc, 0, L0.nr * sizeof(unsigned long long), s));
+  WG_TRY_CUDA(cudaMemsetAsync(c->dred + 3, 0, sizeof(unsigned long long), s));
+  GridP g = gridp(c);
+  if (p->np > 0) {
+    const int64_t maxblocks = 2147483647LL;
+    if (cdiv64(p->np, 256) > maxblocks) { set_error("wg_deposit: too many particles"); return WG_ETOOLARGE; }
+    { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<<<cdiv64(p->np, 256), 256, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, c->racc); c->prof_end(pe); }
+  }
+  double gg = p->w * p->q;
+  gg = gg / c->dx;
+  gg = gg / c->dy;
+  gg = gg / c->dz;
+  { ++c->nlaunch; k_fix_to_rho<<<cdiv64((int64_t)L0.nr, 256), 256, 0, s>>>(c->racc, c->rho, L0.nr, gg * kFixInv, zero_first ? 0 : 1,
+                                                           c->dred + 3); }
+  WG_TRY_CUDA(cudaGetLastError());
+  WG_TRY_CUDA(cudaMemcpyAsync(c->hred + 3, c->dred + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  WG_TRY_CUDA(cudaStreamSynchronize(s));
+  if (c->hred[3]) {
+    set_error("wg_deposit: fixed-point charge accumulator above 2^62 at some node (more than 65536 full "
+              "particle weights on one node)");
+    return WG_EOVERFLOW;
+  }
+  return WG_OK;
+}
+
+int finalize_rho(wg_ctx* c) {
+  const wg_grid& G = c->grid;
+  cudaStream_t s = c->stream;
+  const int* b = G.bounds;
+  size_t nyz = (size_t)(G.ny + 1) * (G.nz + 1), nxz = (size_t)(G.nx + 1) * (G.nz + 1),
+         nxy = (size_t)(G.nx + 1) * (G.ny + 1);
+  if (b[0] >= 1 || b[1] >= 1) { ++c->nlaunch; k_rhobc<<<cdiv64((int64_t)nyz, 256), 256, 0, s>>>(c->rho, G.nx, G.ny, G.nz, 0, b[0], b[1]); }
+  if (b[2] >= 1 || b[3] >= 1) { ++c->nlaunch; k_rhobc<<<cdiv64((int64_t)nxz, 256), 256, 0, s>>>(c->rho, G.nx, G.ny, G.nz, 1, b[2], b[3]); }
+  if (b[4] >= 1 || b[5] >= 1) { ++c->nlaunch; k_rhobc<<<cdiv64((int64_t)nxy, 256), 256, 0, s>>>(c->rho, G.nx, G.ny, G.nz, 2, b[4], b[5]); }
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
+int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double* ex, double* ey, double* ez,
+            int64_t np) {
+  if (np < 0 || (np > 0 && (!x || !y || !z || !ex || !ey || !ez))) {
+    set_error("wg_fetch_e: null arrays");
+    return WG_EINVAL;
+  }
+  if (np == 0) return WG_OK;
+  { ++c->nlaunch; k_fetch_e<<<cdiv64(np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), x, y, z, ex, ey, ez, np); }
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
+int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
+  if (!p || !prm || p->np < 0 ||
+      (p->np > 0 && (!p->x || !p->y || !p->z || !p->ux || !p->uy || !p->uz || !p->gaminv))) {
+    set_error("wg_advance: null arguments");
+    return WG_EINVAL;
+  }
+  if (prm->use_lattice && c->nzl < 0) {
+    set_error("wg_advance: use_lattice set but no lattice installed (wg_set_lattice)");
+    return WG_ESTATE;
+  }
+  if (p->np == 0) return WG_OK;
+  PushP P{p->q, p->m, prm->dt, c->grid.zmmin, c->grid.zmmax, prm->prwall, prm->prwallx, prm->prwally,
+          prm->use_lattice ? c->czs : nullptr, c->cze, c->cdb, c->nzl, c->zlmin, c->dzl};
+  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); k_advance<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, p->x, p->y, p->z, p->ux, p->uy,
+                                                       p->uz, p->gaminv, p->np); c->prof_end(pe); }
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
+int moments(wg_ctx* c, const wg_particles* p, double* out) {
+  if (!p || !out || p->np < 0) { set_error("wg_moments: null arguments"); return WG_EINVAL; }
+  cudaStream_t s = c->stream;
+  const int nb = c->mom_blocks;
+  { ++c->nlaunch; k_moments<<<nb, 256, 0, s>>>(p->x, p->y, p->ux, p->uy, p->uz, p->gaminv, p->np, c->dmom); }
+  { ++c->nlaunch; k_moments_final<<<1, 32, 0, s>>>(c->dmom, nb, c->dmom + (size_t)nb * kMomN); }
+  WG_TRY_CUDA(cudaGetLastError());
+  WG_TRY_CUDA(cudaMemcpyAsync(out, c->dmom + (size_t)nb * kMomN, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  WG_TRY_CUDA(cudaStreamSynchronize(s));
+  return WG_OK;
+}
+
+int moments_scratch_doubles(int nb) { return nb * kMomN + 8; }
+
+}  // namespace wg

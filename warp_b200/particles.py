@@ -1,0 +1,85 @@
+"""Device-resident particle group (the role of top.pgroup) and the seeded
+semi-Gaussian beam loader used for the synthetic workloads.
+
+Arrays are float64 torch tensors on the CUDA device (SoA: x, y, z, ux, uy,
+uz, gaminv, ex, ey, ez). A lost particle has gaminv == 0, the stckxy3d
+convention (pywarp90/w3d.F:11520-11535); lost particles are skipped by the
+deposit, push and moments kernels.
+"""
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .constants import clight, echarge, proton_mass
+
+FIELDS = ("x", "y", "z", "ux", "uy", "uz", "gaminv")
+
+
+class ParticleGroup:
+    def __init__(self, arrays, q=echarge, m=proton_mass, w=1.0, device="cuda", with_fields=True):
+        """arrays: dict of equal-length 1-D arrays (numpy or torch) for FIELDS."""
+        self.q, self.m, self.w = float(q), float(m), float(w)
+        self.device = torch.device(device)
+        n = len(arrays["x"])
+        for f in FIELDS:
+            a = arrays[f]
+            t = torch.as_tensor(a, dtype=torch.float64).to(self.device).contiguous()
+            if t.shape != (n,):
+                raise ValueError("particle array %s has shape %s, expected (%d,)" % (f, tuple(t.shape), n))
+            setattr(self, f, t)
+        if with_fields:
+            self.ex = torch.zeros(n, dtype=torch.float64, device=self.device)
+            self.ey = torch.zeros_like(self.ex)
+            self.ez = torch.zeros_like(self.ex)
+        self._struct = None
+
+    @property
+    def np(self):
+        return int(self.x.shape[0])
+
+    def cstruct(self):
+        s = _lib.Particles()
+        for f in FIELDS:
+            setattr(s, f, getattr(self, f).data_ptr())
+        s.np = self.np
+        s.q, s.m, s.w = self.q, self.m, self.w
+        return s
+
+    def to_numpy(self):
+        return {f: getattr(self, f).cpu().numpy() for f in FIELDS}
+
+    def nlive(self):
+        return int((self.gaminv != 0).sum().item())
+
+
+def semigaussian(n, seed=0, radius=2e-3, mismatch=0.0, angle_rms=5e-3, zmin=0.0, zmax=1.0, ekin_ev=1e6,
+                 mass=proton_mass, xcent=0.0, ycent=0.0):
+    """Seeded semi-Gaussian beam: uniform in an ellipse with semi-axes
+    radius*(1+mismatch) (x) and radius*(1-mismatch) (y), Gaussian transverse
+    angles of rms `angle_rms` (x' = ux/uz), uniform in z. Non-relativistic
+    push (lrelativ = false): gaminv = 1, uz = beta*c. Returns numpy arrays.
+    Philox counter-based generator, so the stream is reproducible."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    gamma = 1. + ekin_ev * echarge / (mass * clight * clight)
+    beta = math.sqrt(1. - 1. / (gamma * gamma))
+    vz = beta * clight
+    r = np.sqrt(rng.random(n))
+    th = 2. * np.pi * rng.random(n)
+    ax, ay = radius * (1. + mismatch), radius * (1. - mismatch)
+    x = xcent + ax * r * np.cos(th)
+    y = ycent + ay * r * np.sin(th)
+    z = zmin + (zmax - zmin) * rng.random(n)
+    xp = angle_rms * rng.standard_normal(n)
+    yp = angle_rms * rng.standard_normal(n)
+    uz = np.full(n, vz)
+    return {"x": x, "y": y, "z": z, "ux": xp * vz, "uy": yp * vz, "uz": uz, "gaminv": np.ones(n)}
+
+
+def beam_weight(current, length, n, ekin_ev=1e6, mass=proton_mass, charge=echarge):
+    """Real particles per macroparticle for a beam of `current` (A) filling
+    `length` (m): w = I L / (q v N)."""
+    gamma = 1. + ekin_ev * echarge / (mass * clight * clight)
+    v = math.sqrt(1. - 1. / (gamma * gamma)) * clight
+    return current * length / (charge * v * n)

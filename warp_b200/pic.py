@@ -1,0 +1,107 @@
+"""3D electrostatic PIC run on one B200: the step of w3dexe/step3d
+(pywarp90/w3d.F:511-986) with the field solve delegated to a registered
+MultiGridB200.
+
+Order inside one step (step3d): particle advance with the field of the
+previous solve (padvnc3d fullv: gather, quads, leapfrog/Boris, drift),
+particle boundaries (periodic z, absorbing pipe), charge deposition
+(loadrho), field solve. Loaded velocities are taken as time-centred at
+t - dt/2, so every step is a fullv step.
+
+Workloads (synthetic, seeded):
+  WORKLOADS["A"]: 32x32x64 cells over 8 cm x 8 cm x 1 m, 2e5 protons at
+      1 MeV, semi-Gaussian (2 mm radius, 5 mrad rms angle, 10 mA), FODO of
+      hard-edge quads 10 cm long at +-15 T/m with 50 cm period, grounded pipe
+      of radius 3.5 cm, periodic z, 50 steps.
+  WORKLOADS["B"]: the same physics on 256x256x512 cells with 5e7 particles,
+      4 mm radius with 20% envelope mismatch, 1000 steps.
+  WORKLOADS["E"]: 256x256x1024 cells, 2e8 particles, plus four
+      electrostatic quadrupole rods (radius 1 cm, +-20 kV) inside the pipe.
+"""
+import math
+import time
+
+import torch
+
+from . import conductors as cond
+from .constants import clight, echarge, proton_mass
+from .fieldsolver import registersolver
+from .lattice import fodo
+from .multigrid import MultiGridB200
+from .particles import ParticleGroup, beam_weight, semigaussian
+
+WORKLOADS = {
+    "A": dict(nx=32, ny=32, nz=64, npart=200_000, radius=2e-3, mismatch=0.0, nsteps=50, rods=False),
+    "B": dict(nx=256, ny=256, nz=512, npart=50_000_000, radius=4e-3, mismatch=0.2, nsteps=1000, rods=False),
+    "E": dict(nx=256, ny=256, nz=1024, npart=200_000_000, radius=4e-3, mismatch=0.2, nsteps=1000, rods=True),
+}
+
+COMMON = dict(xmmin=-0.04, xmmax=0.04, ymmin=-0.04, ymmax=0.04, zmmin=0.0, zmmax=1.0, ekin_ev=1.0e6,
+              angle_rms=5e-3, current=10e-3, quad_gradient=15.0, quad_length=0.10, period=0.50,
+              pipe_radius=0.035, rod_radius=0.01, rod_voltage=20e3, rod_center=0.0225, seed=0,
+              steps_per_period=50)
+
+
+def workload(name, **over):
+    cfg = dict(COMMON)
+    cfg.update(WORKLOADS[name])
+    cfg.update(over)
+    cfg["name"] = name
+    return cfg
+
+
+def beam_velocity(cfg):
+    gamma = 1. + cfg["ekin_ev"] * echarge / (proton_mass * clight * clight)
+    return math.sqrt(1. - 1. / (gamma * gamma)) * clight
+
+
+def timestep(cfg):
+    return (cfg["period"] / cfg["steps_per_period"]) / beam_velocity(cfg)
+
+
+class ESPIC:
+    """Sets up solver, conductors, lattice and beam of a workload."""
+
+    def __init__(self, cfg, precision="fp64", tolkind="mgerror", mgtol=1.e-6, mgmaxiters=100, device="cuda",
+                 particles=None):
+        self.cfg = cfg
+        c = cfg
+        self.solver = MultiGridB200(c["nx"], c["ny"], c["nz"], c["xmmin"], c["xmmax"], c["ymmin"], c["ymmax"],
+                                    c["zmmin"], c["zmmax"], bounds=(0, 0, 0, 0, 2, 2), precision=precision,
+                                    tolkind=tolkind, mgtol=mgtol, mgmaxiters=mgmaxiters, mgverbose=-1,
+                                    device=device)
+        registersolver(self.solver)
+        zc = 0.5 * (c["zmmin"] + c["zmmax"])
+        self.solver.installconductor(cond.ZCylinderOut(radius=c["pipe_radius"], length=100.0, zcent=zc))
+        if c.get("rods"):
+            d = c["rod_center"]
+            for (x, y, v) in ((d, 0., c["rod_voltage"]), (-d, 0., c["rod_voltage"]),
+                              (0., d, -c["rod_voltage"]), (0., -d, -c["rod_voltage"])):
+                self.solver.installconductor(cond.ZCylinder(radius=c["rod_radius"], length=100.0, voltage=v,
+                                                            xcent=x, ycent=y, zcent=zc))
+        self.lattice = fodo(c["quad_gradient"], c["quad_length"], c["period"])
+        self.solver.setlattice(self.lattice)
+        self.dt = timestep(c)
+        if particles is None:
+            particles = semigaussian(c["npart"], seed=c["seed"], radius=c["radius"], mismatch=c["mismatch"],
+                                     angle_rms=c["angle_rms"], zmin=c["zmmin"], zmax=c["zmmax"],
+                                     ekin_ev=c["ekin_ev"])
+        w = beam_weight(c["current"], c["zmmax"] - c["zmmin"], c["npart"], ekin_ev=c["ekin_ev"])
+        self.pgroup = ParticleGroup(particles, q=echarge, m=proton_mass, w=w, device=device)
+        self.solver.addpgroup(self.pgroup)
+        self.it = 0
+
+    def generate(self):
+        """Initial deposit and field solve (w3dgen -> step3d("w3dgen"))."""
+        self.solver.loadrho()
+        self.solver.solve()
+
+    def step(self, n=1):
+        for _ in range(n):
+            self.solver.advance(self.pgroup, self.dt, prwall=self.cfg["pipe_radius"])
+            self.solver.loadrho()
+            self.solver.solve()
+            self.it += 1
+
+    def moments(self):
+        return self.solver.moments(self.pgroup)
