@@ -1057,9 +1057,9 @@ int or_mgsolve(int nx, int ny, int nz, double dx, double dy, double dz, const in
   return 0;
 }
 
-// Relative residual of the discrete Poisson problem with conductors,
-// max|rhs - A phi| / max|rhs| over the nodes the solver updates, evaluated
-// with the level-0 residual operator (scaled units cancel in the ratio).
+// Relative residual max|res| / max|rhs| over the nodes 0..n, where res is
+// the reference's own level-0 residual (getresidual) and rhs = rho*reps0c;
+// both carry the same scale factor, which cancels in the ratio.
 double or_relresidual(int nx, int ny, int nz, double dx, double dy, double dz, const int* bounds,
                       const double* phi, const double* rho, or_conductors* cond, double mgparam) {
   Conductors empty;
@@ -1078,7 +1078,10 @@ double or_relresidual(int nx, int ny, int nz, double dx, double dy, double dz, c
   std::vector<double> rhs(nr), res((size_t)(nx + 3) * (ny + 3) * (nz + 3));
   std::vector<double> ph(phi, phi + res.size());
   for (size_t i = 0; i < nr; ++i) rhs[i] = rho[i] * reps0c;
-  residual3d(nx, ny, nz, dxsqi, dysqi, dzsqi, ph.data(), rhs.data(), res.data(), 0, bounds, P, true, *C);
+  // residual of MultiGrid3D.getresidual (scripts/multigrid.py:940-950):
+  // level-0 residual3d with mgform = 1, so rows next to conductors carry
+  // the ppp = min(dels) scaling of condbndyres
+  residual3d(nx, ny, nz, dxsqi, dysqi, dzsqi, ph.data(), rhs.data(), res.data(), 0, bounds, P, false, *C);
   double rmax = 0., bmax = 0.;
   for (int iz = 0; iz <= nz; ++iz)
     for (int iy = 0; iy <= ny; ++iy)

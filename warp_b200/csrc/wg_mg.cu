@@ -376,11 +376,16 @@ __global__ void k_special_res(const T* __restrict__ phi, const T* __restrict__ r
       handlesubgrid2<T>(2, 3, pym, pyp, dysqic, d, v, voltfac, denom, ppp);
       handlesubgrid2<T>(4, 5, pzm, pzp, dzsqic, d, v, voltfac, denom, ppp);
       if (ppp < (T)1.) {
+        // the reported max always uses the ppp-scaled row (getresidual,
+        // scripts/multigrid.py:940); the stored value drops the scaling for
+        // the residual-correction set-up
+        const T pppmax = ppp;
         if (mgform2init) ppp = (T)1.;
-        T r = ppp * (rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqics + (pym + pyp) * dysqics +
-                     (pzm + pzp) * dzsqics - phi[p] * mgparam * denom);
+        const T inner = rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqics + (pym + pyp) * dysqics +
+                        (pzm + pzp) * dzsqics - phi[p] * mgparam * denom;
+        T r = ppp * inner;
         store(ix, iy, iz, r);
-        m = fabs((double)r);
+        m = fabs((double)(pppmax * inner));
         if (0. >= d[0] && d[0] >= -1.) store(ix - 1, iy, iz, (T)0.);
         if (0. >= d[1] && d[1] >= -1.) store(ix + 1, iy, iz, (T)0.);
         if (0. >= d[2] && d[2] >= -1.) store(ix, iy - 1, iz, (T)0.);
@@ -714,7 +719,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
     for (;;) {
       if (o->tolkind == 1) {
         WG_TRY_CUDA(cudaMemsetAsync(red + 1, 0, sizeof(unsigned long long), s));
-        S.residual<double, 1, double>(0, L0.phi, L0.rhs, nullptr, true, true, red + 1);
+        S.residual<double, 1, double>(0, L0.phi, L0.rhs, nullptr, false, true, red + 1);
         WG_TRY(S.fetch_red(rv, 3));
         relres = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
         if (relres <= o->mgtol) { conv = true; break; }
@@ -784,7 +789,7 @@ int relresidual(wg_ctx* c, double mgparam, double* out) {
   WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
   if (L0.n_int)
     { ++c->nlaunch; k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1); }
-  S.residual<double, 1, double>(0, c->phisave, L0.rhs, nullptr, true, true, c->dred + 1);
+  S.residual<double, 1, double>(0, c->phisave, L0.rhs, nullptr, false, true, c->dred + 1);
   double rv[4];
   WG_TRY(S.fetch_red(rv, 3));
   *out = rv[2] > 0. ? rv[1] / rv[2] : rv[1];

@@ -56,6 +56,8 @@ class MultiGridB200(FieldSolver):
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise ValueError("MultiGridB200 runs on a CUDA device only")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         torch.cuda.set_device(self.device)
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.xmmin, self.xmmax = float(xmmin), float(xmmax)

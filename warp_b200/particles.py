@@ -22,6 +22,8 @@ class ParticleGroup:
         """arrays: dict of equal-length 1-D arrays (numpy or torch) for FIELDS."""
         self.q, self.m, self.w = float(q), float(m), float(w)
         self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         n = len(arrays["x"])
         for f in FIELDS:
             a = arrays[f]
