@@ -155,6 +155,15 @@ int wg_advance(wg_ctx* ctx, const wg_particles* p, const wg_push_params* prm);
  * deterministic order. */
 int wg_moments(wg_ctx* ctx, const wg_particles* p, double* out);
 
+/* Cell keys for sorting particles by cell, as particlesortxyzwithcopy
+ * (top.F:5095-5130): key = ix + (nx+1)*(iy + (ny+1)*iz); lost particles get
+ * (nx+1)(ny+1)(nz+1). keys: device int64 array of length np. */
+int wg_particle_keys(wg_ctx* ctx, const wg_particles* p, int64_t* keys);
+/* Gathers dst[i] = src[perm[i]] for the 7 particle arrays (device perm of
+ * length np; src and dst must not overlap). With perm from a stable sort of
+ * the keys this is particlesortbyindex (top.F:5132). */
+int wg_particle_permute(wg_ctx* ctx, const int64_t* perm, const wg_particles* src, const wg_particles* dst);
+
 /* ---- instrumentation (no reference counterpart: replaces the wall-clock
  * sub-timers lf3dtimesubs / lw3dtimesubs, f3d.v:1308, w3d.v:1396) -------- */
 

@@ -77,3 +77,35 @@ def test_pic_rho_bit_reproducible():
     b.step(3)
     assert np.array_equal(a.solver.rho.cpu().numpy(), b.solver.rho.cpu().numpy())
     assert np.array_equal(a.solver.phi.cpu().numpy(), b.solver.phi.cpu().numpy())
+
+
+def test_pic_sorted_run_equals_unsorted():
+    """Sorting particles by cell (and dropping lost ones) changes neither rho
+    nor phi nor the set of particle states."""
+    from warp_b200 import pic
+    cfg = pic.workload("A", npart=100_000, quad_gradient=40.0)
+    a = pic.ESPIC(cfg)
+    a.generate()
+    a.step(6)
+    b = pic.ESPIC(cfg, sort_interval=2)
+    b.generate()
+    b.step(6)
+    assert np.array_equal(a.solver.rho.cpu().numpy(), b.solver.rho.cpu().numpy())
+    assert np.array_equal(a.solver.phi.cpu().numpy(), b.solver.phi.cpu().numpy())
+    pa, pb = a.pgroup.to_numpy(), b.pgroup.to_numpy()
+    live = pa["gaminv"] != 0
+    assert b.pgroup.np <= a.pgroup.np
+    ka = np.lexsort([pa[k][live] for k in ("uz", "uy", "ux", "z", "y", "x")])
+    kb = np.lexsort([pb[k][pb["gaminv"] != 0] for k in ("uz", "uy", "ux", "z", "y", "x")])
+    for k in ("x", "y", "z", "ux", "uy", "uz"):
+        assert np.array_equal(pa[k][live][ka], pb[k][pb["gaminv"] != 0][kb]), k
+    # keys are non-decreasing right after a sort
+    b.pgroup.sort(b.solver)
+    import ctypes
+    import torch
+    from warp_b200 import _lib
+    keys = torch.empty(b.pgroup.np, dtype=torch.int64, device=b.pgroup.device)
+    s = b.pgroup.cstruct()
+    _lib.check(_lib.lib.wg_particle_keys(b.solver._h, ctypes.byref(s), ctypes.c_void_p(keys.data_ptr())))
+    k = keys.cpu().numpy()
+    assert np.all(np.diff(k) >= 0)

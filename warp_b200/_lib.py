@@ -81,6 +81,8 @@ SIGNATURES = {
     "wg_prof_enable": [_vp, _c.c_int],
     "wg_prof_read": [_vp, _c.c_int, _dp, _i64p, _dp],
     "wg_launch_count": [_vp, _i64p],
+    "wg_particle_keys": [_vp, ctypes.POINTER(Particles), _vp],
+    "wg_particle_permute": [_vp, _vp, ctypes.POINTER(Particles), ctypes.POINTER(Particles)],
 }
 
 PROF_SOR0, PROF_DEPOSIT, PROF_ADVANCE, PROF_RESID0 = 0, 1, 2, 3

@@ -24,6 +24,7 @@ int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double
 int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm);
 int moments(wg_ctx* c, const wg_particles* p, double* out);
 int moments_scratch_doubles(int nb);
+int configure_kernels();
 
 // getnextcoarselevel3d / getmglevels (f3d_mgrid.F:3601-3845), serial,
 // mgcoarsening = 2.
@@ -81,11 +82,10 @@ void free_conductor_data(wg_ctx* c) {
       dfree(S.ijk);
       dfree(S.dels);
       dfree(S.volt);
-      dfree(S.prev);
-      dfree(S.prevf);
+      dfree(S.rhs);
+      dfree(S.rhsf);
       S.n = 0;
     }
-    dfree(L.mask);
     L.has_neumann_sub = false;
   }
 }
@@ -96,9 +96,11 @@ void free_all(wg_ctx* c) {
   c->prof_ev.clear();
   for (Level& L : c->lv) {
     dfree(L.phi);
+    dfree(L.phi2);
     dfree(L.rhs);
     dfree(L.res);
     dfree(L.phif);
+    dfree(L.phif2);
     dfree(L.rhsf);
     dfree(L.resf);
   }
@@ -141,26 +143,13 @@ int upload_conductors(wg_ctx* c) {
       WG_TRY(upload(&S.ijk, idx.data() + 3 * (size_t)s0, 3 * (size_t)S.n));
       WG_TRY(upload(&S.dels, dl.data() + 6 * (size_t)s0, 6 * (size_t)S.n));
       WG_TRY(upload(&S.volt, vl.data() + 6 * (size_t)s0, 6 * (size_t)S.n));
-      WG_TRY(dalloc(&S.prev, (size_t)S.n));
-      if (c->have_fp32) WG_TRY(dalloc(&S.prevf, (size_t)S.n));
+      WG_TRY(dalloc(&S.rhs, (size_t)S.n));
+      if (c->have_fp32) WG_TRY(dalloc(&S.rhsf, (size_t)S.n));
       for (int i = s0; i < s1; ++i)
         for (int k = 0; k < 6; ++k) {
           double d = dl[6 * (size_t)i + k];
           if (0. >= d && d > -1.) L.has_neumann_sub = true;
         }
-    }
-    if (l == 0) {
-      // 1 bit per node marking conductor nodes, for the residual max
-      const LevelDims& d = L.d;
-      std::vector<uint32_t> m((L.nr + 31) / 32, 0u);
-      auto mark = [&](const int32_t* p) {
-        size_t r = (size_t)p[0] + (size_t)(d.nx + 1) * ((size_t)p[1] + (size_t)(d.ny + 1) * (size_t)p[2]);
-        m[r >> 5] |= 1u << (r & 31);
-      };
-      for (int i = a; i < b; ++i) mark(&C.int_indx[3 * (size_t)i]);
-      for (int i = C.istart_even[0]; i < C.istart_even[1]; ++i) mark(&C.even_indx[3 * (size_t)i]);
-      for (int i = C.istart_odd[0]; i < C.istart_odd[1]; ++i) mark(&C.odd_indx[3 * (size_t)i]);
-      WG_TRY(upload(&L.mask, m.data(), m.size()));
     }
   }
   return WG_OK;
@@ -174,10 +163,11 @@ int ensure_fp32_impl(wg_ctx* c) {
   if (c->have_fp32) return WG_OK;
   for (Level& L : c->lv) {
     WG_TRY(dalloc(&L.phif, L.np));
+    WG_TRY(dalloc(&L.phif2, L.np));
     WG_TRY(dalloc(&L.rhsf, L.nr));
     WG_TRY(dalloc(&L.resf, L.np));
     for (DevSubgrid& S : L.sub)
-      if (S.n && !S.prevf) WG_TRY(dalloc(&S.prevf, (size_t)S.n));
+      if (S.n && !S.rhsf) WG_TRY(dalloc(&S.rhsf, (size_t)S.n));
   }
   c->have_fp32 = true;
   return WG_OK;
@@ -226,6 +216,7 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
     L.np = (size_t)(L.d.nx + 3) * (L.d.ny + 3) * (L.d.nz + 3);
     L.nr = (size_t)(L.d.nx + 1) * (L.d.ny + 1) * (L.d.nz + 1);
     rc = dalloc(&L.phi, L.np);
+    if (rc == WG_OK) rc = dalloc(&L.phi2, L.np);
     if (rc == WG_OK) rc = dalloc(&L.rhs, L.nr);
     if (rc == WG_OK && l + 1 < dims.size()) rc = dalloc(&L.res, L.np);
   }
@@ -244,6 +235,7 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
     set_error("wg_create: cudaMallocHost failed");
     rc = WG_ENOMEM;
   }
+  if (rc == WG_OK) rc = configure_kernels();
   if (rc == WG_OK) {
     // empty conductor set so the solver can run without installconductor
     rc = finalize_conductors(c->cond, dims);
@@ -469,6 +461,25 @@ int wg_launch_count(wg_ctx* c, int64_t* n) {
   if (!c || !n) { set_error("null argument"); return WG_EINVAL; }
   *n = c->nlaunch;
   return WG_OK;
+}
+
+}  // extern "C"
+
+namespace wg {
+int cell_keys(wg_ctx* c, const wg_particles* p, int64_t* keys);
+int permute(wg_ctx* c, const int64_t* perm, const wg_particles* src, const wg_particles* dst);
+}  // namespace wg
+
+extern "C" {
+
+int wg_particle_keys(wg_ctx* c, const wg_particles* p, int64_t* keys) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return cell_keys(c, p, keys);
+}
+
+int wg_particle_permute(wg_ctx* c, const int64_t* perm, const wg_particles* src, const wg_particles* dst) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return permute(c, perm, src, dst);
 }
 
 }  // extern "C"

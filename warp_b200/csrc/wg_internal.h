@@ -51,13 +51,16 @@ struct LevelDims {
 };
 
 // Device conductor data of one level (one parity for subgrid lists).
+// The rhs arrays of a level hold, at every conductor node, a NaN whose
+// payload is the node's index in its list (sign bit set for interior
+// points); the node's real rhs value is kept here in `rhs`/`rhsf`.
 struct DevSubgrid {
   int n = 0;
   int32_t* ijk = nullptr;   // 3 per point
   double* dels = nullptr;   // 6 per point
   double* volt = nullptr;   // 6 per point
-  double* prev = nullptr;   // prevphi (FP64 V-cycles)
-  float* prevf = nullptr;   // prevphi (FP32 V-cycles)
+  double* rhs = nullptr;    // rhs value at the point (FP64 levels)
+  float* rhsf = nullptr;    // rhs value at the point (FP32 levels)
 };
 
 struct Level {
@@ -65,16 +68,17 @@ struct Level {
   size_t np = 0;  // (nx+3)(ny+3)(nz+3)
   size_t nr = 0;  // (nx+1)(ny+1)(nz+1)
   double* phi = nullptr;
+  double* phi2 = nullptr;  // second buffer of the out-of-place fused sweep
   double* rhs = nullptr;
   double* res = nullptr;
   float* phif = nullptr;
+  float* phif2 = nullptr;
   float* rhsf = nullptr;
   float* resf = nullptr;
   int n_int = 0;
   int32_t* int_ijk = nullptr;
   double* int_volt = nullptr;
   DevSubgrid sub[2];   // 0 even, 1 odd
-  uint32_t* mask = nullptr;  // 1 bit per node: conductor (interior or subgrid) node
   bool has_neumann_sub = false;
 };
 

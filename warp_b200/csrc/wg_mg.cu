@@ -1,7 +1,7 @@
 // Multigrid Poisson solver with subgrid conductors on one B200.
 //
 // Device kernels for the phases of multigrid3dsolve (pywarp90/f3d_mgrid.F:83-500):
-// red-black SOR half passes, subgrid conductor stencil, residual, restriction,
+// red-black SOR, subgrid conductor stencil, residual, restriction,
 // prolongation and guard-plane boundary conditions, for FP64 and FP32 levels,
 // plus the host-side V-cycle driver. This translation unit is compiled with
 // --fmad=false and evaluates every expression in the reference's operand
@@ -11,6 +11,22 @@
 // Layout: each level keeps phi and res as (nx+3)(ny+3)(nz+3) arrays with one
 // guard cell and rhs as (nx+1)(ny+1)(nz+1), x fastest (the reference's
 // Fortran layout), so the user-visible solver.phi needs no repacking.
+//
+// Conductor nodes are marked inside the rhs arrays: at an interior or
+// subgrid node rhs holds a NaN whose payload is the node's index in its list
+// (sign bit set for interior points) and the real rhs value is kept in the
+// list record. A sweep therefore reads exactly phi and rhs per node and
+// finds the conductor nodes without a separate tag array.
+//
+// Two SOR paths implement sorpass3d:
+//  * the fused sweep (k_sor_fused): both colours of one pass in a single
+//    out-of-place kernel that streams z-planes through shared memory,
+//    updating red on the tile plus a one-cell halo and then black on the
+//    tile, 24 B/node of DRAM traffic in FP64. Used when x and y are
+//    Dirichlet, z is Dirichlet or periodic, and no conductor surface point
+//    is of Neumann type.
+//  * the generic in-place path: one kernel per colour plus the conductor
+//    and boundary kernels, for every other case.
 
 #include <cmath>
 #include <cstdio>
@@ -33,6 +49,33 @@ __host__ __device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
 }
 __host__ __device__ inline size_t rix(int nx, int ny, int ix, int iy, int iz) {
   return (size_t)ix + (size_t)(nx + 1) * ((size_t)iy + (size_t)(ny + 1) * (size_t)iz);
+}
+
+// NaN boxes marking conductor nodes in rhs arrays.
+template <typename T>
+struct Box;
+template <>
+struct Box<double> {
+  static constexpr uint32_t kMax = 0xFFFFFFFFu;
+  __device__ static double make(bool interior, uint32_t idx) {
+    return __longlong_as_double((long long)(0x7FF8000000000000ull | (interior ? 0x8000000000000000ull : 0ull) |
+                                            (unsigned long long)idx));
+  }
+  __device__ static uint32_t idx(double v) { return (uint32_t)((unsigned long long)__double_as_longlong(v)); }
+  __device__ static bool interior(double v) { return __double_as_longlong(v) < 0; }
+};
+template <>
+struct Box<float> {
+  static constexpr uint32_t kMax = 0x3FFFFFu;
+  __device__ static float make(bool interior, uint32_t idx) {
+    return __uint_as_float(0x7FC00000u | (interior ? 0x80000000u : 0u) | (idx & 0x3FFFFFu));
+  }
+  __device__ static uint32_t idx(float v) { return __float_as_uint(v) & 0x3FFFFFu; }
+  __device__ static bool interior(float v) { return __float_as_int(v) < 0; }
+};
+template <typename T>
+__device__ inline bool isbox(T v) {
+  return v != v;
 }
 
 __device__ inline void atomic_max_nonneg(unsigned long long* addr, double v) {
@@ -119,31 +162,6 @@ __global__ void k_bc_z(T* __restrict__ u, int nx, int ny, int nz, Bnd B, int lwi
   }
 }
 
-// ---------------------------------------------------------------------------
-// sorhalfpass3d bulk loop (f3d_mgrid.F:2229-2243): one colour, in place.
-template <typename T>
-__global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny,
-                                                  int ixmin, int ixmax, int iymin, int iymax, int izmin, int parity,
-                                                  T cx, T cy, T cz, T spm1) {
-  const int iz = izmin + blockIdx.z;
-  const int iy = iymin + blockIdx.y * blockDim.y + threadIdx.y;
-  if (iy > iymax) return;
-  const int ix = ixmin + ((ixmin + iy + iz + parity) & 1) + 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (ix > ixmax) return;
-  const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
-  const size_t p = pix(nx, ny, ix, iy, iz);
-  phi[p] = rhs[rix(nx, ny, ix, iy, iz)] + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy +
-           (phi[p - sz] + phi[p + sz]) * cz + spm1 * phi[p];
-}
-
-// Saves phi at the subgrid points of one colour (prevphi, f3d_mgrid.F:2206-2226).
-template <typename T>
-__global__ void k_save_prev(const T* __restrict__ phi, int nx, int ny, const int32_t* __restrict__ ijk, int n,
-                            T* __restrict__ prev) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  prev[i] = phi[pix(nx, ny, ijk[3 * i], ijk[3 * i + 1], ijk[3 * i + 2])];
-}
 
 // handlesubgrid2 (f3d_mgrid.F:2628-2764).
 template <typename T>
@@ -206,22 +224,104 @@ __device__ inline void handlesubgrid2(int im, int ip, T& pm, T& pp, T dsqicos, c
   }
 }
 
+
 struct SorCoef {
   double cx, cy, cz, spm1, mgparam;
 };
 
-// condbndymg (icndbndy = 2, f3d_mgrid.F:2874-2978) for one colour, then
-// cond_potmg (f3d_mgrid.F:2426-2470) for the interior points. The two sets
-// are disjoint and only read the other colour, so one launch does both.
+// Conductor data of one level as kernel arguments.
 template <typename T>
-__global__ void k_special_sor(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny, int nz,
-                              const int32_t* __restrict__ sijk, const double* __restrict__ sdels,
-                              const double* __restrict__ svolt, const T* __restrict__ prev, int nsub,
-                              const int32_t* __restrict__ iijk, const double* __restrict__ ivolt, int nint, Bnd B,
-                              SorCoef c, int voltfac_on, int usev) {
+struct CondArgs {
+  const int32_t* iijk;
+  const double* ivolt;
+  int nint;
+  const int32_t* sijk[2];
+  const double* sdels[2];
+  const double* svolt[2];
+  const T* srhs[2];
+  int nsub[2];
+};
+
+// New value of subgrid point i of colour `par` (condbndymg with icndbndy = 2,
+// f3d_mgrid.F:2874-2978): neighbours p[6] = xm,xp,ym,yp,zm,zp, prev = the
+// point's value before the pass. Without lcndbndy the bulk update is used.
+template <typename T>
+__device__ inline T subgrid_value(const CondArgs<T>& C, int par, int i, T pxm, T pxp, T pym, T pyp, T pzm, T pzp,
+                                  T prev, const SorCoef& c, int voltfac_on, int lcndbndy) {
+  const T dxsqic = (T)c.cx, dysqic = (T)c.cy, dzsqic = (T)c.cz;
+  const T r = C.srhs[par][i];
+  if (lcndbndy) {
+    const T dxsqicos = (T)(c.cx / c.mgparam), dysqicos = (T)(c.cy / c.mgparam), dzsqicos = (T)(c.cz / c.mgparam);
+    const T voltfac = voltfac_on ? (T)1. : (T)0.;
+    T denom = (T)1., ppp = (T)1.;
+    const double* d = C.sdels[par] + 6 * (size_t)i;
+    const double* v = C.svolt[par] + 6 * (size_t)i;
+    handlesubgrid2<T>(0, 1, pxm, pxp, dxsqicos, d, v, voltfac, denom, ppp);
+    handlesubgrid2<T>(2, 3, pym, pyp, dysqicos, d, v, voltfac, denom, ppp);
+    handlesubgrid2<T>(4, 5, pzm, pzp, dzsqicos, d, v, voltfac, denom, ppp);
+    if (ppp < (T)1.)
+      return (r + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic) / denom + (T)c.spm1 * prev;
+  }
+  return r + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic + (T)c.spm1 * prev;
+}
+
+// Marks the conductor nodes of one level in its rhs array (see the header
+// comment) and saves their rhs values in the subgrid records.
+template <typename T>
+__global__ void k_box(T* __restrict__ rhs, int nx, int ny, CondArgs<T> C, T* __restrict__ srhs0,
+                      T* __restrict__ srhs1) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < C.nint) {
+    rhs[rix(nx, ny, C.iijk[3 * i], C.iijk[3 * i + 1], C.iijk[3 * i + 2])] = Box<T>::make(true, (uint32_t)i);
+    return;
+  }
+  i -= C.nint;
+  for (int par = 0; par < 2; ++par) {
+    if (i < C.nsub[par]) {
+      const int32_t* p = C.sijk[par] + 3 * (size_t)i;
+      T& r = rhs[rix(nx, ny, p[0], p[1], p[2])];
+      (par ? srhs1 : srhs0)[i] = r;
+      r = Box<T>::make(false, (uint32_t)i);
+      return;
+    }
+    i -= C.nsub[par];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Generic in-place path.
+
+// sorhalfpass3d bulk loop (f3d_mgrid.F:2229-2243): one colour, in place.
+// Conductor nodes are skipped here: they keep their old value, which is the
+// prevphi of condbndymg, and k_special_sor updates them.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny,
+                                                  int ixmin, int ixmax, int iymin, int iymax, int izmin, int parity,
+                                                  T cx, T cy, T cz, T spm1) {
+  const int iz = izmin + blockIdx.z;
+  const int iy = iymin + blockIdx.y * blockDim.y + threadIdx.y;
+  if (iy > iymax) return;
+  const int ix = ixmin + ((ixmin + iy + iz + parity) & 1) + 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (ix > ixmax) return;
+  const T r = rhs[rix(nx, ny, ix, iy, iz)];
+  if (isbox(r)) return;
+  const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
+  const size_t p = pix(nx, ny, ix, iy, iz);
+  phi[p] = r + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy + (phi[p - sz] + phi[p + sz]) * cz +
+           spm1 * phi[p];
+}
+
+// condbndymg for one colour then cond_potmg (f3d_mgrid.F:2874-2978,
+// 2426-2470). Subgrid and interior sets are disjoint and only read the other
+// colour, so one launch does both.
+template <typename T>
+__global__ void k_special_sor(T* __restrict__ phi, int nx, int ny, int nz, CondArgs<T> C, int par, Bnd B, SorCoef c,
+                              int voltfac_on, int usev, int lcndbndy) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nsub = C.nsub[par];
   if (i < nsub) {
-    const int ix = sijk[3 * i], iy = sijk[3 * i + 1], iz = sijk[3 * i + 2];
+    const int32_t* q = C.sijk[par] + 3 * (size_t)i;
+    const int ix = q[0], iy = q[1], iz = q[2];
     if (ix == 0 && B.b[0] < 1) return;
     if (ix == nx && B.b[1] < 1) return;
     if (iy == 0 && B.b[2] < 1) return;
@@ -230,29 +330,12 @@ __global__ void k_special_sor(T* __restrict__ phi, const T* __restrict__ rhs, in
     if (iz == nz && B.b[5] < 1) return;
     const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
     const size_t p = pix(nx, ny, ix, iy, iz);
-    T pxm = phi[p - 1], pxp = phi[p + 1], pym = phi[p - sy], pyp = phi[p + sy], pzm = phi[p - sz], pzp = phi[p + sz];
-    const T dxsqic = (T)c.cx, dysqic = (T)c.cy, dzsqic = (T)c.cz;
-    const T dxsqicos = (T)(c.cx / c.mgparam), dysqicos = (T)(c.cy / c.mgparam), dzsqicos = (T)(c.cz / c.mgparam);
-    const T voltfac = voltfac_on ? (T)1. : (T)0.;
-    T denom = (T)1., ppp = (T)1.;
-    const double* d = sdels + 6 * (size_t)i;
-    const double* v = svolt + 6 * (size_t)i;
-    handlesubgrid2<T>(0, 1, pxm, pxp, dxsqicos, d, v, voltfac, denom, ppp);
-    handlesubgrid2<T>(2, 3, pym, pyp, dysqicos, d, v, voltfac, denom, ppp);
-    handlesubgrid2<T>(4, 5, pzm, pzp, dzsqicos, d, v, voltfac, denom, ppp);
-    if (ppp < (T)1.) {
-      phi[p] = (rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic) /
-                   denom +
-               (T)c.spm1 * prev[i];
-    } else {
-      // no special direction: the bulk update the reference would have kept
-      phi[p] = rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic +
-               (T)c.spm1 * prev[i];
-    }
+    phi[p] = subgrid_value<T>(C, par, i, phi[p - 1], phi[p + 1], phi[p - sy], phi[p + sy], phi[p - sz], phi[p + sz],
+                              phi[p], c, voltfac_on, lcndbndy);
     return;
   }
   i -= nsub;
-  if (i < nint) phi[pix(nx, ny, iijk[3 * i], iijk[3 * i + 1], iijk[3 * i + 2])] = usev ? (T)ivolt[i] : (T)0.;
+  if (i < C.nint) phi[pix(nx, ny, C.iijk[3 * i], C.iijk[3 * i + 1], C.iijk[3 * i + 2])] = usev ? (T)C.ivolt[i] : (T)0.;
 }
 
 // cond_potmg alone (start of sorpass3d and the mgform=2 initial phi).
@@ -264,7 +347,7 @@ __global__ void k_interior(T* __restrict__ phi, int nx, int ny, const int32_t* _
 }
 
 // condbndymgint (f3d_mgrid.F:2982-3092): Neumann subgrid neighbours take the
-// point's value. Points of both colours in one launch.
+// point's value.
 template <typename T>
 __global__ void k_condbndymgint(T* __restrict__ phi, int nx, int ny, int nz, const int32_t* __restrict__ ijk,
                                 const double* __restrict__ dels, int n, Bnd B) {
@@ -291,18 +374,150 @@ __global__ void k_condbndymgint(T* __restrict__ phi, int nx, int ny, int nz, con
 }
 
 // ---------------------------------------------------------------------------
+// Fused sweep: one sorpass3d (both colours, conductors, guard planes) from
+// phi_in to phi_out. A CTA owns a FTX x FTY column of nodes (guards
+// included) over FZC output planes and marches in z with four planes of phi
+// (halo 2) and three planes of rhs in shared memory: red is updated on
+// plane k over the tile plus a one-cell halo, then black on plane k-1 over
+// the tile, then plane k-1 is stored. Halo values are recomputed by the
+// neighbouring CTAs identically, so tiles need no synchronisation. With
+// periodic z, planes -1 and nz+1 (and nz) are computed from wrapped loads,
+// which gives exactly the guard copies of applyboundaryconditions3d.
+constexpr int FTX = 32, FTY = 16, FHX = FTX + 4, FHY = FTY + 4, FPL = FHX * FHY, FZC = 32, FNT = 256;
+
+template <typename T>
+struct FusedArgs {
+  const T* in;
+  T* out;
+  const T* rhs;
+  int nx, ny, nz, zper;
+  SorCoef c;
+  CondArgs<T> C;
+  int usev, voltfac_on, lcndbndy;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(FNT) k_sor_fused(FusedArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sp = reinterpret_cast<T*>(smraw);  // [4][FPL] phi planes
+  T* sr = sp + 4 * FPL;                 // [3][FPL] rhs planes
+  const int tid = threadIdx.x;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int x0 = -1 + (int)blockIdx.x * FTX, y0 = -1 + (int)blockIdx.y * FTY;
+  const int zs = -1 + (int)blockIdx.z * FZC;
+  const int ze = min(zs + FZC, nz + 2);
+  const T cx = (T)a.c.cx, cy = (T)a.c.cy, cz = (T)a.c.cz, spm1 = (T)a.c.spm1;
+
+  // periodic z: plane nz is the same node set as plane 0 (applyboundaryconditions3d
+  // copies 0 -> nz after every half pass), so virtual planes wrap modulo nz
+  auto wrapz = [&](int p) { return !a.zper ? p : ((p % nz) + nz) % nz; };
+  auto zexists = [&](int p) { return a.zper || (p >= -1 && p <= nz + 1); };
+  auto zupdated = [&](int p) { return a.zper || (p >= 1 && p <= nz - 1); };
+  auto mod3 = [](int p) { return ((p % 3) + 3) % 3; };
+
+  // old phi of virtual plane p (interior conductor nodes at their imposed
+  // value, as cond_potmg leaves them) and its rhs
+  auto load = [&](int p) {
+    T* dp = sp + (p & 3) * FPL;
+    T* dr = sr + mod3(p) * FPL;
+    const bool ok = zexists(p);
+    const int zr = wrapz(p);
+    const bool zreal = zr >= 0 && zr <= nz;
+    for (int i = tid; i < FPL; i += FNT) {
+      const int lx = i % FHX, ly = i / FHX;
+      const int ix = x0 - 2 + lx, iy = y0 - 2 + ly;
+      T v = (T)0., r = (T)0.;
+      if (ok && ix >= -1 && ix <= nx + 1 && iy >= -1 && iy <= ny + 1) {
+        v = a.in[pix(nx, ny, ix, iy, zr)];
+        if (zreal && ix >= 0 && ix <= nx && iy >= 0 && iy <= ny) {
+          r = a.rhs[rix(nx, ny, ix, iy, zr)];
+          if (isbox(r) && Box<T>::interior(r)) {
+            const uint32_t k = Box<T>::idx(r);
+            if (k < (uint32_t)a.C.nint) v = a.usev ? (T)a.C.ivolt[k] : (T)0.;
+          }
+        }
+      }
+      dp[i] = v;
+      dr[i] = r;
+    }
+  };
+
+  // colour `par` (0 red = even ix+iy+iz, 1 black) on virtual plane k, over
+  // the tile grown by `halo` cells
+  auto relax = [&](int k, int par, int halo) {
+    if (!zupdated(k)) return;
+    T* pc = sp + (k & 3) * FPL;
+    const T* pm = sp + ((k - 1) & 3) * FPL;
+    const T* pp = sp + ((k + 1) & 3) * FPL;
+    const T* rr = sr + mod3(k) * FPL;
+    const int zr = wrapz(k);
+    const int w = FTX + 2 * halo, h = FTY + 2 * halo, half = w / 2;
+    for (int i = tid; i < half * h; i += FNT) {
+      const int ly = 2 - halo + i / half;
+      const int iy = y0 - 2 + ly;
+      const int lxs = 2 - halo;
+      const int ixs = x0 - 2 + lxs;
+      const int lx = lxs + (((ixs + iy + zr + par) & 1) ? 1 : 0) + 2 * (i % half);
+      const int ix = x0 - 2 + lx;
+      if (ix < 1 || ix > nx - 1 || iy < 1 || iy > ny - 1) continue;
+      const int q = lx + FHX * ly;
+      const T r = rr[q];
+      const T self = pc[q];
+      T nv;
+      if (isbox(r)) {
+        if (Box<T>::interior(r)) continue;  // imposed at load time
+        const uint32_t k2 = Box<T>::idx(r);
+        if (k2 >= (uint32_t)a.C.nsub[par]) {
+          nv = r;  // not a valid record: propagate the NaN
+        } else {
+          nv = subgrid_value<T>(a.C, par, (int)k2, pc[q - 1], pc[q + 1], pc[q - FHX], pc[q + FHX], pm[q], pp[q], self,
+                                a.c, a.voltfac_on, a.lcndbndy);
+        }
+      } else {
+        nv = r + (pc[q - 1] + pc[q + 1]) * cx + (pc[q - FHX] + pc[q + FHX]) * cy + (pm[q] + pp[q]) * cz + spm1 * self;
+      }
+      pc[q] = nv;
+    }
+  };
+
+  auto store = [&](int k) {
+    const T* pc = sp + (k & 3) * FPL;
+    for (int i = tid; i < FTX * FTY; i += FNT) {
+      const int lx = 2 + i % FTX, ly = 2 + i / FTX;
+      const int ix = x0 + i % FTX, iy = y0 + i / FTX;
+      if (ix <= nx + 1 && iy <= ny + 1) a.out[pix(nx, ny, ix, iy, k)] = pc[lx + FHX * ly];
+    }
+  };
+
+  load(zs - 2);
+  load(zs - 1);
+  load(zs);
+  __syncthreads();
+  relax(zs - 1, 0, 1);
+  for (int k = zs; k <= ze; ++k) {
+    load(k + 1);
+    __syncthreads();
+    relax(k, 0, 1);
+    __syncthreads();
+    if (k - 1 >= zs) {
+      relax(k - 1, 1, 0);
+      __syncthreads();
+      store(k - 1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // residual3d bulk part (f3d_mgrid.F:3519-3586).
 //   MODE 0: writes the padded res array (0 outside the updated range)
-//   MODE 1: no store, only the max over non-special nodes (norm)
+//   MODE 1: no store, only the max over non-conductor nodes (norm)
 //   MODE 2: writes the unpadded FP32 rhs of the next correction solve
-// The max skips nodes flagged in `mask` (conductor nodes), which the special
-// kernel handles.
+// Conductor nodes get 0 here; k_special_res fills them in.
 template <typename T, int MODE, typename TO>
 __global__ void __launch_bounds__(256) k_residual(const T* __restrict__ phi, const T* __restrict__ rhs,
                                                   TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
                                                   int ixmax, int iymin, int iymax, int izmin, int izmax, T cx, T cy,
-                                                  T cz, T mgparam, const uint32_t* __restrict__ mask,
-                                                  unsigned long long* maxout) {
+                                                  T cz, T mgparam, unsigned long long* maxout) {
   // MODE 0 covers the padded array, the others the node array
   const int g = (MODE == 0) ? 1 : 0;
   const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x) - g;
@@ -314,14 +529,13 @@ __global__ void __launch_bounds__(256) k_residual(const T* __restrict__ phi, con
     T r = (T)0.;
     bool inrange = ix >= ixmin && ix <= ixmax && iy >= iymin && iy <= iymax && iz >= izmin && iz <= izmax;
     if (inrange) {
-      const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
-      const size_t p = pix(nx, ny, ix, iy, iz);
-      r = rhs[rix(nx, ny, ix, iy, iz)] + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy +
-          (phi[p - sz] + phi[p + sz]) * cz - phi[p] * mgparam;
-      if (maxout) {
-        size_t ri = rix(nx, ny, ix, iy, iz);
-        bool special = mask && ((mask[ri >> 5] >> (ri & 31)) & 1u);
-        if (!special) m = fabs((double)r);
+      const T b = rhs[rix(nx, ny, ix, iy, iz)];
+      if (!isbox(b)) {
+        const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
+        const size_t p = pix(nx, ny, ix, iy, iz);
+        r = b + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy + (phi[p - sz] + phi[p + sz]) * cz -
+            phi[p] * mgparam;
+        m = fabs((double)r);
       }
     }
     if (MODE == 0) out[pix(nx, ny, ix, iy, iz)] = (TO)r;
@@ -333,13 +547,9 @@ __global__ void __launch_bounds__(256) k_residual(const T* __restrict__ phi, con
 // cond_potmgres (interior -> 0, f3d_mgrid.F:2472-2500) and condbndyres
 // (icndbndy = 2, f3d_mgrid.F:3240-3362) for both colours.
 template <typename T, int MODE, typename TO>
-__global__ void k_special_res(const T* __restrict__ phi, const T* __restrict__ rhs, TO* __restrict__ out, int nx,
-                              int ny, int nz, const int32_t* __restrict__ ijk0, const double* __restrict__ dels0,
-                              const double* __restrict__ volt0, int n0, const int32_t* __restrict__ ijk1,
-                              const double* __restrict__ dels1, const double* __restrict__ volt1, int n1,
-                              const int32_t* __restrict__ iijk, int nint, Bnd B, double dxsqi, double dysqi,
-                              double dzsqi, double mgparam_d, int voltfac_on, int mgform2init,
-                              unsigned long long* maxout) {
+__global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, int nx, int ny, int nz, CondArgs<T> C,
+                              Bnd B, double dxsqi, double dysqi, double dzsqi, double mgparam_d, int voltfac_on,
+                              int mgform2init, int lcndbndy, unsigned long long* maxout) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double m = 0.;
   auto store = [&](int ix, int iy, int iz, T v) {
@@ -347,15 +557,15 @@ __global__ void k_special_res(const T* __restrict__ phi, const T* __restrict__ r
     if (MODE == 2 && ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz)
       out[rix(nx, ny, ix, iy, iz)] = (TO)v;
   };
-  if (i < nint) {
-    store(iijk[3 * i], iijk[3 * i + 1], iijk[3 * i + 2], (T)0.);
-  } else if (i < nint + n0 + n1) {
-    int k = i - nint;
-    const int32_t* ijk = (k < n0) ? ijk0 : ijk1;
-    const double* dd = (k < n0) ? dels0 : dels1;
-    const double* vv = (k < n0) ? volt0 : volt1;
-    if (k >= n0) k -= n0;
-    const int ix = ijk[3 * k], iy = ijk[3 * k + 1], iz = ijk[3 * k + 2];
+  const int n0 = C.nsub[0], n1 = C.nsub[1];
+  if (i < C.nint) {
+    store(C.iijk[3 * i], C.iijk[3 * i + 1], C.iijk[3 * i + 2], (T)0.);
+  } else if (i < C.nint + n0 + n1) {
+    int k = i - C.nint;
+    const int par = (k < n0) ? 0 : 1;
+    if (par) k -= n0;
+    const int32_t* q = C.sijk[par] + 3 * (size_t)k;
+    const int ix = q[0], iy = q[1], iz = q[2];
     bool skip = (ix == 0 && B.b[0] == 0) || (ix == nx && B.b[1] == 0) || (iy == 0 && B.b[2] == 0) ||
                 (iy == ny && B.b[3] == 0) || (iz == 0 && B.b[4] == 0) || (iz == nz && B.b[5] == 0);
     if (!skip) {
@@ -366,26 +576,30 @@ __global__ void k_special_res(const T* __restrict__ phi, const T* __restrict__ r
       const T mgparam = (T)mgparam_d;
       const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
       const size_t p = pix(nx, ny, ix, iy, iz);
+      const T rhsv = C.srhs[par][k];
       T pxm = phi[p - 1], pxp = phi[p + 1], pym = phi[p - sy], pyp = phi[p + sy], pzm = phi[p - sz],
         pzp = phi[p + sz];
       T denom = (T)1., ppp = (T)1.;
-      const T voltfac = voltfac_on ? (T)1. : (T)0.;
-      const double* d = dd + 6 * (size_t)k;
-      const double* v = vv + 6 * (size_t)k;
-      handlesubgrid2<T>(0, 1, pxm, pxp, dxsqic, d, v, voltfac, denom, ppp);
-      handlesubgrid2<T>(2, 3, pym, pyp, dysqic, d, v, voltfac, denom, ppp);
-      handlesubgrid2<T>(4, 5, pzm, pzp, dzsqic, d, v, voltfac, denom, ppp);
+      if (lcndbndy) {
+        const T voltfac = voltfac_on ? (T)1. : (T)0.;
+        const double* d = C.sdels[par] + 6 * (size_t)k;
+        const double* v = C.svolt[par] + 6 * (size_t)k;
+        handlesubgrid2<T>(0, 1, pxm, pxp, dxsqic, d, v, voltfac, denom, ppp);
+        handlesubgrid2<T>(2, 3, pym, pyp, dysqic, d, v, voltfac, denom, ppp);
+        handlesubgrid2<T>(4, 5, pzm, pzp, dzsqic, d, v, voltfac, denom, ppp);
+      }
       if (ppp < (T)1.) {
         // the reported max always uses the ppp-scaled row (getresidual,
         // scripts/multigrid.py:940); the stored value drops the scaling for
         // the residual-correction set-up
         const T pppmax = ppp;
         if (mgform2init) ppp = (T)1.;
-        const T inner = rhs[rix(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqics + (pym + pyp) * dysqics +
-                        (pzm + pzp) * dzsqics - phi[p] * mgparam * denom;
+        const T inner = rhsv + (pxm + pxp) * dxsqics + (pym + pyp) * dysqics + (pzm + pzp) * dzsqics -
+                        phi[p] * mgparam * denom;
         T r = ppp * inner;
         store(ix, iy, iz, r);
         m = fabs((double)(pppmax * inner));
+        const double* d = C.sdels[par] + 6 * (size_t)k;
         if (0. >= d[0] && d[0] >= -1.) store(ix - 1, iy, iz, (T)0.);
         if (0. >= d[1] && d[1] >= -1.) store(ix + 1, iy, iz, (T)0.);
         if (0. >= d[2] && d[2] >= -1.) store(ix, iy - 1, iz, (T)0.);
@@ -393,9 +607,9 @@ __global__ void k_special_res(const T* __restrict__ phi, const T* __restrict__ r
         if (0. >= d[4] && d[4] >= -1.) store(ix, iy, iz - 1, (T)0.);
         if (0. >= d[5] && d[5] >= -1.) store(ix, iy, iz + 1, (T)0.);
       } else {
-        // the bulk value stays; it was left out of the bulk max
-        T r = rhs[rix(nx, ny, ix, iy, iz)] + (phi[p - 1] + phi[p + 1]) * dxsqics +
-              (phi[p - sy] + phi[p + sy]) * dysqics + (phi[p - sz] + phi[p + sz]) * dzsqics - phi[p] * mgparam;
+        // no special direction: the bulk residual the reference keeps
+        T r = rhsv + (pxm + pxp) * dxsqics + (pym + pyp) * dysqics + (pzm + pzp) * dzsqics - phi[p] * mgparam;
+        store(ix, iy, iz, r);
         m = fabs((double)r);
       }
     }
@@ -470,6 +684,7 @@ __global__ void k_expand(T* __restrict__ phi, const T* __restrict__ pc, int nx, 
       wx * wy * wz * pc[pix(nxc, nyc, jx + 1, jy + 1, jz + 1)];
 }
 
+
 // mgerror = max|phisave - phi| over nodes 0..n (f3d_mgrid.F:383-391).
 __global__ void k_maxdiff(const double* __restrict__ a, const double* __restrict__ b, int nx, int ny,
                           unsigned long long* maxout) {
@@ -484,13 +699,14 @@ __global__ void k_maxdiff(const double* __restrict__ a, const double* __restrict
   block_max_to(maxout, m);
 }
 
-// rhs = rho * reps0c (f3d_mgrid.F:223) and max|rhs|.
+// rhs = rho * reps0c (f3d_mgrid.F:223) and max|rhs|; flags a non-finite rho.
 __global__ void k_scale_rhs(const double* __restrict__ rho, double* __restrict__ rhs, size_t n, double s,
-                            unsigned long long* maxout) {
+                            unsigned long long* maxout, unsigned long long* flag) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   double m = 0.;
   if (i < n) {
     double v = rho[i] * s;
+    if (!isfinite(v)) atomicOr(flag, 2ull);
     rhs[i] = v;
     m = fabs(v);
   }
@@ -524,18 +740,36 @@ template <typename T>
 struct Arr;
 template <>
 struct Arr<double> {
-  static double* phi(Level& L) { return L.phi; }
+  static double*& phi(Level& L) { return L.phi; }
+  static double*& phi2(Level& L) { return L.phi2; }
   static double* rhs(Level& L) { return L.rhs; }
   static double* res(Level& L) { return L.res; }
-  static double* prev(DevSubgrid& S) { return S.prev; }
+  static double* srhs(DevSubgrid& S) { return S.rhs; }
 };
 template <>
 struct Arr<float> {
-  static float* phi(Level& L) { return L.phif; }
+  static float*& phi(Level& L) { return L.phif; }
+  static float*& phi2(Level& L) { return L.phif2; }
   static float* rhs(Level& L) { return L.rhsf; }
   static float* res(Level& L) { return L.resf; }
-  static float* prev(DevSubgrid& S) { return S.prevf; }
+  static float* srhs(DevSubgrid& S) { return S.rhsf; }
 };
+
+template <typename T>
+CondArgs<T> cond_args(Level& L) {
+  CondArgs<T> C;
+  C.iijk = L.int_ijk;
+  C.ivolt = L.int_volt;
+  C.nint = L.n_int;
+  for (int p = 0; p < 2; ++p) {
+    C.sijk[p] = L.sub[p].ijk;
+    C.sdels[p] = L.sub[p].dels;
+    C.svolt[p] = L.sub[p].volt;
+    C.srhs[p] = Arr<T>::srhs(L.sub[p]);
+    C.nsub[p] = L.sub[p].n;
+  }
+  return C;
+}
 
 struct Ranges {
   int ixmin, ixmax, iymin, iymax, izmin, izmax;
@@ -559,6 +793,7 @@ struct Solver {
   const wg_solve_opts* o;
   Bnd B;
   cudaStream_t s;
+  bool fused_ok;  // boundary types allow the fused sweep
 
   template <typename T>
   void bc(Level& L, T* u, bool lwithdirichlet) {
@@ -583,36 +818,78 @@ struct Solver {
     if (!L.has_neumann_sub) return;
     for (int par = 0; par < 2; ++par) {
       DevSubgrid& S = L.sub[par];
-      if (S.n)
-        { ++c->nlaunch; k_condbndymgint<T><<<cdiv(S.n, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, S.ijk, S.dels, S.n, B); }
+      if (S.n) {
+        ++c->nlaunch;
+        k_condbndymgint<T><<<cdiv(S.n, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, S.ijk, S.dels, S.n, B);
+      }
     }
+  }
+
+  // Marks conductor nodes in the rhs array of level l.
+  template <typename T>
+  void box(int l) {
+    Level& L = c->lv[l];
+    int n = L.n_int + L.sub[0].n + L.sub[1].n;
+    if (!n) return;
+    ++c->nlaunch;
+    k_box<T><<<cdiv(n, 128), 128, 0, s>>>(Arr<T>::rhs(L), L.d.nx, L.d.ny, cond_args<T>(L), Arr<T>::srhs(L.sub[0]),
+                                          Arr<T>::srhs(L.sub[1]));
   }
 
   // sorpass3d (f3d_mgrid.F:1949-2093)
   template <typename T>
   void sorpass(int l, bool usev) {
     Level& L = c->lv[l];
+    const SorCoef k = coef(L.d);
+    if (fused_ok && !L.has_neumann_sub) {
+      FusedArgs<T> a;
+      a.in = Arr<T>::phi(L);
+      a.out = Arr<T>::phi2(L);
+      a.rhs = Arr<T>::rhs(L);
+      a.nx = L.d.nx;
+      a.ny = L.d.ny;
+      a.nz = L.d.nz;
+      a.zper = B.b[4] == 2;
+      a.c = k;
+      a.C = cond_args<T>(L);
+      a.usev = usev;
+      a.voltfac_on = usev;
+      a.lcndbndy = o->lcndbndy;
+      dim3 grd(cdiv(L.d.nx + 3, FTX), cdiv(L.d.ny + 3, FTY), cdiv(L.d.nz + 3, FZC));
+      const size_t smem = 7 * FPL * sizeof(T);
+      ++c->nlaunch;
+      int pe = (l == 0) ? c->prof_begin(WG_PROF_SOR0, 2. * (double)L.nr) : -1;
+      k_sor_fused<T><<<grd, FNT, smem, s>>>(a);
+      c->prof_end(pe);
+      std::swap(Arr<T>::phi(L), Arr<T>::phi2(L));
+      return;
+    }
     T* phi = Arr<T>::phi(L);
     const T* rhs = Arr<T>::rhs(L);
-    if (L.n_int) { ++c->nlaunch; k_interior<T><<<cdiv(L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev); }
+    if (L.n_int) {
+      ++c->nlaunch;
+      k_interior<T><<<cdiv(L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev);
+    }
     neumann_int<T>(L, phi);
     const Ranges R = ranges(L.d, B.b, true);
-    const SorCoef k = coef(L.d);
     const int nyr = R.iymax - R.iymin + 1, nzr = R.izmax - R.izmin + 1;
     const int nhalf = (R.ixmax - R.ixmin) / 2 + 1;
     for (int parity = 0; parity < 2; ++parity) {
-      DevSubgrid& S = L.sub[parity];
-      int nsub = o->lcndbndy ? S.n : 0;
-      if (nsub) { ++c->nlaunch; k_save_prev<T><<<cdiv(nsub, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, S.ijk, nsub, Arr<T>::prev(S)); }
       if (nyr > 0 && nzr > 0 && nhalf > 0) {
         dim3 blk(32, 8), grd(cdiv(nhalf, 32), cdiv(nyr, 8), nzr);
-        { ++c->nlaunch; int pe = (l == 0) ? c->prof_begin(WG_PROF_SOR0, (double)L.nr) : -1; k_sor_bulk<T><<<grd, blk, 0, s>>>(phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin,
-                                          parity, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1); c->prof_end(pe); }
+        ++c->nlaunch;
+        int pe = (l == 0) ? c->prof_begin(WG_PROF_SOR0, (double)L.nr) : -1;
+        k_sor_bulk<T><<<grd, blk, 0, s>>>(phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin,
+                                          parity, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1);
+        c->prof_end(pe);
       }
-      if (nsub + L.n_int)
-        { ++c->nlaunch; k_special_sor<T><<<cdiv(nsub + L.n_int, 128), 128, 0, s>>>(
-            phi, rhs, L.d.nx, L.d.ny, L.d.nz, S.ijk, S.dels, S.volt, Arr<T>::prev(S), nsub, L.int_ijk, L.int_volt,
-            L.n_int, B, k, (int)usev, (int)usev); }
+      int nsub = L.sub[parity].n;
+      if (nsub + L.n_int) {
+        ++c->nlaunch;
+        k_special_sor<T><<<cdiv(nsub + L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, cond_args<T>(L),
+                                                                    parity, B, k, (int)usev, (int)usev,
+                                                                    o->lcndbndy);
+      }
       neumann_int<T>(L, phi);
       bc<T>(L, phi, false);
     }
@@ -621,25 +898,30 @@ struct Solver {
   // residual3d into the padded res array of level l (MODE 0), or a norm only
   // (MODE 1), or into the FP32 rhs of level 0 (MODE 2).
   template <typename T, int MODE, typename TO>
-  void residual(int l, const T* phi, const T* rhs, TO* out, bool mgform2init, bool voltfac_on,
-                unsigned long long* maxout) {
+  void residual(int l, const T* phi, TO* out, bool mgform2init, bool voltfac_on, unsigned long long* maxout) {
     Level& L = c->lv[l];
+    const T* rhs = Arr<T>::rhs(L);
     const Ranges R = ranges(L.d, B.b, false);
     double dxsqi = 1. / (L.d.dx * L.d.dx), dysqi = 1. / (L.d.dy * L.d.dy), dzsqi = 1. / (L.d.dz * L.d.dz);
     double cst = 0.5 / (dxsqi + dysqi + dzsqi);
     const int g = (MODE == 0) ? 1 : 0;
     dim3 blk(32, 8), grd(cdiv(L.d.nx + 1 + 2 * g, 32), cdiv(L.d.ny + 1 + 2 * g, 8), L.d.nz + 1 + 2 * g);
-    { ++c->nlaunch; int pe = (l == 0) ? c->prof_begin(WG_PROF_RESID0, (double)L.nr) : -1; k_residual<T, MODE, TO><<<grd, blk, 0, s>>>(phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
-                                                R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
-                                                (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst),
-                                                (T)o->mgparam, L.mask, maxout); c->prof_end(pe); }
-    int nsub = o->lcndbndy ? (L.sub[0].n + L.sub[1].n) : 0;
-    int n0 = o->lcndbndy ? L.sub[0].n : 0, n1 = o->lcndbndy ? L.sub[1].n : 0;
-    if (nsub + L.n_int)
-      { ++c->nlaunch; k_special_res<T, MODE, TO><<<cdiv(nsub + L.n_int, 128), 128, 0, s>>>(
-          phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, L.sub[0].ijk, L.sub[0].dels, L.sub[0].volt, n0, L.sub[1].ijk,
-          L.sub[1].dels, L.sub[1].volt, n1, L.int_ijk, L.n_int, B, dxsqi, dysqi, dzsqi, o->mgparam, (int)voltfac_on,
-          (int)mgform2init, maxout); }
+    {
+      ++c->nlaunch;
+      int pe = (l == 0) ? c->prof_begin(WG_PROF_RESID0, (double)L.nr) : -1;
+      k_residual<T, MODE, TO><<<grd, blk, 0, s>>>(phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
+                                                  R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
+                                                  (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst),
+                                                  (T)o->mgparam, maxout);
+      c->prof_end(pe);
+    }
+    int n = L.sub[0].n + L.sub[1].n + L.n_int;
+    if (n) {
+      ++c->nlaunch;
+      k_special_res<T, MODE, TO><<<cdiv(n, 128), 128, 0, s>>>(phi, out, L.d.nx, L.d.ny, L.d.nz, cond_args<T>(L), B,
+                                                              dxsqi, dysqi, dzsqi, o->mgparam, (int)voltfac_on,
+                                                              (int)mgform2init, o->lcndbndy, maxout);
+    }
     if (MODE == 0) bc<TO>(L, (TO*)out, false);
   }
 
@@ -650,7 +932,7 @@ struct Solver {
     for (int i = 0; i < o->downpasses; ++i) sorpass<T>(l, usev);
     const LevelDims& d = L.d;
     if (d.nx >= 4 && d.ny >= 4 && d.nz >= 4 && l < o->mgmaxlevels && l + 1 < (int)c->lv.size()) {
-      residual<T, 0, T>(l, Arr<T>::phi(L), Arr<T>::rhs(L), Arr<T>::res(L), false, usev, nullptr);
+      residual<T, 0, T>(l, Arr<T>::phi(L), Arr<T>::res(L), false, usev, nullptr);
       Level& Lc = c->lv[l + 1];
       const LevelDims& dc = Lc.d;
       double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
@@ -658,16 +940,20 @@ struct Solver {
       double ff = (dxsqi + dysqi + dzsqi) / (dxcsqi + dycsqi + dzcsqi);
       Ranges Rc = ranges(dc, B.b, false);
       dim3 blk(32, 8), grd(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), dc.nz + 1);
-      { ++c->nlaunch; k_restrict<T><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, d.nz, dc.nx, dc.ny, dc.nz,
+      ++c->nlaunch;
+      k_restrict<T><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, d.nz, dc.nx, dc.ny, dc.nz,
                                         Rc.ixmin, Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
-                                        1. * dc.nx / d.nx, 1. * dc.ny / d.ny, 1. * dc.nz / d.nz, ff); }
+                                        1. * dc.nx / d.nx, 1. * dc.ny / d.ny, 1. * dc.nz / d.nz, ff);
+      box<T>(l + 1);
       cudaMemsetAsync(Arr<T>::phi(Lc), 0, Lc.np * sizeof(T), s);
       vcycle<T>(l + 1, false);
       Ranges R = ranges(d, B.b, false);
       dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), R.izmax - R.izmin + 1);
-      if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin)
-        { ++c->nlaunch; k_expand<T><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny, dc.nz, d.nz,
-                                         R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin); }
+      if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin) {
+        ++c->nlaunch;
+        k_expand<T><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny, dc.nz, d.nz,
+                                         R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin);
+      }
       bc<T>(L, Arr<T>::phi(L), false);
     }
     for (int i = 0; i < o->uppasses; ++i) sorpass<T>(l, usev);
@@ -684,7 +970,19 @@ struct Solver {
     }
     return WG_OK;
   }
+
+  // Leaves level 0's phi in the user-visible buffer.
+  int restore_phi(double* user) {
+    Level& L0 = c->lv[0];
+    if (L0.phi != user) {
+      WG_TRY_CUDA(cudaMemcpyAsync(user, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      std::swap(L0.phi, L0.phi2);
+    }
+    return WG_OK;
+  }
 };
+
+bool fused_allowed(const int* b) { return b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0 && (b[4] == 0 || b[4] == 2); }
 
 }  // namespace
 
@@ -697,17 +995,28 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
     set_error("wg_solve: invalid options");
     return WG_EINVAL;
   }
-  if (o->precision == 1) WG_TRY(ensure_fp32(c));
-  Solver S{c, o, {}, c->stream};
+  if (o->precision == 1) {
+    WG_TRY(ensure_fp32(c));
+    for (Level& L : c->lv)
+      for (DevSubgrid& S : L.sub)
+        if ((uint32_t)S.n > Box<float>::kMax || (uint32_t)L.n_int > Box<float>::kMax) {
+          set_error("wg_solve: more than 4194303 conductor points of one kind on a level (FP32 limit)");
+          return WG_ETOOLARGE;
+        }
+  }
+  Solver S{c, o, {}, c->stream, false};
   for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
+  S.fused_ok = fused_allowed(S.B.b);
   cudaStream_t s = c->stream;
   Level& L0 = c->lv[0];
+  double* user_phi = L0.phi;
   const LevelDims& d = L0.d;
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = o->mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
   unsigned long long* red = c->dred;
   WG_TRY_CUDA(cudaMemsetAsync(red, 0, 4 * sizeof(unsigned long long), s));
-  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, red + 2); }
+  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, red + 2, red + 3); }
+  S.box<double>(0);
   S.bc<double>(L0, L0.phi, false);
   dim3 blk(32, 8), grdn(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1);
   dim3 grdp(cdiv(d.nx + 3, 32), cdiv(d.ny + 3, 8), d.nz + 3);
@@ -715,11 +1024,16 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   double err = 2. * o->mgtol + 1., relres = -1.;
   bool conv = false;
   double rv[4];
+  WG_TRY(S.fetch_red(rv, 3));
+  if (c->hred[3] & 2ull) {
+    set_error("wg_solve: rho contains NaN or Inf");
+    return WG_EINVAL;
+  }
   if (o->precision == 0) {
     for (;;) {
       if (o->tolkind == 1) {
         WG_TRY_CUDA(cudaMemsetAsync(red + 1, 0, sizeof(unsigned long long), s));
-        S.residual<double, 1, double>(0, L0.phi, L0.rhs, nullptr, false, true, red + 1);
+        S.residual<double, 1, double>(0, L0.phi, nullptr, false, true, red + 1);
         WG_TRY(S.fetch_red(rv, 3));
         relres = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
         if (relres <= o->mgtol) { conv = true; break; }
@@ -740,17 +1054,20 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   } else {
     for (;;) {
       // residual of the FP64 solution with actual voltages (mgform = 2 set-up)
-      if (L0.n_int)
-        { ++c->nlaunch; k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(L0.phi, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1); }
+      if (L0.n_int) {
+        ++c->nlaunch;
+        k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(L0.phi, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);
+      }
       S.neumann_int<double>(L0, L0.phi);
       WG_TRY_CUDA(cudaMemsetAsync(red + 1, 0, sizeof(unsigned long long), s));
-      S.residual<double, 2, float>(0, L0.phi, L0.rhs, L0.rhsf, true, true, red + 1);
+      S.residual<double, 2, float>(0, L0.phi, L0.rhsf, true, true, red + 1);
       if (o->tolkind == 1 || it >= o->mgmaxiters) {
         WG_TRY(S.fetch_red(rv, 3));
         relres = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
         if (o->tolkind == 1 && relres <= o->mgtol) { conv = true; break; }
       }
       if (it >= o->mgmaxiters) break;
+      S.box<float>(0);
       WG_TRY_CUDA(cudaMemsetAsync(L0.phif, 0, L0.np * sizeof(float), s));
       S.vcycle<float>(0, false);
       WG_TRY_CUDA(cudaMemsetAsync(red, 0, sizeof(unsigned long long), s));
@@ -764,6 +1081,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       }
     }
   }
+  WG_TRY(S.restore_phi(user_phi));
   S.bc<double>(L0, L0.phi, true);
   WG_TRY_CUDA(cudaGetLastError());
   WG_TRY_CUDA(cudaStreamSynchronize(s));
@@ -776,7 +1094,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
 
 int relresidual(wg_ctx* c, double mgparam, double* out) {
   wg_solve_opts o{mgparam, 0., 0, 101, 1, 1, 1, 0, 1};
-  Solver S{c, &o, {}, c->stream};
+  Solver S{c, &o, {}, c->stream, false};
   for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
   cudaStream_t s = c->stream;
   Level& L0 = c->lv[0];
@@ -784,15 +1102,27 @@ int relresidual(wg_ctx* c, double mgparam, double* out) {
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
   WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
-  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, c->dred + 2); }
+  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, c->dred + 2, c->dred + 3); }
+  S.box<double>(0);
   // residual of a copy with the conductor voltages imposed, as the solver sees it
   WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  if (L0.n_int)
-    { ++c->nlaunch; k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1); }
-  S.residual<double, 1, double>(0, c->phisave, L0.rhs, nullptr, false, true, c->dred + 1);
+  if (L0.n_int) {
+    ++c->nlaunch;
+    k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);
+  }
+  S.residual<double, 1, double>(0, c->phisave, nullptr, false, true, c->dred + 1);
   double rv[4];
   WG_TRY(S.fetch_red(rv, 3));
   *out = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
+  return WG_OK;
+}
+
+// Shared memory of the fused sweep exceeds the 48 KB default for FP64.
+int configure_kernels() {
+  WG_TRY_CUDA(cudaFuncSetAttribute(k_sor_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(7 * FPL * sizeof(double))));
+  WG_TRY_CUDA(cudaFuncSetAttribute(k_sor_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(7 * FPL * sizeof(float))));
   return WG_OK;
 }
 

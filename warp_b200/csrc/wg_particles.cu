@@ -277,6 +277,40 @@ __global__ void __launch_bounds__(256) k_advance(const double* __restrict__ phi,
   uzp[i] = uz;
 }
 
+// Cell key of particlesortxyzwithcopy (top.F:5095-5130):
+// ix + (nx+1)*(iy + (ny+1)*iz); lost particles get the key past the last
+// node so that a stable sort moves them behind the live ones.
+__global__ void k_cell_keys(const double* __restrict__ xp, const double* __restrict__ yp,
+                            const double* __restrict__ zp, const double* __restrict__ gaminv, int64_t np, GridP g,
+                            int64_t* __restrict__ key) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  if (gaminv[i] == 0.) {
+    key[i] = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+    return;
+  }
+  int ii, jj, kk;
+  double f;
+  cellfrac((xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, f);
+  cellfrac((yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, f);
+  cellfrac((zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, f);
+  key[i] = (int64_t)ii + (int64_t)(g.nx + 1) * ((int64_t)jj + (int64_t)(g.ny + 1) * kk);
+}
+
+// dst[k][i] = src[k][perm[i]] for the 7 particle arrays.
+__global__ void k_permute(const int64_t* __restrict__ perm, int64_t np, wg_particles src, wg_particles dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int64_t j = perm[i];
+  dst.x[i] = src.x[j];
+  dst.y[i] = src.y[j];
+  dst.z[i] = src.z[j];
+  dst.ux[i] = src.ux[j];
+  dst.uy[i] = src.uy[j];
+  dst.uz[i] = src.uz[j];
+  dst.gaminv[i] = src.gaminv[j];
+}
+
 constexpr int kMomN = 11;
 
 // Per-block partial sums of the moments of live particles (getzmmnt,
@@ -436,5 +470,24 @@ int moments(wg_ctx* c, const wg_particles* p, double* out) {
 }
 
 int moments_scratch_doubles(int nb) { return nb * kMomN + 8; }
+
+int cell_keys(wg_ctx* c, const wg_particles* p, int64_t* keys) {
+  if (!p || !keys || p->np < 0) { set_error("wg_particle_keys: null arguments"); return WG_EINVAL; }
+  if (p->np == 0) return WG_OK;
+  { ++c->nlaunch; k_cell_keys<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(p->x, p->y, p->z, p->gaminv, p->np, gridp(c), keys); }
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
+int permute(wg_ctx* c, const int64_t* perm, const wg_particles* src, const wg_particles* dst) {
+  if (!perm || !src || !dst || src->np != dst->np || src->np < 0) {
+    set_error("wg_particle_permute: bad arguments");
+    return WG_EINVAL;
+  }
+  if (src->np == 0) return WG_OK;
+  { ++c->nlaunch; k_permute<<<cdiv64(src->np, 256), 256, 0, c->stream>>>(perm, src->np, *src, *dst); }
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
 
 }  // namespace wg

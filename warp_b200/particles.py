@@ -49,6 +49,41 @@ class ParticleGroup:
         s.q, s.m, s.w = self.q, self.m, self.w
         return s
 
+    def sort(self, solver, compact=True):
+        """Sorts the particles by cell of the solver's grid
+        (particlesortxyzwithcopy, pywarp90/top.F:5095): keys from the
+        library, a stable sort of the keys, one permutation kernel over the
+        7 arrays. Lost particles (gaminv == 0) end up at the back; with
+        compact=True they are dropped. Order within a cell keeps the old
+        order, so the result is deterministic."""
+        import ctypes
+        n = self.np
+        if n == 0:
+            return
+        keys = torch.empty(n, dtype=torch.int64, device=self.device)
+        s = self.cstruct()
+        _lib.check(_lib.lib.wg_particle_keys(solver._h, ctypes.byref(s), ctypes.c_void_p(keys.data_ptr())))
+        perm = torch.argsort(keys, stable=True)
+        nlive = n
+        if compact:
+            sentinel = (solver.nx + 1) * (solver.ny + 1) * (solver.nz + 1)
+            nlive = int(torch.searchsorted(keys[perm], torch.tensor([sentinel], device=self.device)).item())
+        new = {f: torch.empty(nlive, dtype=torch.float64, device=self.device) for f in FIELDS}
+        d = _lib.Particles()
+        for f in FIELDS:
+            setattr(d, f, new[f].data_ptr())
+        d.np = nlive
+        s.np = nlive
+        d.q, d.m, d.w = self.q, self.m, self.w
+        _lib.check(_lib.lib.wg_particle_permute(solver._h, ctypes.c_void_p(perm.data_ptr()), ctypes.byref(s),
+                                                ctypes.byref(d)))
+        for f in FIELDS:
+            setattr(self, f, new[f])
+        if hasattr(self, "ex") and self.ex.shape[0] != nlive:
+            self.ex = torch.zeros(nlive, dtype=torch.float64, device=self.device)
+            self.ey = torch.zeros_like(self.ex)
+            self.ez = torch.zeros_like(self.ex)
+
     def to_numpy(self):
         return {f: getattr(self, f).cpu().numpy() for f in FIELDS}
 

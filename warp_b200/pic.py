@@ -19,9 +19,6 @@ Workloads (synthetic, seeded):
       electrostatic quadrupole rods (radius 1 cm, +-20 kV) inside the pipe.
 """
 import math
-import time
-
-import torch
 
 from . import conductors as cond
 from .constants import clight, echarge, proton_mass
@@ -63,7 +60,7 @@ class ESPIC:
     """Sets up solver, conductors, lattice and beam of a workload."""
 
     def __init__(self, cfg, precision="fp64", tolkind="mgerror", mgtol=1.e-6, mgmaxiters=100, device="cuda",
-                 particles=None):
+                 particles=None, sort_interval=0):
         self.cfg = cfg
         c = cfg
         self.solver = MultiGridB200(c["nx"], c["ny"], c["nz"], c["xmmin"], c["xmmax"], c["ymmin"], c["ymmax"],
@@ -89,16 +86,22 @@ class ESPIC:
         w = beam_weight(c["current"], c["zmmax"] - c["zmmin"], c["npart"], ekin_ev=c["ekin_ev"])
         self.pgroup = ParticleGroup(particles, q=echarge, m=proton_mass, w=w, device=device)
         self.solver.addpgroup(self.pgroup)
+        self.sort_interval = int(sort_interval)
         self.it = 0
 
     def generate(self):
         """Initial deposit and field solve (w3dgen -> step3d("w3dgen"))."""
+        if self.sort_interval > 0:
+            self.pgroup.sort(self.solver)
         self.solver.loadrho()
         self.solver.solve()
 
     def step(self, n=1):
         for _ in range(n):
             self.solver.advance(self.pgroup, self.dt, prwall=self.cfg["pipe_radius"])
+            if self.sort_interval > 0 and (self.it + 1) % self.sort_interval == 0:
+                # re-sort by cell (and drop lost particles) every sort_interval steps
+                self.pgroup.sort(self.solver)
             self.solver.loadrho()
             self.solver.solve()
             self.it += 1
