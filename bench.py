@@ -157,6 +157,8 @@ def e2e_steps(run, steps):
     pinned memory, advances, deposits, solves and copies them back."""
     import torch
     pg = run.pgroup
+    # the host owns the particle order in this mode: no device-side re-sort
+    run.sort_interval = 0
     names = ("x", "y", "z", "ux", "uy", "uz", "gaminv")
     host = {k: torch.empty(pg.np, dtype=torch.float64, pin_memory=True) for k in names}
     for k in names:
