@@ -246,8 +246,8 @@ struct CondArgs {
 // f3d_mgrid.F:2874-2978): neighbours p[6] = xm,xp,ym,yp,zm,zp, prev = the
 // point's value before the pass. Without lcndbndy the bulk update is used.
 template <typename T>
-__device__ inline T subgrid_value(const CondArgs<T>& C, int par, int i, T pxm, T pxp, T pym, T pyp, T pzm, T pzp,
-                                  T prev, const SorCoef& c, int voltfac_on, int lcndbndy) {
+__device__ __noinline__ T subgrid_value(const CondArgs<T>& C, int par, int i, T pxm, T pxp, T pym, T pyp, T pzm,
+                                        T pzp, T prev, const SorCoef& c, int voltfac_on, int lcndbndy) {
   const T dxsqic = (T)c.cx, dysqic = (T)c.cy, dzsqic = (T)c.cz;
   const T r = C.srhs[par][i];
   if (lcndbndy) {
@@ -396,8 +396,46 @@ struct FusedArgs {
   int usev, voltfac_on, lcndbndy;
 };
 
+// Per-thread load slots of one halo-2 plane tile (FPL elements over FNT
+// threads): the tile-relative offsets are the same for every plane.
+constexpr int FLD = (FPL + FNT - 1) / FNT;
+
+template <typename T, int HALO>
+__device__ inline void fused_relax(T* __restrict__ pc, const T* __restrict__ pm, const T* __restrict__ pp,
+                                   const T* __restrict__ rr, int par, int zr, int x0, int y0, const FusedArgs<T>& a,
+                                   T cx, T cy, T cz, T spm1) {
+  constexpr int W = FTX + 2 * HALO, H = FTY + 2 * HALO, HALF = W / 2;
+  const int nx = a.nx, ny = a.ny;
+#pragma unroll 2
+  for (int i = threadIdx.x; i < HALF * H; i += FNT) {
+    const int ly = 2 - HALO + i / HALF;
+    const int iy = y0 - 2 + ly;
+    const int ixs = x0 - HALO;
+    const int lx = 2 - HALO + ((ixs + iy + zr + par) & 1) + 2 * (i % HALF);
+    const int ix = x0 - 2 + lx;
+    if (ix < 1 || ix > nx - 1 || iy < 1 || iy > ny - 1) continue;
+    const int q = lx + FHX * ly;
+    const T r = rr[q];
+    const T self = pc[q];
+    T nv;
+    if (isbox(r)) {
+      if (Box<T>::interior(r)) continue;  // imposed at load time
+      const uint32_t k2 = Box<T>::idx(r);
+      if (k2 >= (uint32_t)a.C.nsub[par]) {
+        nv = r;  // not a valid record: propagate the NaN
+      } else {
+        nv = subgrid_value<T>(a.C, par, (int)k2, pc[q - 1], pc[q + 1], pc[q - FHX], pc[q + FHX], pm[q], pp[q], self,
+                              a.c, a.voltfac_on, a.lcndbndy);
+      }
+    } else {
+      nv = r + (pc[q - 1] + pc[q + 1]) * cx + (pc[q - FHX] + pc[q + FHX]) * cy + (pm[q] + pp[q]) * cz + spm1 * self;
+    }
+    pc[q] = nv;
+  }
+}
+
 template <typename T>
-__global__ void __launch_bounds__(FNT) k_sor_fused(FusedArgs<T> a) {
+__global__ void __launch_bounds__(FNT, 3) k_sor_fused(FusedArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sp = reinterpret_cast<T*>(smraw);  // [4][FPL] phi planes
   T* sr = sp + 4 * FPL;                 // [3][FPL] rhs planes
@@ -407,6 +445,7 @@ __global__ void __launch_bounds__(FNT) k_sor_fused(FusedArgs<T> a) {
   const int zs = -1 + (int)blockIdx.z * FZC;
   const int ze = min(zs + FZC, nz + 2);
   const T cx = (T)a.c.cx, cy = (T)a.c.cy, cz = (T)a.c.cz, spm1 = (T)a.c.spm1;
+  const size_t pplane = (size_t)(nx + 3) * (ny + 3), rplane = (size_t)(nx + 1) * (ny + 1);
 
   // periodic z: plane nz is the same node set as plane 0 (applyboundaryconditions3d
   // copies 0 -> nz after every half pass), so virtual planes wrap modulo nz
@@ -415,71 +454,66 @@ __global__ void __launch_bounds__(FNT) k_sor_fused(FusedArgs<T> a) {
   auto zupdated = [&](int p) { return a.zper || (p >= 1 && p <= nz - 1); };
   auto mod3 = [](int p) { return ((p % 3) + 3) % 3; };
 
-  // old phi of virtual plane p (interior conductor nodes at their imposed
-  // value, as cond_potmg leaves them) and its rhs
-  auto load = [&](int p) {
-    T* dp = sp + (p & 3) * FPL;
-    T* dr = sr + mod3(p) * FPL;
+  // this thread's load slots: phi offset within a plane (-1 if outside the
+  // padded array) and rhs offset (-1 if not a node)
+  int poff[FLD], roff[FLD];
+#pragma unroll
+  for (int j = 0; j < FLD; ++j) {
+    const int i = tid + j * FNT;
+    poff[j] = -1;
+    roff[j] = -1;
+    if (i < FPL) {
+      const int ix = x0 - 2 + i % FHX, iy = y0 - 2 + i / FHX;
+      if (ix >= -1 && ix <= nx + 1 && iy >= -1 && iy <= ny + 1) {
+        poff[j] = (ix + 1) + (nx + 3) * (iy + 1);
+        if (ix >= 0 && ix <= nx && iy >= 0 && iy <= ny) roff[j] = ix + (nx + 1) * iy;
+      }
+    }
+  }
+  T vreg[FLD], rreg[FLD];
+  // global loads of virtual plane p into registers
+  auto fetch = [&](int p) {
     const bool ok = zexists(p);
     const int zr = wrapz(p);
     const bool zreal = zr >= 0 && zr <= nz;
-    for (int i = tid; i < FPL; i += FNT) {
-      const int lx = i % FHX, ly = i / FHX;
-      const int ix = x0 - 2 + lx, iy = y0 - 2 + ly;
-      T v = (T)0., r = (T)0.;
-      if (ok && ix >= -1 && ix <= nx + 1 && iy >= -1 && iy <= ny + 1) {
-        v = a.in[pix(nx, ny, ix, iy, zr)];
-        if (zreal && ix >= 0 && ix <= nx && iy >= 0 && iy <= ny) {
-          r = a.rhs[rix(nx, ny, ix, iy, zr)];
-          if (isbox(r) && Box<T>::interior(r)) {
-            const uint32_t k = Box<T>::idx(r);
-            if (k < (uint32_t)a.C.nint) v = a.usev ? (T)a.C.ivolt[k] : (T)0.;
-          }
-        }
-      }
-      dp[i] = v;
-      dr[i] = r;
+#pragma unroll
+    for (int j = 0; j < FLD; ++j) {
+      vreg[j] = (T)0.;
+      rreg[j] = (T)0.;
+      if (ok && poff[j] >= 0) vreg[j] = a.in[(size_t)poff[j] + pplane * (size_t)(zr + 1)];
+      if (ok && zreal && roff[j] >= 0) rreg[j] = a.rhs[(size_t)roff[j] + rplane * (size_t)zr];
     }
   };
-
-  // colour `par` (0 red = even ix+iy+iz, 1 black) on virtual plane k, over
-  // the tile grown by `halo` cells
-  auto relax = [&](int k, int par, int halo) {
-    if (!zupdated(k)) return;
-    T* pc = sp + (k & 3) * FPL;
-    const T* pm = sp + ((k - 1) & 3) * FPL;
-    const T* pp = sp + ((k + 1) & 3) * FPL;
-    const T* rr = sr + mod3(k) * FPL;
-    const int zr = wrapz(k);
-    const int w = FTX + 2 * halo, h = FTY + 2 * halo, half = w / 2;
-    for (int i = tid; i < half * h; i += FNT) {
-      const int ly = 2 - halo + i / half;
-      const int iy = y0 - 2 + ly;
-      const int lxs = 2 - halo;
-      const int ixs = x0 - 2 + lxs;
-      const int lx = lxs + (((ixs + iy + zr + par) & 1) ? 1 : 0) + 2 * (i % half);
-      const int ix = x0 - 2 + lx;
-      if (ix < 1 || ix > nx - 1 || iy < 1 || iy > ny - 1) continue;
-      const int q = lx + FHX * ly;
-      const T r = rr[q];
-      const T self = pc[q];
-      T nv;
-      if (isbox(r)) {
-        if (Box<T>::interior(r)) continue;  // imposed at load time
-        const uint32_t k2 = Box<T>::idx(r);
-        if (k2 >= (uint32_t)a.C.nsub[par]) {
-          nv = r;  // not a valid record: propagate the NaN
-        } else {
-          nv = subgrid_value<T>(a.C, par, (int)k2, pc[q - 1], pc[q + 1], pc[q - FHX], pc[q + FHX], pm[q], pp[q], self,
-                                a.c, a.voltfac_on, a.lcndbndy);
+  // registers -> shared slots of plane p; interior conductor nodes take their
+  // imposed value (cond_potmg at the start of sorpass3d)
+  auto deposit = [&](int p) {
+    T* dp = sp + (p & 3) * FPL;
+    T* dr = sr + mod3(p) * FPL;
+#pragma unroll
+    for (int j = 0; j < FLD; ++j) {
+      const int i = tid + j * FNT;
+      if (i < FPL) {
+        T v = vreg[j];
+        const T r = rreg[j];
+        if (isbox(r) && Box<T>::interior(r)) {
+          const uint32_t k = Box<T>::idx(r);
+          if (k < (uint32_t)a.C.nint) v = a.usev ? (T)a.C.ivolt[k] : (T)0.;
         }
-      } else {
-        nv = r + (pc[q - 1] + pc[q + 1]) * cx + (pc[q - FHX] + pc[q + FHX]) * cy + (pm[q] + pp[q]) * cz + spm1 * self;
+        dp[i] = v;
+        dr[i] = r;
       }
-      pc[q] = nv;
     }
   };
-
+  auto red = [&](int k) {
+    if (zupdated(k))
+      fused_relax<T, 1>(sp + (k & 3) * FPL, sp + ((k - 1) & 3) * FPL, sp + ((k + 1) & 3) * FPL, sr + mod3(k) * FPL,
+                        0, wrapz(k), x0, y0, a, cx, cy, cz, spm1);
+  };
+  auto black = [&](int k) {
+    if (zupdated(k))
+      fused_relax<T, 0>(sp + (k & 3) * FPL, sp + ((k - 1) & 3) * FPL, sp + ((k + 1) & 3) * FPL, sr + mod3(k) * FPL,
+                        1, wrapz(k), x0, y0, a, cx, cy, cz, spm1);
+  };
   auto store = [&](int k) {
     const T* pc = sp + (k & 3) * FPL;
     for (int i = tid; i < FTX * FTY; i += FNT) {
@@ -489,21 +523,23 @@ __global__ void __launch_bounds__(FNT) k_sor_fused(FusedArgs<T> a) {
     }
   };
 
-  load(zs - 2);
-  load(zs - 1);
-  load(zs);
+  // prologue: planes zs-2 .. zs+1, red on zs-1
+  for (int p = zs - 2; p <= zs + 1; ++p) {
+    fetch(p);
+    deposit(p);
+  }
   __syncthreads();
-  relax(zs - 1, 0, 1);
+  red(zs - 1);
   for (int k = zs; k <= ze; ++k) {
-    load(k + 1);
+    // the next plane's loads are in flight while this plane is relaxed
+    fetch(k + 2);
+    red(k);
     __syncthreads();
-    relax(k, 0, 1);
+    if (k - 1 >= zs) black(k - 1);
     __syncthreads();
-    if (k - 1 >= zs) {
-      relax(k - 1, 1, 0);
-      __syncthreads();
-      store(k - 1);
-    }
+    if (k - 1 >= zs) store(k - 1);
+    deposit(k + 2);
+    __syncthreads();
   }
 }
 
@@ -982,7 +1018,9 @@ struct Solver {
   }
 };
 
-bool fused_allowed(const int* b) { return b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0 && (b[4] == 0 || b[4] == 2); }
+bool fused_allowed(const int* b) {
+  return b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0 && ((b[4] == 0 && b[5] == 0) || (b[4] == 2 && b[5] == 2));
+}
 
 }  // namespace
 

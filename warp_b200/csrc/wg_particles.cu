@@ -38,62 +38,106 @@ __device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
   return (size_t)(ix + 1) + (size_t)(nx + 3) * ((size_t)(iy + 1) + (size_t)(ny + 3) * (size_t)(iz + 1));
 }
 
-// setrho3ddirect1 (w3d.F:7757-7960): 8 CIC weights per particle, summed per
-// cell within a warp (runs of equal cell index, as sorted particles give),
-// one 64-bit atomic per node per run.
-__global__ void __launch_bounds__(256) k_deposit(const double* __restrict__ xp, const double* __restrict__ yp,
-                                                 const double* __restrict__ zp, const double* __restrict__ gaminv,
-                                                 int64_t np, GridP g, unsigned long long* __restrict__ acc) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  int key = -1;
-  unsigned long long w[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) w[k] = 0ull;
-  if (i < np && gaminv[i] != 0.) {
-    const double dxi = 1. / g.dx, dyi = 1. / g.dy, dzi = 1. / g.dz;
-    int ii, jj, kk;
-    double u1, v1, w1;
-    cellfrac((xp[i] - g.xmmin) * dxi, g.nx, ii, u1);
-    cellfrac((yp[i] - g.ymmin) * dyi, g.ny, jj, v1);
-    cellfrac((zp[i] - g.zgrid - g.zmmin) * dzi, g.nz, kk, w1);
-    const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
-    key = ii + (g.nx + 1) * (jj + (g.ny + 1) * kk);
-    w[0] = (unsigned long long)llrint(u0 * v0 * w0 * kFixScale);
-    w[1] = (unsigned long long)llrint(u1 * v0 * w0 * kFixScale);
-    w[2] = (unsigned long long)llrint(u0 * v1 * w0 * kFixScale);
-    w[3] = (unsigned long long)llrint(u1 * v1 * w0 * kFixScale);
-    w[4] = (unsigned long long)llrint(u0 * v0 * w1 * kFixScale);
-    w[5] = (unsigned long long)llrint(u1 * v0 * w1 * kFixScale);
-    w[6] = (unsigned long long)llrint(u0 * v1 * w1 * kFixScale);
-    w[7] = (unsigned long long)llrint(u1 * v1 * w1 * kFixScale);
+// setrho3ddirect1 (w3d.F:7757-7960) with 64-bit fixed-point weights. A CTA
+// takes a chunk of DEP_NT*DEP_PPT consecutive particles. Their 8 CIC weights
+// per node are first summed over runs of equal cell within each warp (sorted
+// particles give long runs), then into a shared-memory copy of the chunk's
+// bounding box of nodes, which is added to the global accumulator once; when
+// the box is larger than DEP_BOX nodes (unsorted particles) the run sums go
+// straight to global memory. Integer adds commute, so the result does not
+// depend on any of these orders.
+constexpr int DEP_NT = 256, DEP_PPT = 16, DEP_BOX = 4096;
+
+__device__ inline bool dep_cell(const double* xp, const double* yp, const double* zp, const double* gaminv,
+                                int64_t i, int64_t np, const GridP& g, int& ii, int& jj, int& kk, double& u1,
+                                double& v1, double& w1) {
+  if (i >= np || gaminv[i] == 0.) return false;
+  cellfrac((xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, u1);
+  cellfrac((yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, v1);
+  cellfrac((zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, w1);
+  return true;
+}
+
+__global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ xp, const double* __restrict__ yp,
+                                                    const double* __restrict__ zp,
+                                                    const double* __restrict__ gaminv, int64_t np, GridP g,
+                                                    unsigned long long* __restrict__ acc) {
+  __shared__ unsigned long long box[DEP_BOX];
+  __shared__ int bmin[3], bmax[3];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int64_t base = (int64_t)blockIdx.x * (DEP_NT * DEP_PPT);
+  if (tid < 3) {
+    bmin[tid] = 0x7fffffff;
+    bmax[tid] = -1;
   }
-  // segmented suffix sums over runs of equal key within the warp
-  const int knext = __shfl_down_sync(0xffffffffu, key, 1);
-  const bool tail = (lane == 31) || (knext != key);
-  const unsigned tails = __ballot_sync(0xffffffffu, tail);
-  const int seg_end = __ffs(tails & (0xffffffffu << lane)) - 1;
-  const int kprev = __shfl_up_sync(0xffffffffu, key, 1);
-  const bool head = (lane == 0) || (kprev != key);
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      unsigned long long t = __shfl_down_sync(0xffffffffu, w[k], off);
-      if (lane + off <= seg_end) w[k] += t;
+  __syncthreads();
+  int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-1, -1, -1};
+  for (int j = 0; j < DEP_PPT; ++j) {
+    int c[3];
+    double f1, f2, f3;
+    if (dep_cell(xp, yp, zp, gaminv, base + tid + (int64_t)j * DEP_NT, np, g, c[0], c[1], c[2], f1, f2, f3))
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = min(lo[d], c[d]);
+        hi[d] = max(hi[d], c[d]);
+      }
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (hi[d] >= 0) {
+      atomicMin(&bmin[d], lo[d]);
+      atomicMax(&bmax[d], hi[d]);
     }
   }
-  if (head && key >= 0) {
+  __syncthreads();
+  // node box [bmin, bmax+1] in each direction
+  const int ox = bmin[0], oy = bmin[1], oz = bmin[2];
+  const int bx = bmax[0] - ox + 2, by = bmax[1] - oy + 2, bz = bmax[2] - oz + 2;
+  const bool any = bmax[0] >= 0;
+  const bool use_box = any && (long long)bx * by * bz <= DEP_BOX;
+  if (use_box)
+    for (int i = tid; i < bx * by * bz; i += DEP_NT) box[i] = 0ull;
+  __syncthreads();
+  if (any) {
     const int sx = 1, sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
-    unsigned long long* a = acc + key;
-    atomicAdd(a, w[0]);
-    atomicAdd(a + sx, w[1]);
-    atomicAdd(a + sy, w[2]);
-    atomicAdd(a + sx + sy, w[3]);
-    atomicAdd(a + sz, w[4]);
-    atomicAdd(a + sx + sz, w[5]);
-    atomicAdd(a + sy + sz, w[6]);
-    atomicAdd(a + sx + sy + sz, w[7]);
+    for (int j = 0; j < DEP_PPT; ++j) {
+      int ii = 0, jj = 0, kk = 0;
+      double u1 = 0., v1 = 0., w1 = 0.;
+      const bool live = dep_cell(xp, yp, zp, gaminv, base + tid + (int64_t)j * DEP_NT, np, g, ii, jj, kk, u1, v1, w1);
+      const int key = live ? ii + (g.nx + 1) * (jj + (g.ny + 1) * kk) : -1;
+      const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+      const bool tail = (lane == 31) || (knext != key);
+      const unsigned tails = __ballot_sync(0xffffffffu, tail);
+      const int seg_end = __ffs(tails & (0xffffffffu << lane)) - 1;
+      const int kprev = __shfl_up_sync(0xffffffffu, key, 1);
+      const bool head = ((lane == 0) || (kprev != key)) && live;
+      const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+#pragma unroll
+      for (int n = 0; n < 8; ++n) {
+        const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
+        const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
+        unsigned long long v = live ? (unsigned long long)llrint(wgt * kFixScale) : 0ull;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const unsigned long long t = __shfl_down_sync(0xffffffffu, v, off);
+          if (lane + off <= seg_end) v += t;
+        }
+        if (head && v) {
+          if (use_box)
+            atomicAdd(&box[(ii + dx - ox) + bx * ((jj + dy - oy) + by * (kk + dz - oz))], v);
+          else
+            atomicAdd(acc + key + dx * sx + dy * sy + dz * sz, v);
+        }
+      }
+    }
+  }
+  if (use_box) {
+    __syncthreads();
+    for (int i = tid; i < bx * by * bz; i += DEP_NT) {
+      const unsigned long long v = box[i];
+      if (v) {
+        const int lx = i % bx, ly = (i / bx) % by, lz = i / (bx * by);
+        atomicAdd(acc + (ox + lx) + (g.nx + 1) * ((oy + ly) + (g.ny + 1) * (oz + lz)), v);
+      }
+    }
   }
 }
 
@@ -394,7 +438,7 @@ int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
   if (p->np > 0) {
     const int64_t maxblocks = 2147483647LL;
     if (cdiv64(p->np, 256) > maxblocks) { set_error("wg_deposit: too many particles"); return WG_ETOOLARGE; }
-    { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<<<cdiv64(p->np, 256), 256, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, c->racc); c->prof_end(pe); }
+    { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, c->racc); c->prof_end(pe); }
   }
   double gg = p->w * p->q;
   gg = gg / c->dx;
