@@ -120,9 +120,6 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
     run.step(warmup)
     stream = torch.cuda.current_stream()
     h = s._h
-    if prof:
-        mask = (1 << _lib.PROF_SOR0) | (1 << _lib.PROF_ADVANCE) | (1 << _lib.PROF_DEPOSIT) | (1 << _lib.PROF_RESID0)
-        _lib.check(_lib.lib.wg_prof_enable(h, mask))
     n0 = _lib.ctypes.c_int64()
     _lib.check(_lib.lib.wg_launch_count(h, _lib.ctypes.byref(n0)))
     vc = 0
@@ -140,6 +137,13 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
     out = {"ms_per_step": ms / steps, "vcycles_per_solve": vc / steps, "launches": n1.value - n0.value,
            "live": run.pgroup.nlive(), "relres": s.relres}
     if prof:
+        # kernel durations from CUDA events on the launching stream, over the
+        # same number of further steps (event timing runs the V-cycles kernel
+        # by kernel instead of from the captured graph)
+        mask = (1 << _lib.PROF_SOR0) | (1 << _lib.PROF_ADVANCE) | (1 << _lib.PROF_DEPOSIT) | (1 << _lib.PROF_RESID0)
+        _lib.check(_lib.lib.wg_prof_enable(h, mask))
+        for _ in range(steps):
+            run.step()
         kinds = {"sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE, "deposit": _lib.PROF_DEPOSIT,
                  "resid0": _lib.PROF_RESID0}
         out["kernels"] = {}

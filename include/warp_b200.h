@@ -54,7 +54,11 @@ typedef struct {
                       1: FP32 V-cycles inside FP64 defect correction */
   int tolkind;     /* 0: mgerror = max|dphi| in volts (reference criterion)
                       1: relative residual max|rhs-A phi|/max|rhs| */
+  int flags;       /* WG_SOLVE_* bits below */
 } wg_solve_opts;
+
+#define WG_SOLVE_GRAPH 1  /* replay each V-cycle from a captured CUDA graph */
+#define WG_SOLVE_FUSED 2  /* fused out-of-place red+black sweep where allowed */
 
 typedef struct {
   int mgiters;      /* V-cycles done */

@@ -90,7 +90,18 @@ void free_conductor_data(wg_ctx* c) {
   }
 }
 
+void free_graphs(wg_ctx* c) {
+  for (int i = 0; i < 2; ++i) {
+    if (c->vgraph[i]) cudaGraphExecDestroy(c->vgraph[i]);
+    c->vgraph[i] = nullptr;
+    c->vgraph_key[i] = 0ull;
+  }
+}
+
 void free_all(wg_ctx* c) {
+  free_graphs(c);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  c->cap_stream = nullptr;
   free_conductor_data(c);
   for (auto& e : c->prof_ev) cudaEventDestroy(e);
   c->prof_ev.clear();
@@ -124,6 +135,8 @@ int upload(T** d, const T* h, size_t n) {
 }
 
 int upload_conductors(wg_ctx* c) {
+  free_graphs(c);
+  c->cond_version += 1;
   free_conductor_data(c);
   HostConductors& C = c->cond;
   for (size_t l = 0; l < c->lv.size(); ++l) {
@@ -161,6 +174,8 @@ using namespace wg;
 
 int ensure_fp32_impl(wg_ctx* c) {
   if (c->have_fp32) return WG_OK;
+  free_graphs(c);
+  c->cond_version += 1;
   for (Level& L : c->lv) {
     WG_TRY(dalloc(&L.phif, L.np));
     WG_TRY(dalloc(&L.phif2, L.np));

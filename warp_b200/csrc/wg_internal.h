@@ -115,8 +115,14 @@ struct wg_ctx {
   int nzl = -1;
   double zlmin = 0., dzl = 1.;
   bool have_fp32 = false;
-  // kernels launched by this context (cumulative)
+  // kernels launched by this context (cumulative; a graph replay counts its kernels)
   long long nlaunch = 0;
+  // captured V-cycles (index 0: FP64, 1: FP32), valid for vgraph_key
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t vgraph[2] = {nullptr, nullptr};
+  unsigned long long vgraph_key[2] = {0ull, 0ull};
+  long long vgraph_kernels[2] = {0, 0};
+  long long cond_version = 1;  // bumped whenever device conductor arrays change
   // CUDA-event timing of selected kernel kinds (WG_PROF_* bits)
   int prof_mask = 0;
   std::vector<cudaEvent_t> prof_ev;  // start/stop pairs

@@ -829,7 +829,10 @@ struct Solver {
   const wg_solve_opts* o;
   Bnd B;
   cudaStream_t s;
-  bool fused_ok;  // boundary types allow the fused sweep
+  bool fused_ok;  // boundary types and options allow the fused sweep
+  bool capturing = false;
+
+  int prof_begin(int l, int kind, double units) { return (!capturing && l == 0) ? c->prof_begin(kind, units) : -1; }
 
   template <typename T>
   void bc(Level& L, T* u, bool lwithdirichlet) {
@@ -894,7 +897,7 @@ struct Solver {
       dim3 grd(cdiv(L.d.nx + 3, FTX), cdiv(L.d.ny + 3, FTY), cdiv(L.d.nz + 3, FZC));
       const size_t smem = 7 * FPL * sizeof(T);
       ++c->nlaunch;
-      int pe = (l == 0) ? c->prof_begin(WG_PROF_SOR0, 2. * (double)L.nr) : -1;
+      int pe = prof_begin(l, WG_PROF_SOR0, 2. * (double)L.nr);
       k_sor_fused<T><<<grd, FNT, smem, s>>>(a);
       c->prof_end(pe);
       std::swap(Arr<T>::phi(L), Arr<T>::phi2(L));
@@ -914,7 +917,7 @@ struct Solver {
       if (nyr > 0 && nzr > 0 && nhalf > 0) {
         dim3 blk(32, 8), grd(cdiv(nhalf, 32), cdiv(nyr, 8), nzr);
         ++c->nlaunch;
-        int pe = (l == 0) ? c->prof_begin(WG_PROF_SOR0, (double)L.nr) : -1;
+        int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
         k_sor_bulk<T><<<grd, blk, 0, s>>>(phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin,
                                           parity, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1);
         c->prof_end(pe);
@@ -944,7 +947,7 @@ struct Solver {
     dim3 blk(32, 8), grd(cdiv(L.d.nx + 1 + 2 * g, 32), cdiv(L.d.ny + 1 + 2 * g, 8), L.d.nz + 1 + 2 * g);
     {
       ++c->nlaunch;
-      int pe = (l == 0) ? c->prof_begin(WG_PROF_RESID0, (double)L.nr) : -1;
+      int pe = prof_begin(l, WG_PROF_RESID0, (double)L.nr);
       k_residual<T, MODE, TO><<<grd, blk, 0, s>>>(phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
                                                   R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
                                                   (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst),
@@ -1018,6 +1021,47 @@ struct Solver {
   }
 };
 
+// The V-cycle of precision T from a captured CUDA graph (recaptured when the
+// options or the conductor arrays change), or launched kernel by kernel.
+template <typename T>
+int run_vcycle(Solver& S, bool usev) {
+  wg_ctx* c = S.c;
+  const wg_solve_opts* o = S.o;
+  if (!(o->flags & WG_SOLVE_GRAPH) || c->prof_mask) {
+    S.vcycle<T>(0, usev);
+    return WG_OK;
+  }
+  const int gi = sizeof(T) == 8 ? 0 : 1;
+  unsigned long long mp;
+  memcpy(&mp, &o->mgparam, sizeof(mp));
+  unsigned long long key = mp ^ ((unsigned long long)o->mgmaxlevels << 1) ^ ((unsigned long long)o->downpasses << 9) ^
+                           ((unsigned long long)o->uppasses << 17) ^ ((unsigned long long)o->lcndbndy << 25) ^
+                           ((unsigned long long)S.fused_ok << 27) ^ ((unsigned long long)usev << 28) ^
+                           ((unsigned long long)c->cond_version << 32);
+  if (!c->vgraph[gi] || c->vgraph_key[gi] != key) {
+    if (c->vgraph[gi]) cudaGraphExecDestroy(c->vgraph[gi]);
+    c->vgraph[gi] = nullptr;
+    if (!c->cap_stream) WG_TRY_CUDA(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+    Solver G = S;
+    G.s = c->cap_stream;
+    G.capturing = true;
+    const long long n0 = c->nlaunch;
+    cudaGraph_t g;
+    WG_TRY_CUDA(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+    G.vcycle<T>(0, usev);
+    WG_TRY_CUDA(cudaStreamEndCapture(c->cap_stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&c->vgraph[gi], g, 0);
+    cudaGraphDestroy(g);
+    WG_TRY_CUDA(e);
+    c->vgraph_key[gi] = key;
+    c->vgraph_kernels[gi] = c->nlaunch - n0;
+    c->nlaunch = n0;
+  }
+  WG_TRY_CUDA(cudaGraphLaunch(c->vgraph[gi], S.s));
+  c->nlaunch += c->vgraph_kernels[gi];
+  return WG_OK;
+}
+
 bool fused_allowed(const int* b) {
   return b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0 && ((b[4] == 0 && b[5] == 0) || (b[4] == 2 && b[5] == 2));
 }
@@ -1044,7 +1088,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   }
   Solver S{c, o, {}, c->stream, false};
   for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
-  S.fused_ok = fused_allowed(S.B.b);
+  S.fused_ok = fused_allowed(S.B.b) && (o->flags & WG_SOLVE_FUSED);
   cudaStream_t s = c->stream;
   Level& L0 = c->lv[0];
   double* user_phi = L0.phi;
@@ -1079,7 +1123,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       if (it >= o->mgmaxiters) break;
       if (o->tolkind == 0)
         WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      S.vcycle<double>(0, true);
+      WG_TRY(run_vcycle<double>(S, true));
       it += 1;
       if (o->tolkind == 0) {
         WG_TRY_CUDA(cudaMemsetAsync(red, 0, sizeof(unsigned long long), s));
@@ -1107,7 +1151,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       if (it >= o->mgmaxiters) break;
       S.box<float>(0);
       WG_TRY_CUDA(cudaMemsetAsync(L0.phif, 0, L0.np * sizeof(float), s));
-      S.vcycle<float>(0, false);
+      WG_TRY(run_vcycle<float>(S, false));
       WG_TRY_CUDA(cudaMemsetAsync(red, 0, sizeof(unsigned long long), s));
       { ++c->nlaunch; k_add_corr<<<grdp, blk, 0, s>>>(L0.phi, L0.phif, d.nx, d.ny, d.nz, red); }
       S.bc<double>(L0, L0.phi, false);
@@ -1131,7 +1175,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
 }
 
 int relresidual(wg_ctx* c, double mgparam, double* out) {
-  wg_solve_opts o{mgparam, 0., 0, 101, 1, 1, 1, 0, 1};
+  wg_solve_opts o{mgparam, 0., 0, 101, 1, 1, 1, 0, 1, 0};
   Solver S{c, &o, {}, c->stream, false};
   for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
   cudaStream_t s = c->stream;

@@ -48,7 +48,7 @@ class MultiGridB200(FieldSolver):
     def __init__(self, nx, ny, nz, xmmin, xmmax, ymmin, ymmax, zmmin, zmmax, bounds=(0, 0, 0, 0, 0, 0),
                  mgparam=1.2, mgtol=1.e-6, mgmaxiters=100, mgmaxlevels=101, downpasses=1, uppasses=1,
                  lcndbndy=True, icndbndy=2, mgform=1, mgverbose=0, precision="fp64", tolkind="mgerror",
-                 device=None):
+                 device=None, use_graphs=True, fused_sweep=False):
         if icndbndy != 2:
             raise ValueError("MultiGridB200 supports icndbndy = 2 (quadratic subgrid stencil) only")
         if mgform != 1:
@@ -71,6 +71,8 @@ class MultiGridB200(FieldSolver):
         self.mgmaxlevels, self.downpasses, self.uppasses = int(mgmaxlevels), int(downpasses), int(uppasses)
         self.lcndbndy, self.icndbndy, self.mgform, self.mgverbose = bool(lcndbndy), icndbndy, mgform, mgverbose
         self.precision, self.tolkind = precision, tolkind
+        # replay V-cycles from captured CUDA graphs; fused out-of-place sweep
+        self.use_graphs, self.fused_sweep = bool(use_graphs), bool(fused_sweep)
         self.mgiters, self.mgerror, self.relres, self.converged = 0, 0., -1., True
         self.conductordatalist = []
         self._conductors_installed = False
@@ -89,8 +91,9 @@ class MultiGridB200(FieldSolver):
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            _lib.lib.wg_destroy(h)
+        lib = getattr(_lib, "lib", None)
+        if h and lib is not None:
+            lib.wg_destroy(h)
             self._h = None
 
     # -- plumbing -----------------------------------------------------------
@@ -229,9 +232,10 @@ class MultiGridB200(FieldSolver):
             _lib.check(_lib.lib.wg_finalize_rho(self._h))
 
     def _opts(self):
+        flags = (_lib.SOLVE_GRAPH if self.use_graphs else 0) | (_lib.SOLVE_FUSED if self.fused_sweep else 0)
         return _lib.SolveOpts(self.mgparam, self.mgtol, self.mgmaxiters, self.mgmaxlevels, self.downpasses,
                               self.uppasses, int(self.lcndbndy), _PRECISION[self.precision],
-                              _TOLKIND[self.tolkind])
+                              _TOLKIND[self.tolkind], flags)
 
     def solve(self, iwhich=0):
         """dosolve -> multigrid3dsolve (multigrid.py:846-917,
