@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-vcycles", type=float, default=None)
     ap.add_argument("--ref-sample", type=int, default=1_000_000)
+    ap.add_argument("--npart", type=int, default=None, help="override the particle count (profiling runs)")
     return ap.parse_args()
 
 
@@ -235,7 +236,7 @@ def main():
     args = parse()
     rank, world, local = dist_env()
     from warp_b200 import pic
-    cfg = pic.workload(args.workload)
+    cfg = pic.workload(args.workload) if args.npart is None else pic.workload(args.workload, npart=args.npart)
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -294,7 +295,7 @@ def main():
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         ms_head = float(t.item())
     value = world * 1000.0 / ms_head
-    e2e_ms, h2d, d2h = e2e_steps(head_run, args.e2e_steps)
+    e2e_ms, h2d, d2h = e2e_steps(head_run, args.e2e_steps) if args.e2e_steps > 0 else (float("nan"), 0, 0)
     if world > 1:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)

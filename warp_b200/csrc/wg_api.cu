@@ -119,6 +119,7 @@ void free_all(wg_ctx* c) {
   dfree(c->rho);
   dfree(c->racc);
   dfree(c->dred);
+  dfree(c->dslot);
   dfree(c->dmom);
   dfree(c->czs);
   dfree(c->cze);
@@ -240,6 +241,7 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
   if (rc == WG_OK) rc = dalloc(&c->rho, L0.nr);
   if (rc == WG_OK) rc = dalloc(&c->racc, L0.nr);
   if (rc == WG_OK) rc = dalloc(&c->dred, (size_t)4);
+  if (rc == WG_OK) rc = dalloc(&c->dslot, (size_t)3 * 32 * 16);
   if (rc == WG_OK) {
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, c->device);

@@ -105,6 +105,7 @@ struct wg_ctx {
   unsigned long long* racc = nullptr; // fixed-point deposit accumulator
   // reductions: [0] max|dphi| bits, [1] max|res| bits, [2] max|rhs| bits, [3] flags
   unsigned long long* dred = nullptr;
+  unsigned long long* dslot = nullptr; // per-block max slots of [0..2], folded into dred
   unsigned long long* hred = nullptr;  // pinned host copy
   double* dmom = nullptr;              // moment partial sums
   int mom_blocks = 0;

@@ -86,8 +86,15 @@ __device__ inline double warp_max(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
-// Block-wide max folded into *addr (all threads must call).
-__device__ inline void block_max_to(unsigned long long* addr, double v) {
+// Max reductions land in one of kRedSlots slots, kRedStride words apart
+// (separate cache lines), so that the blocks of a large grid do not all
+// serialise on one address; k_fold_max combines the slots.
+constexpr int kRedSlots = 32, kRedStride = 16, kRedQ = kRedSlots * kRedStride;
+
+// Block-wide max folded into the slot of this block under `base` (all
+// threads must call). The atomic is skipped when the slot already holds a
+// larger value.
+__device__ inline void block_max_to(unsigned long long* base, double v) {
   __shared__ double sm[32];
   v = warp_max(v);
   int lane = threadIdx.x & 31, wid = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
@@ -97,8 +104,26 @@ __device__ inline void block_max_to(unsigned long long* addr, double v) {
   if (wid == 0) {
     double w = (lane < nw) ? sm[lane] : 0.;
     w = warp_max(w);
-    if (lane == 0 && w > 0.) atomic_max_nonneg(addr, w);
+    if (lane == 0 && w > 0.) {
+      const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+      unsigned long long* addr = base + kRedStride * (bid % kRedSlots);
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(w);
+      if (bits > *(volatile unsigned long long*)addr) atomic_max_nonneg(addr, w);
+    }
   }
+}
+
+// out[q] = max over the slots of reduction q (q < nq).
+__global__ void k_fold_max(const unsigned long long* __restrict__ slots, unsigned long long* __restrict__ out,
+                           int nq) {
+  const int q = threadIdx.x / 32, lane = threadIdx.x & 31;
+  if (q >= nq) return;
+  unsigned long long v = slots[q * kRedQ + kRedStride * lane];
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = t > v ? t : v;
+  }
+  if (lane == 0) out[q] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -998,7 +1023,15 @@ struct Solver {
     for (int i = 0; i < o->uppasses; ++i) sorpass<T>(l, usev);
   }
 
+  // reduction slot area of quantity q: 0 max|dphi|, 1 max|res|, 2 max|rhs|
+  unsigned long long* slotq(int q) { return c->dslot + (size_t)q * kRedQ; }
+  int clear_slots(int q) {
+    WG_TRY_CUDA(cudaMemsetAsync(slotq(q), 0, kRedQ * sizeof(unsigned long long), s));
+    return WG_OK;
+  }
+
   int fetch_red(double* out, int n) {
+    { ++c->nlaunch; k_fold_max<<<1, 96, 0, s>>>(c->dslot, c->dred, 3); }
     WG_TRY_CUDA(cudaMemcpyAsync(c->hred, c->dred, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     WG_TRY_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n; ++i) {
@@ -1095,9 +1128,9 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   const LevelDims& d = L0.d;
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = o->mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
-  unsigned long long* red = c->dred;
-  WG_TRY_CUDA(cudaMemsetAsync(red, 0, 4 * sizeof(unsigned long long), s));
-  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, red + 2, red + 3); }
+  WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
+  WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
+  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
   S.box<double>(0);
   S.bc<double>(L0, L0.phi, false);
   dim3 blk(32, 8), grdn(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1);
@@ -1114,8 +1147,8 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   if (o->precision == 0) {
     for (;;) {
       if (o->tolkind == 1) {
-        WG_TRY_CUDA(cudaMemsetAsync(red + 1, 0, sizeof(unsigned long long), s));
-        S.residual<double, 1, double>(0, L0.phi, nullptr, false, true, red + 1);
+        WG_TRY(S.clear_slots(1));
+        S.residual<double, 1, double>(0, L0.phi, nullptr, false, true, S.slotq(1));
         WG_TRY(S.fetch_red(rv, 3));
         relres = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
         if (relres <= o->mgtol) { conv = true; break; }
@@ -1126,8 +1159,8 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       WG_TRY(run_vcycle<double>(S, true));
       it += 1;
       if (o->tolkind == 0) {
-        WG_TRY_CUDA(cudaMemsetAsync(red, 0, sizeof(unsigned long long), s));
-        { ++c->nlaunch; k_maxdiff<<<grdn, blk, 0, s>>>(c->phisave, L0.phi, d.nx, d.ny, red); }
+        WG_TRY(S.clear_slots(0));
+        { ++c->nlaunch; k_maxdiff<<<grdn, blk, 0, s>>>(c->phisave, L0.phi, d.nx, d.ny, S.slotq(0)); }
         WG_TRY(S.fetch_red(rv, 1));
         err = rv[0];
         if (!(err > o->mgtol)) { conv = true; break; }
@@ -1141,8 +1174,8 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
         k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(L0.phi, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);
       }
       S.neumann_int<double>(L0, L0.phi);
-      WG_TRY_CUDA(cudaMemsetAsync(red + 1, 0, sizeof(unsigned long long), s));
-      S.residual<double, 2, float>(0, L0.phi, L0.rhsf, true, true, red + 1);
+      WG_TRY(S.clear_slots(1));
+      S.residual<double, 2, float>(0, L0.phi, L0.rhsf, true, true, S.slotq(1));
       if (o->tolkind == 1 || it >= o->mgmaxiters) {
         WG_TRY(S.fetch_red(rv, 3));
         relres = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
@@ -1152,8 +1185,8 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       S.box<float>(0);
       WG_TRY_CUDA(cudaMemsetAsync(L0.phif, 0, L0.np * sizeof(float), s));
       WG_TRY(run_vcycle<float>(S, false));
-      WG_TRY_CUDA(cudaMemsetAsync(red, 0, sizeof(unsigned long long), s));
-      { ++c->nlaunch; k_add_corr<<<grdp, blk, 0, s>>>(L0.phi, L0.phif, d.nx, d.ny, d.nz, red); }
+      WG_TRY(S.clear_slots(0));
+      { ++c->nlaunch; k_add_corr<<<grdp, blk, 0, s>>>(L0.phi, L0.phif, d.nx, d.ny, d.nz, S.slotq(0)); }
       S.bc<double>(L0, L0.phi, false);
       it += 1;
       if (o->tolkind == 0) {
@@ -1184,7 +1217,8 @@ int relresidual(wg_ctx* c, double mgparam, double* out) {
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
   WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
-  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, c->dred + 2, c->dred + 3); }
+  WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
+  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
   S.box<double>(0);
   // residual of a copy with the conductor voltages imposed, as the solver sees it
   WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -1192,7 +1226,7 @@ int relresidual(wg_ctx* c, double mgparam, double* out) {
     ++c->nlaunch;
     k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);
   }
-  S.residual<double, 1, double>(0, c->phisave, nullptr, false, true, c->dred + 1);
+  S.residual<double, 1, double>(0, c->phisave, nullptr, false, true, S.slotq(1));
   double rv[4];
   WG_TRY(S.fetch_red(rv, 3));
   *out = rv[2] > 0. ? rv[1] / rv[2] : rv[1];
