@@ -185,6 +185,21 @@ int wg_prof_read(wg_ctx* ctx, int kind, double* total_ms, int64_t* launches, dou
 /* Number of kernels this context has launched since it was created. */
 int wg_launch_count(wg_ctx* ctx, int64_t* n);
 
+/* ---- learned warm start: BF16 tensor-core 3x3x3 convolutions (no
+ * reference counterpart: WARP has no learned components) ------------------ */
+
+/* y[v][yoff+co] = relu?(bias[co] + sum_{t,ci} x[v+off_t][ci] * w[t][co][ci]),
+ * optionally multiplied by (mask[v][co] > 0). x: [D][H][W][cin] bf16,
+ * w: [27][cout][cin] bf16 (tap t = 9*(dz+1) + 3*(dy+1) + (dx+1)), bias fp32 or
+ * NULL, y: [D][H][W][ystride] bf16. cin, cout multiples of 16, cout <= 128.
+ * Zero padding outside the box. *err is set non-zero if a wait timed out. */
+int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
+                 int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream);
+/* dw[t][co][ci] += sum_v dy[v][co] * x[v+off_t][ci] with channel-major
+ * operands xT: [cin][D][H][W], dyT: [cout][D][H][W] (bf16), dw fp32. */
+int wg_conv3_wgrad(const void* xT, const void* dyT, int D, int H, int W, int cin, int cout, float* dw, int* err,
+                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,9 @@ SIGNATURES = {
     "wg_launch_count": [_vp, _i64p],
     "wg_particle_keys": [_vp, ctypes.POINTER(Particles), _vp],
     "wg_particle_permute": [_vp, _vp, ctypes.POINTER(Particles), ctypes.POINTER(Particles)],
+    "wg_conv3_fwd": [_vp] + [_c.c_int] * 4 + [_vp, _vp, _c.c_int, _vp, _c.c_int, _c.c_int, _vp, _c.c_int, _c.c_int,
+                     _vp, _vp],
+    "wg_conv3_wgrad": [_vp, _vp] + [_c.c_int] * 5 + [_vp, _vp, _vp],
 }
 
 PROF_SOR0, PROF_DEPOSIT, PROF_ADVANCE, PROF_RESID0 = 0, 1, 2, 3

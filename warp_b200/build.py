@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwarp_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["wg_api.cu", "wg_mg.cu", "wg_particles.cu", "wg_conductors.cpp"]
+SOURCES = ["wg_api.cu", "wg_mg.cu", "wg_particles.cu", "wg_conductors.cpp", "wg_unet.cu"]
 
 
 def nvcc():
