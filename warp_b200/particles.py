@@ -114,6 +114,24 @@ def semigaussian(n, seed=0, radius=2e-3, mismatch=0.0, angle_rms=5e-3, zmin=0.0,
     return {"x": x, "y": y, "z": z, "ux": xp * vz, "uy": yp * vz, "uz": uz, "gaminv": np.ones(n)}
 
 
+def semigaussian_device(n, generator, radius=2e-3, mismatch=0.0, angle_rms=5e-3, zmin=0.0, zmax=1.0,
+                        ekin_ev=1e6, mass=proton_mass, device="cuda"):
+    """semigaussian() drawn on the device from a seeded torch.Generator (used
+    to generate many training beams quickly). Returns a dict of tensors."""
+    gamma = 1. + ekin_ev * echarge / (mass * clight * clight)
+    vz = math.sqrt(1. - 1. / (gamma * gamma)) * clight
+    kw = dict(generator=generator, device=device, dtype=torch.float64)
+    r = torch.sqrt(torch.rand(n, **kw))
+    th = 2. * math.pi * torch.rand(n, **kw)
+    x = radius * (1. + mismatch) * r * torch.cos(th)
+    y = radius * (1. - mismatch) * r * torch.sin(th)
+    z = zmin + (zmax - zmin) * torch.rand(n, **kw)
+    ux = angle_rms * torch.randn(n, **kw) * vz
+    uy = angle_rms * torch.randn(n, **kw) * vz
+    return {"x": x, "y": y, "z": z, "ux": ux, "uy": uy, "uz": torch.full((n,), vz, **{k: kw[k] for k in ("device", "dtype")}),
+            "gaminv": torch.ones(n, device=device, dtype=torch.float64)}
+
+
 def beam_weight(current, length, n, ekin_ev=1e6, mass=proton_mass, charge=echarge):
     """Real particles per macroparticle for a beam of `current` (A) filling
     `length` (m): w = I L / (q v N)."""

@@ -150,31 +150,50 @@ class UNet3D(torch.nn.Module):
 
 
 class WarmStart:
-    """Network input/output scaling around the solver's arrays: the network
-    sees rho and phi^(n-1) on the nodes 0..nx-1, 0..ny-1, 0..nz-1 scaled to
-    O(1), and predicts the change phi^n - phi^(n-1) in units of max|phi^(n-1)|."""
+    """Scaling around the solver's arrays. The network sees, on the nodes
+    0..nx-1, 0..ny-1, 0..nz-1 (z, y, x order), phi^(n-1)/s and
+    rho * rho_factor / s with s = max|phi^(n-1)|, and predicts
+    out_scale * (phi^n - phi^(n-1)) / s. With rho_factor ~ dx^2/eps0 both
+    inputs are O(1) whatever the beam current."""
 
-    def __init__(self, net, rho_scale):
+    def __init__(self, net, rho_factor, out_scale=30.0):
         self.net = net
-        self.rho_scale = float(rho_scale)
+        self.rho_factor = float(rho_factor)
+        self.out_scale = float(out_scale)
+
+    def _core(self, rho, phi):
+        return rho[:-1, :-1, :-1].permute(2, 1, 0), phi[1:-2, 1:-2, 1:-2].permute(2, 1, 0)
 
     def inputs(self, rho, phi_prev):
-        """rho: solver.rho [nx+1,ny+1,nz+1] (x fastest, Fortran view);
-        phi_prev: solver.phi [nx+3,ny+3,nz+3]. Returns ([D,H,W,16] bf16, s)."""
-        r = rho[:-1, :-1, :-1].permute(2, 1, 0)
-        p = phi_prev[1:-2, 1:-2, 1:-2].permute(2, 1, 0)
+        """rho: solver.rho [nx+1,ny+1,nz+1] (Fortran view); phi_prev: solver.phi
+        [nx+3,ny+3,nz+3]. Returns ([D,H,W,2] bf16, s)."""
+        r, p = self._core(rho, phi_prev)
         s = float(p.abs().max().item()) or 1.0
-        x = torch.zeros(r.shape + (16,), dtype=torch.bfloat16, device=rho.device)
-        x[..., 0] = (r * self.rho_scale).to(torch.bfloat16)
+        x = torch.empty(r.shape + (2,), dtype=torch.bfloat16, device=rho.device)
+        x[..., 0] = (r * (self.rho_factor / s)).to(torch.bfloat16)
         x[..., 1] = (p / s).to(torch.bfloat16)
         return x, s
 
+    def pair(self, rho, phi_prev, phi):
+        """Training pair (inputs, target) of one solved step."""
+        x, s = self.inputs(rho, phi_prev)
+        _, p0 = self._core(rho, phi_prev)
+        _, p1 = self._core(rho, phi)
+        y = ((p1 - p0) * (self.out_scale / s)).to(torch.bfloat16).contiguous()
+        return x.contiguous(), y
+
+    @torch.no_grad()
+    def predict(self, x2):
+        x = torch.zeros(x2.shape[:3] + (16,), dtype=torch.bfloat16, device=x2.device)
+        x[..., :2] = x2
+        return self.net(x)
+
     @torch.no_grad()
     def guess(self, solver):
-        """Writes phi^(n-1) + predicted change into solver.phi (nodes 0..n-1;
-        the boundary and periodic copies are set by the solver)."""
+        """Adds the predicted change to solver.phi (which holds phi^(n-1)) on
+        the nodes 0..n-1; the solver's boundary handling sets the rest."""
         x, s = self.inputs(solver.rho, solver.phi)
-        d = self.net(x)
+        d = self.predict(x)
         interior = solver.phi[1:-2, 1:-2, 1:-2]
-        interior.add_((d * s).permute(2, 1, 0).to(torch.float64))
+        interior.add_((d * (s / self.out_scale)).permute(2, 1, 0).to(torch.float64))
         check_errors(solver.device)
