@@ -51,6 +51,23 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(ms, world, device):
+    """Slowest rank's time (device-timed per rank): every replica ran the
+    same number of steps, so the job took as long as the slowest one."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(ms_per_step, world):
+    """Whole-job steps/s of `world` independent replicas."""
+    return world * 1000.0 / ms_per_step
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -289,17 +306,10 @@ def main():
             del run
             torch.cuda.empty_cache()
         results[f] = res
-    ms_head = results[headline]["ms_per_step"]
-    if world > 1:
-        t = torch.tensor([ms_head], device=dev, dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms_head = float(t.item())
-    value = world * 1000.0 / ms_head
+    ms_head = max_over_ranks(results[headline]["ms_per_step"], world, dev)
+    value = replica_throughput(ms_head, world)
     e2e_ms, h2d, d2h = e2e_steps(head_run, args.e2e_steps) if args.e2e_steps > 0 else (float("nan"), 0, 0)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
     peak, peak_kind = measured_peaks()
     kern = results[headline]["kernels"]
     sor = kern["sor0"]
