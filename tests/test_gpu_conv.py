@@ -82,12 +82,16 @@ def test_unet_gradients_against_oracle_chain():
     unet.check_errors(y.device)
     xn, wn = x.detach().float().cpu().numpy(), w.detach().cpu().numpy()
     pre = co.conv3_fwd(xn, wn)
-    gz = g.float().cpu().numpy() * (pre > 0)
-    # the kernel's ReLU mask comes from the bf16 output; compare where the
-    # pre-activation is not within rounding of zero
-    ok = np.abs(pre) > 1e-2 * np.max(np.abs(pre))
-    gz = gz * ok
+    # the ReLU mask comes from the kernel's bf16 output; it must agree with
+    # the oracle's pre-activation sign wherever that is not within rounding
+    # of zero, and the chain rule is checked for that mask
+    act = y.detach().float().cpu().numpy() > 0
+    near0 = np.abs(pre) <= 1e-2 * np.max(np.abs(pre))
+    assert np.all((act == (pre > 0)) | near0)
+    gz = g.float().cpu().numpy() * act
     rdw = co.conv3_wgrad(xn, gz)
     rdb = gz.sum(axis=(0, 1, 2))
-    assert np.max(np.abs(b.grad.cpu().numpy() - rdb)) <= 2e-2 * np.max(np.abs(rdb)) + 1e-1
+    rdx = co.conv3_dgrad(gz, wn)
+    assert np.max(np.abs(b.grad.cpu().numpy() - rdb)) <= 1e-3 * np.max(np.abs(rdb))
     assert np.max(np.abs(w.grad.cpu().numpy() - rdw)) <= 2e-2 * np.max(np.abs(rdw))
+    assert np.max(np.abs(x.grad.float().cpu().numpy() - rdx)) <= 2e-2 * np.max(np.abs(rdx))
