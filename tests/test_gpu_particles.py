@@ -76,6 +76,9 @@ def test_fetch_e_bitexact():
     assert np.array_equal(pg.ex.cpu().numpy(), ex)
     assert np.array_equal(pg.ey.cpu().numpy(), ey)
     assert np.array_equal(pg.ez.cpu().numpy(), ez)
+    # host-array form of the same gather
+    eh = s.fetche_host(p["x"], p["y"], p["z"])
+    assert np.array_equal(eh[0], ex) and np.array_equal(eh[1], ey) and np.array_equal(eh[2], ez)
 
 
 def test_advance_bitexact_with_quads_and_pipe():

@@ -277,6 +277,20 @@ class MultiGridB200(FieldSolver):
 
     fetchfieldfrompositions = fetche
 
+    def fetche_host(self, x, y, z):
+        """E at host positions (numpy arrays), returned as three host arrays:
+        the call a host-array caller such as WARP's own
+        fetchfieldfrompositions (multigrid.py:521-558) makes. Positions are
+        copied in, the gather runs on the device, the fields are copied out."""
+        self._bind_stream()
+        pos = [torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(self.device) for a in (x, y, z)]
+        n = int(pos[0].shape[0])
+        e = torch.zeros((3, n), dtype=torch.float64, device=self.device)
+        if n:
+            _lib.check(_lib.lib.wg_fetch_e(self._h, pos[0].data_ptr(), pos[1].data_ptr(), pos[2].data_ptr(),
+                                           e[0].data_ptr(), e[1].data_ptr(), e[2].data_ptr(), n))
+        return e.cpu().numpy()
+
     # -- drop-in particle advance ------------------------------------------
     def setlattice(self, lattice, nzl=None, zlmin=None, dzl=None):
         """Installs the quad tables of `lattice` (warp_b200.lattice.Lattice)
