@@ -136,6 +136,20 @@ int wg_relresidual(wg_ctx* ctx, double mgparam, double* out);
  * 64-bit fixed-point grid, so rho is bit-identical from run to run.
  * zero_first clears rho first (loadrho3d zeroes rho before depositing). */
 int wg_deposit(wg_ctx* ctx, const wg_particles* p, int zero_first);
+/* The deposit of wg_deposit into a caller-owned rho(0:nx,0:ny,0:nz) array,
+ * with no context and no allocation (no counterpart in the reference). For
+ * callers that cannot let a library allocate device memory: host codes that
+ * manage every device buffer themselves, or that keep a step free of
+ * cudaMalloc/cudaFree because those synchronize the device. Its fixed-point
+ * accumulator is a fixed array inside the library, so the grid is limited to
+ * (nx+1)(ny+1)(nz+1) <= 1048576 nodes (8 MiB); larger grids get WG_ETOOLARGE.
+ * Call with the device that holds rho and the particles current. The first
+ * call on each device looks up that array's device address; make that first
+ * call before any stream capture. Work is queued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream), which is synchronized before
+ * return. Calls that overlap on one device (other streams or threads) share
+ * the accumulator and race: serialize them. */
+int wg_deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream);
 /* applyrhoboundaryconditions3d (w3d.F:2660-2750) on rho. */
 int wg_finalize_rho(wg_ctx* ctx);
 /* sete3d -> sete_from_phi_linear3d (w3d.F:3656, 3963-4108), via

@@ -18,6 +18,7 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st);
 int relresidual(wg_ctx* c, double mgparam, double* out);
 int deposit(wg_ctx* c, const wg_particles* p, int zero_first);
+int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream);
 int finalize_rho(wg_ctx* c);
 int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double* ex, double* ey, double* ez,
             int64_t np);
@@ -395,6 +396,10 @@ int wg_relresidual(wg_ctx* c, double mgparam, double* out) {
 int wg_deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
   if (!c) { set_error("null context"); return WG_EINVAL; }
   return deposit(c, p, zero_first);
+}
+
+int wg_deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream) {
+  return deposit_noalloc(grid, p, rho, zero_first, stream);
 }
 
 int wg_finalize_rho(wg_ctx* c) {

@@ -9,6 +9,8 @@
 // FP64 running sum only by the rounding of each weight to 2^-46.
 
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "wg_internal.h"
 
@@ -531,6 +533,90 @@ int permute(wg_ctx* c, const int64_t* perm, const wg_particles* src, const wg_pa
   if (src->np == 0) return WG_OK;
   { ++c->nlaunch; k_permute<<<cdiv64(src->np, 256), 256, 0, c->stream>>>(perm, src->np, *src, *dst); }
   WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
+// ---- deposition into caller memory with no allocation ----------------------
+//
+// For callers that own every device buffer and cannot let a library allocate:
+// a host code with its own device memory manager, or one that keeps a step
+// free of cudaMalloc/cudaFree because those calls synchronize the device and
+// would stall its other streams. The fixed-point accumulator lives in a
+// file-scope device array instead of a context, so this path needs neither
+// wg_create nor any allocation. Two calls that overlap on one device (other
+// streams or host threads) share that array and race.
+
+namespace {
+
+constexpr int64_t kNoAllocMaxNodes = 1 << 20;  // (nx+1)(ny+1)(nz+1) limit: 8 MiB of accumulator
+constexpr int kNoAllocMaxDevices = 64;
+
+// accumulator nodes [0, kNoAllocMaxNodes), then the overflow flag
+__device__ __align__(256) unsigned long long g_noalloc_acc[kNoAllocMaxNodes + 32];
+
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream) {
+  if (!grid || !p || !rho) { set_error("wg_deposit_noalloc: null argument"); return WG_EINVAL; }
+  const wg_grid& G = *grid;
+  if (G.nx < 1 || G.ny < 1 || G.nz < 1 || !(G.xmmax > G.xmmin) || !(G.ymmax > G.ymmin) || !(G.zmmax > G.zmmin)) {
+    set_error("wg_deposit_noalloc: need nx, ny, nz >= 1 and increasing mesh extents");
+    return WG_EINVAL;
+  }
+  if (p->np < 0 || (p->np > 0 && (!p->x || !p->y || !p->z || !p->gaminv))) {
+    set_error("wg_deposit_noalloc: null particle arrays");
+    return WG_EINVAL;
+  }
+  const int64_t nr = (int64_t)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+  if (nr > kNoAllocMaxNodes) {
+    set_error("wg_deposit_noalloc: grid has " + std::to_string(nr) + " nodes, above the fixed limit of " +
+              std::to_string(kNoAllocMaxNodes) + " nodes ((nx+1)(ny+1)(nz+1)); use wg_deposit for larger grids");
+    return WG_ETOOLARGE;
+  }
+  if (cdiv64(p->np, DEP_NT * DEP_PPT) > 2147483647LL) {
+    set_error("wg_deposit_noalloc: too many particles");
+    return WG_ETOOLARGE;
+  }
+  int dev = 0;
+  WG_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_error("wg_deposit_noalloc: device ordinal above " + std::to_string(kNoAllocMaxDevices - 1));
+    return WG_EINVAL;
+  }
+  unsigned long long* acc;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* a = nullptr;
+      WG_TRY_CUDA(cudaGetSymbolAddress(&a, g_noalloc_acc));
+      g_noalloc_ptr[dev] = static_cast<unsigned long long*>(a);
+    }
+    acc = g_noalloc_ptr[dev];
+  }
+  unsigned long long* flag = acc + kNoAllocMaxNodes;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  WG_TRY_CUDA(cudaMemsetAsync(acc, 0, (size_t)nr * sizeof(unsigned long long), s));
+  WG_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned long long), s));
+  const double dx = (G.xmmax - G.xmmin) / G.nx, dy = (G.ymmax - G.ymmin) / G.ny, dz = (G.zmmax - G.zmmin) / G.nz;
+  GridP g{G.nx, G.ny, G.nz, dx, dy, dz, G.xmmin, G.ymmin, G.zmmin, 0.};
+  if (p->np > 0) k_deposit<<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, acc);
+  double gg = p->w * p->q;
+  gg = gg / dx;
+  gg = gg / dy;
+  gg = gg / dz;
+  k_fix_to_rho<<<cdiv64(nr, 256), 256, 0, s>>>(acc, rho, (size_t)nr, gg * kFixInv, zero_first ? 0 : 1, flag);
+  WG_TRY_CUDA(cudaGetLastError());
+  unsigned long long hflag = 0;
+  WG_TRY_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(hflag), cudaMemcpyDeviceToHost, s));
+  WG_TRY_CUDA(cudaStreamSynchronize(s));
+  if (hflag) {
+    set_error("wg_deposit_noalloc: fixed-point charge accumulator above 2^62 at some node (more than 65536 full "
+              "particle weights on one node)");
+    return WG_EOVERFLOW;
+  }
   return WG_OK;
 }
 
