@@ -158,12 +158,15 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
         # kernel durations from CUDA events on the launching stream, over the
         # same number of further steps (event timing runs the V-cycles kernel
         # by kernel instead of from the captured graph)
-        mask = (1 << _lib.PROF_SOR0) | (1 << _lib.PROF_ADVANCE) | (1 << _lib.PROF_DEPOSIT) | (1 << _lib.PROF_RESID0)
+        kinds = {"sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE, "deposit": _lib.PROF_DEPOSIT,
+                 "resid0": _lib.PROF_RESID0, "restrict0": _lib.PROF_RESTRICT0, "expand0": _lib.PROF_EXPAND0,
+                 "corr": _lib.PROF_CORR}
+        mask = 0
+        for v in kinds.values():
+            mask |= 1 << v
         _lib.check(_lib.lib.wg_prof_enable(h, mask))
         for _ in range(steps):
             run.step()
-        kinds = {"sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE, "deposit": _lib.PROF_DEPOSIT,
-                 "resid0": _lib.PROF_RESID0}
         out["kernels"] = {}
         for k, v in kinds.items():
             t, n, u = _lib.ctypes.c_double(), _lib.ctypes.c_int64(), _lib.ctypes.c_double()
@@ -313,14 +316,17 @@ def main():
     peak, peak_kind = measured_peaks()
     kern = results[headline]["kernels"]
     sor = kern["sor0"]
-    # algorithmic bytes per profiled unit: a fused sweep is recorded as 2 units
-    # per node (read phi + rhs, write phi = 24 B/node FP64, 12 B/node FP32)
-    bytes_per_node = 6.0 if headline == "mixed" else 12.0
+    # algorithmic bytes of one red or black half sweep of the finest level
+    # (one profiled unit per node): read phi of every node, read rhs and
+    # write phi of the half being updated = 16 B/node FP64, 8 B/node FP32
+    bytes_per_node = 8.0 if headline == "mixed" else 16.0
+    sor_kernel = "k_sor_bulk<%s> (finest level, one red or black half sweep)" % (
+        "float" if headline == "mixed" else "double")
     achieved = None
     if sor["launches"]:
         per_launch_bytes = bytes_per_node * sor["units"] / sor["launches"]
         achieved = per_launch_bytes / (sor["ms"] / sor["launches"] * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_sor_fused (finest level, red+black sweep)", "achieved": achieved,
+    roofline = {"bound": "hbm", "kernel": sor_kernel, "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                 "peak_kind": peak_kind, "traffic": None,
                 "bytes_per_node_per_launch": bytes_per_node}

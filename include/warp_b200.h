@@ -189,6 +189,9 @@ int wg_particle_permute(wg_ctx* ctx, const int64_t* perm, const wg_particles* sr
 #define WG_PROF_DEPOSIT 1  /* charge deposition (units: particles) */
 #define WG_PROF_ADVANCE 2  /* fused gather + push (units: particles) */
 #define WG_PROF_RESID0 3   /* residual on the finest level (units: nodes) */
+#define WG_PROF_RESTRICT0 4 /* restriction from the finest level (units: fine nodes) */
+#define WG_PROF_EXPAND0 5   /* prolongation into the finest level (units: fine nodes) */
+#define WG_PROF_CORR 6      /* FP64 correction update of the mixed form (units: nodes) */
 
 /* Starts CUDA-event timing of the kernel kinds in `mask` (bits 1<<WG_PROF_*),
  * clearing earlier records; mask 0 stops it. */
@@ -205,7 +208,7 @@ int wg_launch_count(wg_ctx* ctx, int64_t* n);
 /* y[v][yoff+co] = relu?(bias[co] + sum_{t,ci} x[v+off_t][ci] * w[t][co][ci]),
  * optionally multiplied by (mask[v][co] > 0). x: [D][H][W][cin] bf16,
  * w: [27][cout][cin] bf16 (tap t = 9*(dz+1) + 3*(dy+1) + (dx+1)), bias fp32 or
- * NULL, y: [D][H][W][ystride] bf16. cin, cout multiples of 16, cout <= 128.
+ * NULL, y: [D][H][W][ystride] bf16. cin, cout multiples of 16, cout <= 256.
  * Zero padding outside the box. *err is set non-zero if a wait timed out. */
 int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
                  int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream);

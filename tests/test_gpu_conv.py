@@ -22,7 +22,7 @@ def _rand(shape, seed, scale=1.0):
 
 
 @pytest.mark.parametrize("dims,cin,cout", [((5, 6, 40), 16, 16), ((4, 4, 33), 32, 64), ((3, 5, 7), 48, 128),
-                                           ((8, 8, 16), 128, 32)])
+                                           ((8, 8, 16), 128, 32), ((3, 4, 18), 64, 192)])
 def test_conv3_fwd_matches_oracle(dims, cin, cout):
     from warp_b200 import unet
     D, H, W = dims

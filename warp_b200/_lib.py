@@ -93,7 +93,7 @@ SIGNATURES = {
     "wg_conv3_wgrad": [_vp, _vp] + [_c.c_int] * 5 + [_vp, _vp, _vp],
 }
 
-PROF_SOR0, PROF_DEPOSIT, PROF_ADVANCE, PROF_RESID0 = 0, 1, 2, 3
+PROF_SOR0, PROF_DEPOSIT, PROF_ADVANCE, PROF_RESID0, PROF_RESTRICT0, PROF_EXPAND0, PROF_CORR = 0, 1, 2, 3, 4, 5, 6
 
 
 def _load():

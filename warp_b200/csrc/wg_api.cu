@@ -1,6 +1,7 @@
 // C ABI entry points (include/warp_b200.h): context, level allocation,
 // conductor upload, and dispatch to the solver and particle kernels.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -91,6 +92,62 @@ void free_conductor_data(wg_ctx* c) {
   }
 }
 
+// Index and weight tables of expand3d (f3d_mgrid.F:1777-1947) from coarse
+// level dc into level L, evaluated with the same integer and double
+// expressions the reference uses per node.
+int expand_tables(Level& L, const LevelDims& dc) {
+  const int n[3] = {L.d.nx, L.d.ny, L.d.nz}, nc[3] = {dc.nx, dc.ny, dc.nz};
+  const size_t tot = (size_t)(n[0] + 3) + (n[1] + 3) + (n[2] + 3);
+  std::vector<int32_t> j(tot);
+  std::vector<double> w(tot);
+  size_t o = 0;
+  for (int a = 0; a < 3; ++a)
+    for (int i = -1; i <= n[a] + 1; ++i, ++o) {
+      j[o] = (i * nc[a]) / n[a];
+      w[o] = 1. * (i * nc[a]) / n[a] - j[o];
+    }
+  WG_TRY(dalloc(&L.ej, tot));
+  WG_TRY(dalloc(&L.ew, tot));
+  WG_TRY_CUDA(cudaMemcpy(L.ej, j.data(), tot * sizeof(int32_t), cudaMemcpyHostToDevice));
+  WG_TRY_CUDA(cudaMemcpy(L.ew, w.data(), tot * sizeof(double), cudaMemcpyHostToDevice));
+  return WG_OK;
+}
+
+// Window and weight tables of restrict3d (f3d_mgrid.F:1593-1775) from level
+// L into coarse level dc, with the reference's per-node expressions.
+int restrict_tables(Level& L, const LevelDims& dc) {
+  const int n[3] = {L.d.nx, L.d.ny, L.d.nz}, nc[3] = {dc.nx, dc.ny, dc.nz};
+  const size_t tot = (size_t)(nc[0] + 1) + (nc[1] + 1) + (nc[2] + 1);
+  std::vector<int32_t> lo(tot), cnt(tot);
+  std::vector<double> w(tot * kRestrictTaps, 0.);
+  size_t o = 0;
+  for (int a = 0; a < 3; ++a) {
+    const double dci = 1. * nc[a] / n[a];
+    for (int ic = 0; ic <= nc[a]; ++ic, ++o) {
+      int l = ((ic - 1) * n[a] + 4 * nc[a]) / nc[a] - 3;
+      int h = ((ic + 1) * n[a] - 1) / nc[a];
+      l = std::max(l, -1);
+      h = std::min(h, n[a] + 1);
+      const int k = std::max(0, h - l + 1);
+      if (k > kRestrictTaps) {
+        set_error("wg_create: restriction window wider than 4 fine cells (coarsening ratio above 2)");
+        return WG_EINVAL;
+      }
+      lo[o] = l;
+      cnt[o] = k;
+      if (a < 2) L.rmax = std::max(L.rmax, k);
+      for (int t = 0; t < k; ++t) w[o * kRestrictTaps + t] = 1. - std::fabs(ic - (l + t + 0.) * dci);
+    }
+  }
+  WG_TRY(dalloc(&L.rlo, tot));
+  WG_TRY(dalloc(&L.rn, tot));
+  WG_TRY(dalloc(&L.rw, tot * kRestrictTaps));
+  WG_TRY_CUDA(cudaMemcpy(L.rlo, lo.data(), tot * sizeof(int32_t), cudaMemcpyHostToDevice));
+  WG_TRY_CUDA(cudaMemcpy(L.rn, cnt.data(), tot * sizeof(int32_t), cudaMemcpyHostToDevice));
+  WG_TRY_CUDA(cudaMemcpy(L.rw, w.data(), tot * kRestrictTaps * sizeof(double), cudaMemcpyHostToDevice));
+  return WG_OK;
+}
+
 void free_graphs(wg_ctx* c) {
   for (int i = 0; i < 2; ++i) {
     if (c->vgraph[i]) cudaGraphExecDestroy(c->vgraph[i]);
@@ -115,6 +172,11 @@ void free_all(wg_ctx* c) {
     dfree(L.phif2);
     dfree(L.rhsf);
     dfree(L.resf);
+    dfree(L.ej);
+    dfree(L.ew);
+    dfree(L.rlo);
+    dfree(L.rn);
+    dfree(L.rw);
   }
   dfree(c->phisave);
   dfree(c->rho);
@@ -224,6 +286,11 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
   c->dx = (G.xmmax - G.xmmin) / G.nx;
   c->dy = (G.ymmax - G.ymmin) / G.ny;
   c->dz = (G.zmmax - G.zmmin) / G.nz;
+  if ((double)(G.nx + 3) * (G.ny + 3) * (G.nz + 3) >= 2147483647.) {
+    set_error("wg_create: the padded grid (nx+3)(ny+3)(nz+3) must hold fewer than 2^31 nodes");
+    delete c;
+    return WG_ETOOLARGE;
+  }
   std::vector<LevelDims> dims = mglevels(G.nx, G.ny, G.nz, c->dx, c->dy, c->dz);
   c->lv.resize(dims.size());
   int rc = WG_OK;
@@ -236,6 +303,8 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
     if (rc == WG_OK) rc = dalloc(&L.phi2, L.np);
     if (rc == WG_OK) rc = dalloc(&L.rhs, L.nr);
     if (rc == WG_OK && l + 1 < dims.size()) rc = dalloc(&L.res, L.np);
+    if (rc == WG_OK && l + 1 < dims.size()) rc = expand_tables(L, dims[l + 1]);
+    if (rc == WG_OK && l + 1 < dims.size()) rc = restrict_tables(L, dims[l + 1]);
   }
   Level& L0 = c->lv[0];
   if (rc == WG_OK) rc = dalloc(&c->phisave, L0.np);

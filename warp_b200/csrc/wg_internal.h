@@ -80,7 +80,21 @@ struct Level {
   double* int_volt = nullptr;
   DevSubgrid sub[2];   // 0 even, 1 odd
   bool has_neumann_sub = false;
+  // prolongation from the next coarser level: per fine index i = -1..n+1
+  // (stored at i+1) the coarse cell j = (i*nc)/n and weight 1.*(i*nc)/n - j,
+  // x entries first, then y, then z
+  int32_t* ej = nullptr;
+  double* ew = nullptr;
+  // restriction into the next coarser level: per coarse index ic = 0..nc
+  // the first fine index, the tap count (<= kRestrictTaps) and the tap
+  // weights 1 - |ic - i*nc/n|, x entries first, then y, then z
+  int32_t* rlo = nullptr;
+  int32_t* rn = nullptr;
+  double* rw = nullptr;
+  int rmax = 0;  // widest x or y window
 };
+
+constexpr int kRestrictTaps = 4;
 
 std::vector<LevelDims> mglevels(int nx, int ny, int nz, double dx, double dy, double dz);
 

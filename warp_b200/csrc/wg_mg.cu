@@ -73,6 +73,18 @@ struct Box<float> {
   __device__ static uint32_t idx(float v) { return __float_as_uint(v) & 0x3FFFFFu; }
   __device__ static bool interior(float v) { return __float_as_int(v) < 0; }
 };
+// z planes per thread of the bulk stencil kernels
+template <typename T>
+struct ZPlanes;
+template <>
+struct ZPlanes<double> {
+  static constexpr int value = 2;
+};
+template <>
+struct ZPlanes<float> {
+  static constexpr int value = 4;
+};
+
 template <typename T>
 __device__ inline bool isbox(T v) {
   return v != v;
@@ -319,21 +331,45 @@ __global__ void k_box(T* __restrict__ rhs, int nx, int ny, CondArgs<T> C, T* __r
 // sorhalfpass3d bulk loop (f3d_mgrid.F:2229-2243): one colour, in place.
 // Conductor nodes are skipped here: they keep their old value, which is the
 // prevphi of condbndymg, and k_special_sor updates them.
-template <typename T>
+template <typename T, int ZPT>
 __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny,
-                                                  int ixmin, int ixmax, int iymin, int iymax, int izmin, int parity,
-                                                  T cx, T cy, T cz, T spm1) {
-  const int iz = izmin + blockIdx.z;
-  const int iy = iymin + blockIdx.y * blockDim.y + threadIdx.y;
+                                                  int ixmin, int ixmax, int iymin, int iymax, int izmin, int izmax,
+                                                  int parity, T cx, T cy, T cz, T spm1) {
+  // ZPT consecutive planes per thread; every load of the thread is issued
+  // before the first store (the nodes of one colour read only nodes of the
+  // other colour, so the order within the half sweep does not matter).
+  // Offsets are 32-bit (the level holds fewer than 2^31 padded nodes).
+  const int iy = iymin + (int)(blockIdx.y * blockDim.y + threadIdx.y);
   if (iy > iymax) return;
-  const int ix = ixmin + ((ixmin + iy + iz + parity) & 1) + 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (ix > ixmax) return;
-  const T r = rhs[rix(nx, ny, ix, iy, iz)];
-  if (isbox(r)) return;
-  const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
-  const size_t p = pix(nx, ny, ix, iy, iz);
-  phi[p] = r + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy + (phi[p - sz] + phi[p + sz]) * cz +
-           spm1 * phi[p];
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iz0 = izmin + (int)blockIdx.z * ZPT;
+  const int sy = nx + 3, sz = sy * (ny + 3), ry = nx + 1, rz = ry * (ny + 1);
+  const int xb = ixmin + 2 * t, odd0 = (ixmin + iy + iz0 + parity) & 1;
+  const int p0 = (xb + 1) + sy * (iy + 1) + sz * (iz0 + 1);
+  const int q0 = xb + ry * iy + rz * iz0;
+  T r[ZPT], c[ZPT], xm[ZPT], xp[ZPT], ym[ZPT], yp[ZPT], zm[ZPT], zp[ZPT];
+  bool ok[ZPT];
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k) {
+    const int sh = (odd0 + k) & 1;
+    ok[k] = iz0 + k <= izmax && xb + sh <= ixmax;
+    if (ok[k]) {
+      const int p = p0 + k * sz + sh;
+      r[k] = rhs[q0 + k * rz + sh];
+      c[k] = phi[p];
+      xm[k] = phi[p - 1];
+      xp[k] = phi[p + 1];
+      ym[k] = phi[p - sy];
+      yp[k] = phi[p + sy];
+      zm[k] = phi[p - sz];
+      zp[k] = phi[p + sz];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k)
+    if (ok[k] && !isbox(r[k]))
+      phi[p0 + k * sz + ((odd0 + k) & 1)] =
+          r[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz + spm1 * c[k];
 }
 
 // condbndymg for one colour then cond_potmg (f3d_mgrid.F:2874-2978,
@@ -574,35 +610,53 @@ __global__ void __launch_bounds__(FNT, 3) k_sor_fused(FusedArgs<T> a) {
 //   MODE 1: no store, only the max over non-conductor nodes (norm)
 //   MODE 2: writes the unpadded FP32 rhs of the next correction solve
 // Conductor nodes get 0 here; k_special_res fills them in.
-template <typename T, int MODE, typename TO>
+template <typename T, int MODE, typename TO, int ZPT>
 __global__ void __launch_bounds__(256) k_residual(const T* __restrict__ phi, const T* __restrict__ rhs,
                                                   TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
                                                   int ixmax, int iymin, int iymax, int izmin, int izmax, T cx, T cy,
                                                   T cz, T mgparam, unsigned long long* maxout) {
-  // MODE 0 covers the padded array, the others the node array
+  // MODE 0 covers the padded array, the others the node array; ZPT planes
+  // per thread with all loads issued first; 32-bit offsets
   const int g = (MODE == 0) ? 1 : 0;
   const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x) - g;
   const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y) - g;
-  const int iz = (int)blockIdx.z - g;
-  double m = 0.;
-  bool live = ix <= nx + g && iy <= ny + g;
-  if (live) {
-    T r = (T)0.;
-    bool inrange = ix >= ixmin && ix <= ixmax && iy >= iymin && iy <= iymax && iz >= izmin && iz <= izmax;
-    if (inrange) {
-      const T b = rhs[rix(nx, ny, ix, iy, iz)];
-      if (!isbox(b)) {
-        const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
-        const size_t p = pix(nx, ny, ix, iy, iz);
-        r = b + (phi[p - 1] + phi[p + 1]) * cx + (phi[p - sy] + phi[p + sy]) * cy + (phi[p - sz] + phi[p + sz]) * cz -
-            phi[p] * mgparam;
-        m = fabs((double)r);
-      }
+  const int iz0 = (int)blockIdx.z * ZPT - g;
+  const bool live = ix <= nx + g && iy <= ny + g;
+  const bool xyin = ix >= ixmin && ix <= ixmax && iy >= iymin && iy <= iymax;
+  const int sy = nx + 3, sz = sy * (ny + 3), ry = nx + 1, rz = ry * (ny + 1);
+  const int p0 = (ix + 1) + sy * (iy + 1) + sz * (iz0 + 1);
+  const int q0 = ix + ry * iy + rz * iz0;
+  T b[ZPT], c[ZPT], xm[ZPT], xp[ZPT], ym[ZPT], yp[ZPT], zm[ZPT], zp[ZPT];
+  bool in[ZPT];
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k) {
+    const int iz = iz0 + k;
+    in[k] = live && xyin && iz >= izmin && iz <= izmax;
+    if (in[k]) {
+      const int p = p0 + k * sz;
+      b[k] = rhs[q0 + k * rz];
+      c[k] = phi[p];
+      xm[k] = phi[p - 1];
+      xp[k] = phi[p + 1];
+      ym[k] = phi[p - sy];
+      yp[k] = phi[p + sy];
+      zm[k] = phi[p - sz];
+      zp[k] = phi[p + sz];
     }
-    if (MODE == 0) out[pix(nx, ny, ix, iy, iz)] = (TO)r;
-    if (MODE == 2) out[rix(nx, ny, ix, iy, iz)] = (TO)r;
   }
-  if (maxout) block_max_to(maxout, m);
+  T m = (T)0.;
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k) {
+    if (!live || iz0 + k > nz + g) continue;
+    T r = (T)0.;
+    if (in[k] && !isbox(b[k])) {
+      r = b[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz - c[k] * mgparam;
+      m = fmax(m, fabs(r));
+    }
+    if (MODE == 0) out[p0 + k * sz] = (TO)r;
+    if (MODE == 2) out[q0 + k * rz] = (TO)r;
+  }
+  if (maxout) block_max_to(maxout, (double)m);
 }
 
 // cond_potmgres (interior -> 0, f3d_mgrid.F:2472-2500) and condbndyres
@@ -678,40 +732,55 @@ __global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, i
   if (maxout) block_max_to(maxout, m);
 }
 
-// restrict3d (f3d_mgrid.F:1593-1775), serial: one thread per coarse node,
-// summing the tent-weighted fine residual in the reference's loop order.
-template <typename T>
-__global__ void k_restrict(const T* __restrict__ res, T* __restrict__ rhoc, int nx, int ny, int nz, int nxc, int nyc,
-                           int nzc, int ixcmin, int ixcmax, int iycmin, int iycmax, int izcmin, int izcmax, double dxi,
-                           double dyi, double dzi, double ff) {
-  const int ixc = blockIdx.x * blockDim.x + threadIdx.x;
-  const int iyc = blockIdx.y * blockDim.y + threadIdx.y;
+// restrict3d (f3d_mgrid.F:1593-1775): one thread per coarse node, summing
+// the tent-weighted fine residual in the reference's loop order (z, y, x).
+// Windows and weights come from per-axis tables (Level::rlo/rn/rw) and are
+// at most NT wide per axis; the loads of one fine plane are issued together
+// before the ordered sums. The products keep the reference's order,
+// (wx * wy) * wz, with wx * wy formed once per thread; 32-bit offsets.
+template <typename T, int NT>
+__global__ void __launch_bounds__(256) k_restrict(const T* __restrict__ res, T* __restrict__ rhoc, int nx, int ny,
+                                                  int nxc, int nyc, int ixcmin, int ixcmax, int iycmin, int iycmax,
+                                                  int izcmin, int izcmax, const int32_t* __restrict__ tlo,
+                                                  const int32_t* __restrict__ tn, const double* __restrict__ tw,
+                                                  double ff) {
+  const int ixc = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iyc = (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int izc = blockIdx.z;
   if (ixc > nxc || iyc > nyc) return;
-  const size_t o = rix(nxc, nyc, ixc, iyc, izc);
+  const int o = ixc + (nxc + 1) * (iyc + (nyc + 1) * izc);
   if (ixc < ixcmin || ixc > ixcmax || iyc < iycmin || iyc > iycmax || izc < izcmin || izc > izcmax) {
     rhoc[o] = (T)0.;
     return;
   }
-  auto lim = [](int ic, int n, int nc, int& lo, int& hi) {
-    lo = ((ic - 1) * n + 4 * nc) / nc - 3;
-    hi = ((ic + 1) * n - 1) / nc;
-    lo = max(lo, -1);
-    hi = min(hi, n + 1);
-  };
-  int ixmin, ixmax, iymin, iymax, izmin, izmax;
-  lim(ixc, nx, nxc, ixmin, ixmax);
-  lim(iyc, ny, nyc, iymin, iymax);
-  lim(izc, nz, nzc, izmin, izmax);
+  const int ox = ixc, oy = nxc + 1 + iyc, oz = nxc + 1 + nyc + 1 + izc;
+  const int lx = tlo[ox], ly = tlo[oy], lz = tlo[oz];
+  const int cx = tn[ox], cy = tn[oy], cz = tn[oz];
+  T wxy[NT][NT];
+#pragma unroll
+  for (int ky = 0; ky < NT; ++ky)
+#pragma unroll
+    for (int kx = 0; kx < NT; ++kx) wxy[ky][kx] = (T)tw[ox * kRestrictTaps + kx] * (T)tw[oy * kRestrictTaps + ky];
+  const int sy = nx + 3, sz = sy * (ny + 3);
+  const int b0 = (lx + 1) + sy * (ly + 1) + sz * (lz + 1);
   T r = (T)0., w = (T)0.;
-  for (int iz = izmin; iz <= izmax; ++iz) {
-    const T wz = (T)(1. - fabs(izc - (iz + 0.) * dzi));
-    for (int iy = iymin; iy <= iymax; ++iy) {
-      const T wy = (T)(1. - fabs(iyc - (iy + 0.) * dyi));
-      for (int ix = ixmin; ix <= ixmax; ++ix) {
-        const T wx = (T)(1. - fabs(ixc - (ix + 0.) * dxi));
-        r = r + wx * wy * wz * res[pix(nx, ny, ix, iy, iz)];
-        w = w + wx * wy * wz;
+  for (int kz = 0; kz < cz; ++kz) {
+    const T wz = (T)tw[oz * kRestrictTaps + kz];
+    const T* plane = res + (b0 + kz * sz);
+    T v[NT][NT];
+#pragma unroll
+    for (int ky = 0; ky < NT; ++ky)
+#pragma unroll
+      for (int kx = 0; kx < NT; ++kx) v[ky][kx] = (ky < cy && kx < cx) ? plane[ky * sy + kx] : (T)0.;
+#pragma unroll
+    for (int ky = 0; ky < NT; ++ky) {
+      if (ky >= cy) break;
+#pragma unroll
+      for (int kx = 0; kx < NT; ++kx) {
+        if (kx >= cx) break;
+        const T t = wxy[ky][kx] * wz;
+        r = r + t * v[ky][kx];
+        w = w + t;
       }
     }
   }
@@ -724,25 +793,56 @@ __global__ void k_restrict(const T* __restrict__ res, T* __restrict__ rhoc, int 
 }
 
 // expand3d (f3d_mgrid.F:1777-1947): trilinear prolongation added to phi.
-template <typename T>
-__global__ void k_expand(T* __restrict__ phi, const T* __restrict__ pc, int nx, int ny, int nxc, int nyc, int nzc,
-                         int nz, int ixmin, int ixmax, int iymin, int iymax, int izmin) {
-  const int ix = ixmin + blockIdx.x * blockDim.x + threadIdx.x;
-  const int iy = iymin + blockIdx.y * blockDim.y + threadIdx.y;
-  const int iz = izmin + blockIdx.z;
+// Coarse indices and weights come from per-axis tables (Level::ej/ew); ZPT
+// consecutive fine planes per thread, all loads issued before the sums;
+// 32-bit offsets. The weight products keep the reference's left-to-right
+// order, ((wx' * wy') * wz') * q, with the x-y part formed once per thread.
+template <typename T, int ZPT>
+__global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __restrict__ pc, int nx, int ny,
+                                                int nxc, int nyc, int ixmin, int ixmax, int iymin, int iymax,
+                                                int izmin, int izmax, const int32_t* __restrict__ ej,
+                                                const double* __restrict__ ew) {
+  const int ix = ixmin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = iymin + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int iz0 = izmin + (int)blockIdx.z * ZPT;
   if (ix > ixmax || iy > iymax) return;
-  const int jz = (iz * nzc) / nz, jy = (iy * nyc) / ny, jx = (ix * nxc) / nx;
-  const T wz = (T)(1. * (iz * nzc) / nz - jz), wy = (T)(1. * (iy * nyc) / ny - jy), wx = (T)(1. * (ix * nxc) / nx - jx);
+  const int oy = nx + 3, oz = nx + 3 + ny + 3;
+  const int jx = ej[ix + 1], jy = ej[oy + iy + 1];
   const T one = (T)1.;
-  T& p = phi[pix(nx, ny, ix, iy, iz)];
-  p = p + (one - wx) * (one - wy) * (one - wz) * pc[pix(nxc, nyc, jx, jy, jz)] +
-      wx * (one - wy) * (one - wz) * pc[pix(nxc, nyc, jx + 1, jy, jz)] +
-      (one - wx) * wy * (one - wz) * pc[pix(nxc, nyc, jx, jy + 1, jz)] +
-      wx * wy * (one - wz) * pc[pix(nxc, nyc, jx + 1, jy + 1, jz)] +
-      (one - wx) * (one - wy) * wz * pc[pix(nxc, nyc, jx, jy, jz + 1)] +
-      wx * (one - wy) * wz * pc[pix(nxc, nyc, jx + 1, jy, jz + 1)] +
-      (one - wx) * wy * wz * pc[pix(nxc, nyc, jx, jy + 1, jz + 1)] +
-      wx * wy * wz * pc[pix(nxc, nyc, jx + 1, jy + 1, jz + 1)];
+  const T wx = (T)ew[ix + 1], wy = (T)ew[oy + iy + 1];
+  const T a00 = (one - wx) * (one - wy), a10 = wx * (one - wy), a01 = (one - wx) * wy, a11 = wx * wy;
+  const int sy = nx + 3, sz = sy * (ny + 3);
+  const int syc = nxc + 3, szc = syc * (nyc + 3);
+  const int cxy = (jx + 1) + syc * (jy + 1);
+  const int f0 = (ix + 1) + sy * (iy + 1) + sz * (iz0 + 1);
+  T q[ZPT][8], f[ZPT], wz[ZPT];
+  bool ok[ZPT];
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k) {
+    const int iz = iz0 + k;
+    ok[k] = iz <= izmax;
+    if (ok[k]) {
+      const int jz = ej[oz + iz + 1];
+      wz[k] = (T)ew[oz + iz + 1];
+      const T* b = pc + (cxy + szc * (jz + 1));
+      q[k][0] = b[0];
+      q[k][1] = b[1];
+      q[k][2] = b[syc];
+      q[k][3] = b[syc + 1];
+      q[k][4] = b[szc];
+      q[k][5] = b[szc + 1];
+      q[k][6] = b[szc + syc];
+      q[k][7] = b[szc + syc + 1];
+      f[k] = phi[f0 + k * sz];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k) {
+    if (!ok[k]) continue;
+    const T z = wz[k], z1 = one - z;
+    phi[f0 + k * sz] = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3] +
+                       a00 * z * q[k][4] + a10 * z * q[k][5] + a01 * z * q[k][6] + a11 * z * q[k][7];
+  }
 }
 
 
@@ -775,19 +875,34 @@ __global__ void k_scale_rhs(const double* __restrict__ rho, double* __restrict__
 }
 
 // Residual-correction update phi = e + phisave (f3d_mgrid.F:355-358) with
-// e from an FP32 V-cycle; max|dphi| over nodes 0..n.
-__global__ void k_add_corr(double* __restrict__ phi, const float* __restrict__ e, int nx, int ny, int nz,
-                           unsigned long long* maxout) {
+// e from an FP32 V-cycle; max|dphi| over nodes 0..n. Four planes per thread.
+constexpr int kCorrPlanes = 4;
+__global__ void __launch_bounds__(256) k_add_corr(double* __restrict__ phi, const float* __restrict__ e, int nx,
+                                                  int ny, int nz, unsigned long long* maxout) {
   const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 1;
   const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
-  const int iz = (int)blockIdx.z - 1;
+  const int iz0 = (int)blockIdx.z * kCorrPlanes - 1;
   double m = 0.;
   if (ix <= nx + 1 && iy <= ny + 1) {
-    size_t p = pix(nx, ny, ix, iy, iz);
-    double old = phi[p];
-    double nw = (double)e[p] + old;
-    phi[p] = nw;
-    if (ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz) m = fabs(old - nw);
+    const int sz = (nx + 3) * (ny + 3);
+    const int p0 = (ix + 1) + (nx + 3) * (iy + 1) + sz * (iz0 + 1);
+    double old[kCorrPlanes];
+    float ev[kCorrPlanes];
+#pragma unroll
+    for (int k = 0; k < kCorrPlanes; ++k) {
+      if (iz0 + k <= nz + 1) {
+        old[k] = phi[p0 + k * sz];
+        ev[k] = e[p0 + k * sz];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kCorrPlanes; ++k) {
+      const int iz = iz0 + k;
+      if (iz > nz + 1) continue;
+      const double nw = (double)ev[k] + old[k];
+      phi[p0 + k * sz] = nw;
+      if (ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz) m = fmax(m, fabs(old[k] - nw));
+    }
   }
   block_max_to(maxout, m);
 }
@@ -940,19 +1055,25 @@ struct Solver {
     const int nhalf = (R.ixmax - R.ixmin) / 2 + 1;
     for (int parity = 0; parity < 2; ++parity) {
       if (nyr > 0 && nzr > 0 && nhalf > 0) {
-        dim3 blk(32, 8), grd(cdiv(nhalf, 32), cdiv(nyr, 8), nzr);
+        constexpr int zpt = ZPlanes<T>::value;
+        dim3 blk(32, 8), grd(cdiv(nhalf, 32), cdiv(nyr, 8), cdiv(nzr, zpt));
         ++c->nlaunch;
         int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
-        k_sor_bulk<T><<<grd, blk, 0, s>>>(phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin,
-                                          parity, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1);
+        k_sor_bulk<T, zpt><<<grd, blk, 0, s>>>(phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin,
+                                               R.izmax, parity, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1);
         c->prof_end(pe);
       }
       int nsub = L.sub[parity].n;
-      if (nsub + L.n_int) {
+      // Interior conductor nodes were set by k_interior at the start of the
+      // pass; no kernel of the pass writes them unless Neumann subgrid
+      // points copy values into their neighbours, so only then are they
+      // set again after each half pass.
+      CondArgs<T> ca = cond_args<T>(L);
+      if (!L.has_neumann_sub) ca.nint = 0;
+      if (nsub + ca.nint) {
         ++c->nlaunch;
-        k_special_sor<T><<<cdiv(nsub + L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, cond_args<T>(L),
-                                                                    parity, B, k, (int)usev, (int)usev,
-                                                                    o->lcndbndy);
+        k_special_sor<T><<<cdiv(nsub + ca.nint, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, ca, parity, B, k,
+                                                                    (int)usev, (int)usev, o->lcndbndy);
       }
       neumann_int<T>(L, phi);
       bc<T>(L, phi, false);
@@ -969,20 +1090,25 @@ struct Solver {
     double dxsqi = 1. / (L.d.dx * L.d.dx), dysqi = 1. / (L.d.dy * L.d.dy), dzsqi = 1. / (L.d.dz * L.d.dz);
     double cst = 0.5 / (dxsqi + dysqi + dzsqi);
     const int g = (MODE == 0) ? 1 : 0;
-    dim3 blk(32, 8), grd(cdiv(L.d.nx + 1 + 2 * g, 32), cdiv(L.d.ny + 1 + 2 * g, 8), L.d.nz + 1 + 2 * g);
+    constexpr int zpt = ZPlanes<T>::value;
+    dim3 blk(32, 8), grd(cdiv(L.d.nx + 1 + 2 * g, 32), cdiv(L.d.ny + 1 + 2 * g, 8), cdiv(L.d.nz + 1 + 2 * g, zpt));
     {
       ++c->nlaunch;
       int pe = prof_begin(l, WG_PROF_RESID0, (double)L.nr);
-      k_residual<T, MODE, TO><<<grd, blk, 0, s>>>(phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
+      k_residual<T, MODE, TO, zpt><<<grd, blk, 0, s>>>(phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
                                                   R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
                                                   (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst),
                                                   (T)o->mgparam, maxout);
       c->prof_end(pe);
     }
-    int n = L.sub[0].n + L.sub[1].n + L.n_int;
+    // interior conductor nodes are boxed, so the bulk kernel already stored
+    // their zero residual
+    CondArgs<T> ca = cond_args<T>(L);
+    ca.nint = 0;
+    int n = L.sub[0].n + L.sub[1].n;
     if (n) {
       ++c->nlaunch;
-      k_special_res<T, MODE, TO><<<cdiv(n, 128), 128, 0, s>>>(phi, out, L.d.nx, L.d.ny, L.d.nz, cond_args<T>(L), B,
+      k_special_res<T, MODE, TO><<<cdiv(n, 128), 128, 0, s>>>(phi, out, L.d.nx, L.d.ny, L.d.nz, ca, B,
                                                               dxsqi, dysqi, dzsqi, o->mgparam, (int)voltfac_on,
                                                               (int)mgform2init, o->lcndbndy, maxout);
     }
@@ -1005,18 +1131,27 @@ struct Solver {
       Ranges Rc = ranges(dc, B.b, false);
       dim3 blk(32, 8), grd(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), dc.nz + 1);
       ++c->nlaunch;
-      k_restrict<T><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, d.nz, dc.nx, dc.ny, dc.nz,
-                                        Rc.ixmin, Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
-                                        1. * dc.nx / d.nx, 1. * dc.ny / d.ny, 1. * dc.nz / d.nz, ff);
+      int pr = prof_begin(l, WG_PROF_RESTRICT0, (double)L.nr);
+      if (L.rmax <= 3)
+        k_restrict<T, 3><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin,
+                                             Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax, L.rlo, L.rn, L.rw, ff);
+      else
+        k_restrict<T, kRestrictTaps><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny,
+                                                         Rc.ixmin, Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
+                                                         L.rlo, L.rn, L.rw, ff);
+      c->prof_end(pr);
       box<T>(l + 1);
       cudaMemsetAsync(Arr<T>::phi(Lc), 0, Lc.np * sizeof(T), s);
       vcycle<T>(l + 1, false);
       Ranges R = ranges(d, B.b, false);
-      dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), R.izmax - R.izmin + 1);
+      constexpr int zpt = ZPlanes<T>::value;
+      dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), cdiv(R.izmax - R.izmin + 1, zpt));
       if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin) {
         ++c->nlaunch;
-        k_expand<T><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny, dc.nz, d.nz,
-                                         R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin);
+        int pe = prof_begin(l, WG_PROF_EXPAND0, (double)L.nr);
+        k_expand<T, zpt><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny, R.ixmin,
+                                              R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
+        c->prof_end(pe);
       }
       bc<T>(L, Arr<T>::phi(L), false);
     }
@@ -1134,7 +1269,6 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   S.box<double>(0);
   S.bc<double>(L0, L0.phi, false);
   dim3 blk(32, 8), grdn(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1);
-  dim3 grdp(cdiv(d.nx + 3, 32), cdiv(d.ny + 3, 8), d.nz + 3);
   int it = 0;
   double err = 2. * o->mgtol + 1., relres = -1.;
   bool conv = false;
@@ -1186,7 +1320,13 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       WG_TRY_CUDA(cudaMemsetAsync(L0.phif, 0, L0.np * sizeof(float), s));
       WG_TRY(run_vcycle<float>(S, false));
       WG_TRY(S.clear_slots(0));
-      { ++c->nlaunch; k_add_corr<<<grdp, blk, 0, s>>>(L0.phi, L0.phif, d.nx, d.ny, d.nz, S.slotq(0)); }
+      {
+        ++c->nlaunch;
+        dim3 grdc(cdiv(d.nx + 3, 32), cdiv(d.ny + 3, 8), cdiv(d.nz + 3, kCorrPlanes));
+        int pe = S.prof_begin(0, WG_PROF_CORR, (double)L0.nr);
+        k_add_corr<<<grdc, blk, 0, s>>>(L0.phi, L0.phif, d.nx, d.ny, d.nz, S.slotq(0));
+        c->prof_end(pe);
+      }
       S.bc<double>(L0, L0.phi, false);
       it += 1;
       if (o->tolkind == 0) {

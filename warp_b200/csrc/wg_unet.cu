@@ -124,7 +124,7 @@ struct ConvArgs {
   int* err;
 };
 
-// Forward / data-gradient implicit GEMM, N = cout (16..128, multiple of 16).
+// Forward / data-gradient implicit GEMM, N = cout (16..256, multiple of 16).
 __global__ void __launch_bounds__(CNT) k_conv3_mma(ConvArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int N = a.cout;
@@ -350,9 +350,9 @@ extern "C" {
 
 int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
                  int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream) {
-  if (!x || !w || !y || !err || D < 1 || H < 1 || W < 1 || cin < 16 || cin % 16 || cout < 16 || cout > 128 ||
+  if (!x || !w || !y || !err || D < 1 || H < 1 || W < 1 || cin < 16 || cin % 16 || cout < 16 || cout > 256 ||
       cout % 16 || ystride < yoff + cout || (yoff % 8) || (ystride % 8) || (mask && mstride < cout)) {
-    set_error("wg_conv3_fwd: bad arguments (cin, cout multiples of 16, cout <= 128, 16-byte aligned rows)");
+    set_error("wg_conv3_fwd: bad arguments (cin, cout multiples of 16, cout <= 256, 16-byte aligned rows)");
     return WG_EINVAL;
   }
   ConvArgs a{(const __nv_bfloat16*)x, (const __nv_bfloat16*)w, bias, (__nv_bfloat16*)y,
