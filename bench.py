@@ -33,6 +33,10 @@ WORKLOAD = "B"
 DEFAULT_REF_VCYCLES = 6
 # particles are re-sorted by cell every SORT_INTERVAL steps (inside the timed steps)
 SORT_INTERVAL = 10
+# DRAM bytes (read + write) per finest-level node of one k_sor_bulk<float>
+# half sweep, from an ncu --set full capture of one launch on the
+# 257x257x513-node level: 271.7 MB read + 91.6 MB written
+SOR_F32_TRAFFIC_PER_NODE = (271.714048e6 + 91.577344e6) / (257 * 257 * 513)
 
 
 def parse():
@@ -328,7 +332,9 @@ def main():
         achieved = per_launch_bytes / (sor["ms"] / sor["launches"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": sor_kernel, "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "peak_kind": peak_kind, "traffic": None,
+                "peak_kind": peak_kind,
+                "traffic": (SOR_F32_TRAFFIC_PER_NODE * sor["units"] / sor["launches"]
+                            if headline == "mixed" and sor["launches"] else None),
                 "bytes_per_node_per_launch": bytes_per_node}
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": True, "scaling": "weak",
