@@ -283,16 +283,13 @@ struct CondArgs {
 // f3d_mgrid.F:2874-2978): neighbours p[6] = xm,xp,ym,yp,zm,zp, prev = the
 // point's value before the pass. Without lcndbndy the bulk update is used.
 template <typename T>
-__device__ __noinline__ T subgrid_value(const CondArgs<T>& C, int par, int i, T pxm, T pxp, T pym, T pyp, T pzm,
-                                        T pzp, T prev, const SorCoef& c, int voltfac_on, int lcndbndy) {
+__device__ __forceinline__ T subgrid_core(T r, const double* d, const double* v, T pxm, T pxp, T pym, T pyp, T pzm,
+                                          T pzp, T prev, const SorCoef& c, int voltfac_on, int lcndbndy) {
   const T dxsqic = (T)c.cx, dysqic = (T)c.cy, dzsqic = (T)c.cz;
-  const T r = C.srhs[par][i];
   if (lcndbndy) {
     const T dxsqicos = (T)(c.cx / c.mgparam), dysqicos = (T)(c.cy / c.mgparam), dzsqicos = (T)(c.cz / c.mgparam);
     const T voltfac = voltfac_on ? (T)1. : (T)0.;
     T denom = (T)1., ppp = (T)1.;
-    const double* d = C.sdels[par] + 6 * (size_t)i;
-    const double* v = C.svolt[par] + 6 * (size_t)i;
     handlesubgrid2<T>(0, 1, pxm, pxp, dxsqicos, d, v, voltfac, denom, ppp);
     handlesubgrid2<T>(2, 3, pym, pyp, dysqicos, d, v, voltfac, denom, ppp);
     handlesubgrid2<T>(4, 5, pzm, pzp, dzsqicos, d, v, voltfac, denom, ppp);
@@ -300,6 +297,13 @@ __device__ __noinline__ T subgrid_value(const CondArgs<T>& C, int par, int i, T 
       return (r + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic) / denom + (T)c.spm1 * prev;
   }
   return r + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic + (T)c.spm1 * prev;
+}
+
+template <typename T>
+__device__ __noinline__ T subgrid_value(const CondArgs<T>& C, int par, int i, T pxm, T pxp, T pym, T pyp, T pzm,
+                                        T pzp, T prev, const SorCoef& c, int voltfac_on, int lcndbndy) {
+  return subgrid_core<T>(C.srhs[par][i], C.sdels[par] + 6 * (size_t)i, C.svolt[par] + 6 * (size_t)i, pxm, pxp, pym,
+                         pyp, pzm, pzp, prev, c, voltfac_on, lcndbndy);
 }
 
 // Marks the conductor nodes of one level in its rhs array (see the header
@@ -328,13 +332,62 @@ __global__ void k_box(T* __restrict__ rhs, int nx, int ny, CondArgs<T> C, T* __r
 // ---------------------------------------------------------------------------
 // Generic in-place path.
 
+// Writes v to node p at plane iz and, when wtz is set (periodic z with
+// non-periodic x and y), to its periodic images: plane nz (image of 0), and
+// the guard planes nz+1 (image of 1) and -1 (image of nz-1). This is what
+// applyboundaryconditions3d would copy afterwards.
+template <typename T>
+__device__ inline void store_wt(T* phi, int p, int iz, int nz, int sz, int wtz, T v) {
+  phi[p] = v;
+  if (wtz) {
+    if (iz <= 1) phi[p + nz * sz] = v;
+    if (iz == nz - 1) phi[p - nz * sz] = v;
+  }
+}
+
+// condbndymg update of subgrid point i of colour par (no-op on Dirichlet
+// boundary planes). With wtz the plane nz is left to the write-through of
+// plane 0.
+template <typename T>
+__device__ __forceinline__ void special_point(T* phi, int nx, int ny, int nz, const CondArgs<T>& C, int par, const Bnd& B,
+                                     const SorCoef& c, int voltfac_on, int lcndbndy, int i, int wtz) {
+  // pointers chosen without indexing the parameter arrays by a runtime value
+  const int32_t* q = (par ? C.sijk[1] : C.sijk[0]) + 3 * (size_t)i;
+  const double* dl = (par ? C.sdels[1] : C.sdels[0]) + 6 * (size_t)i;
+  const double* vl = (par ? C.svolt[1] : C.svolt[0]) + 6 * (size_t)i;
+  const T r = (par ? C.srhs[1] : C.srhs[0])[i];
+  const int ix = q[0], iy = q[1], iz = q[2];
+  if (ix == 0 && B.b[0] < 1) return;
+  if (ix == nx && B.b[1] < 1) return;
+  if (iy == 0 && B.b[2] < 1) return;
+  if (iy == ny && B.b[3] < 1) return;
+  if (iz == 0 && B.b[4] < 1) return;
+  if (iz == nz && B.b[5] < 1) return;
+  if (wtz && iz == nz) return;
+  const int sy = nx + 3, sz = sy * (ny + 3);
+  const int p = (ix + 1) + sy * (iy + 1) + sz * (iz + 1);
+  const T v = subgrid_core<T>(r, dl, vl, phi[p - 1], phi[p + 1], phi[p - sy], phi[p + sy], phi[p - sz], phi[p + sz],
+                              phi[p], c, voltfac_on, lcndbndy);
+  store_wt(phi, p, iz, nz, sz, wtz, v);
+}
+
 // sorhalfpass3d bulk loop (f3d_mgrid.F:2229-2243): one colour, in place.
 // Conductor nodes are skipped here: they keep their old value, which is the
 // prevphi of condbndymg, and k_special_sor updates them.
 template <typename T, int ZPT>
 __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny,
                                                   int ixmin, int ixmax, int iymin, int iymax, int izmin, int izmax,
-                                                  int parity, T cx, T cy, T cz, T spm1) {
+                                                  int parity, T cx, T cy, T cz, T spm1, int nz, int wtz, int nbz,
+                                                  CondArgs<T> C, Bnd B, SorCoef sc, int voltfac_on, int lcndbndy) {
+  // blocks with blockIdx.z >= nbz update the subgrid conductor points of
+  // this colour (condbndymg); they read only nodes of the other colour too
+  if ((int)blockIdx.z >= nbz) {
+    const int i = ((((int)blockIdx.z - nbz) * (int)gridDim.y + (int)blockIdx.y) * (int)gridDim.x + (int)blockIdx.x) *
+                      (int)(blockDim.x * blockDim.y) +
+                  (int)(threadIdx.y * blockDim.x + threadIdx.x);
+    if (i < (parity ? C.nsub[1] : C.nsub[0])) special_point<T>(phi, nx, ny, nz, C, parity, B, sc, voltfac_on, lcndbndy, i, wtz);
+    return;
+  }
   // ZPT consecutive planes per thread; every load of the thread is issued
   // before the first store (the nodes of one colour read only nodes of the
   // other colour, so the order within the half sweep does not matter).
@@ -368,8 +421,8 @@ __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* 
 #pragma unroll
   for (int k = 0; k < ZPT; ++k)
     if (ok[k] && !isbox(r[k]))
-      phi[p0 + k * sz + ((odd0 + k) & 1)] =
-          r[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz + spm1 * c[k];
+      store_wt(phi, p0 + k * sz + ((odd0 + k) & 1), iz0 + k, nz, sz, wtz,
+               r[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz + spm1 * c[k]);
 }
 
 // condbndymg for one colour then cond_potmg (f3d_mgrid.F:2874-2978,
@@ -379,20 +432,9 @@ template <typename T>
 __global__ void k_special_sor(T* __restrict__ phi, int nx, int ny, int nz, CondArgs<T> C, int par, Bnd B, SorCoef c,
                               int voltfac_on, int usev, int lcndbndy) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nsub = C.nsub[par];
+  const int nsub = par ? C.nsub[1] : C.nsub[0];
   if (i < nsub) {
-    const int32_t* q = C.sijk[par] + 3 * (size_t)i;
-    const int ix = q[0], iy = q[1], iz = q[2];
-    if (ix == 0 && B.b[0] < 1) return;
-    if (ix == nx && B.b[1] < 1) return;
-    if (iy == 0 && B.b[2] < 1) return;
-    if (iy == ny && B.b[3] < 1) return;
-    if (iz == 0 && B.b[4] < 1) return;
-    if (iz == nz && B.b[5] < 1) return;
-    const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
-    const size_t p = pix(nx, ny, ix, iy, iz);
-    phi[p] = subgrid_value<T>(C, par, i, phi[p - 1], phi[p + 1], phi[p - sy], phi[p + sy], phi[p - sz], phi[p + sz],
-                              phi[p], c, voltfac_on, lcndbndy);
+    special_point<T>(phi, nx, ny, nz, C, par, B, c, voltfac_on, lcndbndy, i, 0);
     return;
   }
   i -= nsub;
@@ -402,9 +444,13 @@ __global__ void k_special_sor(T* __restrict__ phi, int nx, int ny, int nz, CondA
 // cond_potmg alone (start of sorpass3d and the mgform=2 initial phi).
 template <typename T>
 __global__ void k_interior(T* __restrict__ phi, int nx, int ny, const int32_t* __restrict__ iijk,
-                           const double* __restrict__ ivolt, int nint, int usev) {
+                           const double* __restrict__ ivolt, int nint, int usev, int nz = 0, int wtz = 0) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nint) phi[pix(nx, ny, iijk[3 * i], iijk[3 * i + 1], iijk[3 * i + 2])] = usev ? (T)ivolt[i] : (T)0.;
+  if (i >= nint) return;
+  const int ix = iijk[3 * i], iy = iijk[3 * i + 1], iz = iijk[3 * i + 2];
+  const int sy = nx + 3, sz = sy * (ny + 3);
+  if (wtz && iz == nz) return;
+  store_wt(phi, (ix + 1) + sy * (iy + 1) + sz * (iz + 1), iz, nz, sz, wtz, usev ? (T)ivolt[i] : (T)0.);
 }
 
 // condbndymgint (f3d_mgrid.F:2982-3092): Neumann subgrid neighbours take the
@@ -679,7 +725,12 @@ __global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, i
     int k = i - C.nint;
     const int par = (k < n0) ? 0 : 1;
     if (par) k -= n0;
-    const int32_t* q = C.sijk[par] + 3 * (size_t)k;
+    // parity arrays chosen without indexing the parameter arrays at run time
+    const int32_t* sijk = par ? C.sijk[1] : C.sijk[0];
+    const T* srhs = par ? C.srhs[1] : C.srhs[0];
+    const double* sdels = par ? C.sdels[1] : C.sdels[0];
+    const double* svolt = par ? C.svolt[1] : C.svolt[0];
+    const int32_t* q = sijk + 3 * (size_t)k;
     const int ix = q[0], iy = q[1], iz = q[2];
     bool skip = (ix == 0 && B.b[0] == 0) || (ix == nx && B.b[1] == 0) || (iy == 0 && B.b[2] == 0) ||
                 (iy == ny && B.b[3] == 0) || (iz == 0 && B.b[4] == 0) || (iz == nz && B.b[5] == 0);
@@ -691,14 +742,14 @@ __global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, i
       const T mgparam = (T)mgparam_d;
       const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
       const size_t p = pix(nx, ny, ix, iy, iz);
-      const T rhsv = C.srhs[par][k];
+      const T rhsv = srhs[k];
       T pxm = phi[p - 1], pxp = phi[p + 1], pym = phi[p - sy], pyp = phi[p + sy], pzm = phi[p - sz],
         pzp = phi[p + sz];
       T denom = (T)1., ppp = (T)1.;
       if (lcndbndy) {
         const T voltfac = voltfac_on ? (T)1. : (T)0.;
-        const double* d = C.sdels[par] + 6 * (size_t)k;
-        const double* v = C.svolt[par] + 6 * (size_t)k;
+        const double* d = sdels + 6 * (size_t)k;
+        const double* v = svolt + 6 * (size_t)k;
         handlesubgrid2<T>(0, 1, pxm, pxp, dxsqic, d, v, voltfac, denom, ppp);
         handlesubgrid2<T>(2, 3, pym, pyp, dysqic, d, v, voltfac, denom, ppp);
         handlesubgrid2<T>(4, 5, pzm, pzp, dzsqic, d, v, voltfac, denom, ppp);
@@ -714,7 +765,7 @@ __global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, i
         T r = ppp * inner;
         store(ix, iy, iz, r);
         m = fabs((double)(pppmax * inner));
-        const double* d = C.sdels[par] + 6 * (size_t)k;
+        const double* d = sdels + 6 * (size_t)k;
         if (0. >= d[0] && d[0] >= -1.) store(ix - 1, iy, iz, (T)0.);
         if (0. >= d[1] && d[1] >= -1.) store(ix + 1, iy, iz, (T)0.);
         if (0. >= d[2] && d[2] >= -1.) store(ix, iy - 1, iz, (T)0.);
@@ -1045,24 +1096,27 @@ struct Solver {
     }
     T* phi = Arr<T>::phi(L);
     const T* rhs = Arr<T>::rhs(L);
+    // One launch per half pass (bulk nodes and subgrid points together)
+    // when no Neumann subgrid points exist and the boundary copy after each
+    // half pass is either empty (all Dirichlet) or the periodic-z copy,
+    // which the kernel then does itself by writing every updated node of
+    // planes 0, 1 and nz-1 to its images.
+    const int* b = B.b;
+    const bool xy_dir = b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0;
+    const bool zper = b[4] == 2 && b[5] == 2, zdir = b[4] == 0 && b[5] == 0;
+    const bool merged = !L.has_neumann_sub && xy_dir && (zper || zdir) && L.d.nz >= 2;
+    const int wtz = (merged && zper) ? 1 : 0;
     if (L.n_int) {
       ++c->nlaunch;
-      k_interior<T><<<cdiv(L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev);
+      k_interior<T><<<cdiv(L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev,
+                                                        L.d.nz, wtz);
     }
     neumann_int<T>(L, phi);
     const Ranges R = ranges(L.d, B.b, true);
-    const int nyr = R.iymax - R.iymin + 1, nzr = R.izmax - R.izmin + 1;
+    const int izmax = wtz ? std::min(R.izmax, L.d.nz - 1) : R.izmax;
+    const int nyr = R.iymax - R.iymin + 1, nzr = izmax - R.izmin + 1;
     const int nhalf = (R.ixmax - R.ixmin) / 2 + 1;
     for (int parity = 0; parity < 2; ++parity) {
-      if (nyr > 0 && nzr > 0 && nhalf > 0) {
-        constexpr int zpt = ZPlanes<T>::value;
-        dim3 blk(32, 8), grd(cdiv(nhalf, 32), cdiv(nyr, 8), cdiv(nzr, zpt));
-        ++c->nlaunch;
-        int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
-        k_sor_bulk<T, zpt><<<grd, blk, 0, s>>>(phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin,
-                                               R.izmax, parity, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1);
-        c->prof_end(pe);
-      }
       int nsub = L.sub[parity].n;
       // Interior conductor nodes were set by k_interior at the start of the
       // pass; no kernel of the pass writes them unless Neumann subgrid
@@ -1070,13 +1124,27 @@ struct Solver {
       // set again after each half pass.
       CondArgs<T> ca = cond_args<T>(L);
       if (!L.has_neumann_sub) ca.nint = 0;
-      if (nsub + ca.nint) {
+      constexpr int zpt = ZPlanes<T>::value;
+      const bool bulk = nyr > 0 && nzr > 0 && nhalf > 0;
+      dim3 blk(32, 8);
+      const unsigned gx = bulk ? cdiv(nhalf, 32) : 1, gy = bulk ? cdiv(nyr, 8) : 1;
+      const int nbz = bulk ? (int)cdiv(nzr, zpt) : 0;
+      const int nspz = merged ? (int)cdiv((size_t)nsub, 256u * gx * gy) : 0;
+      if (nbz + nspz > 0) {
+        ++c->nlaunch;
+        int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
+        k_sor_bulk<T, zpt><<<dim3(gx, gy, nbz + nspz), blk, 0, s>>>(
+            phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, izmax, parity, (T)k.cx, (T)k.cy,
+            (T)k.cz, (T)k.spm1, L.d.nz, wtz, nbz, ca, B, k, (int)usev, o->lcndbndy);
+        c->prof_end(pe);
+      }
+      if (!merged && nsub + ca.nint) {
         ++c->nlaunch;
         k_special_sor<T><<<cdiv(nsub + ca.nint, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, ca, parity, B, k,
                                                                     (int)usev, (int)usev, o->lcndbndy);
       }
       neumann_int<T>(L, phi);
-      bc<T>(L, phi, false);
+      if (!merged) bc<T>(L, phi, false);
     }
   }
 

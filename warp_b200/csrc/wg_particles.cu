@@ -41,13 +41,20 @@ __device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
 }
 
 // setrho3ddirect1 (w3d.F:7757-7960) with 64-bit fixed-point weights. A CTA
-// takes a chunk of DEP_NT*DEP_PPT consecutive particles. Their 8 CIC weights
-// per node are first summed over runs of equal cell within each warp (sorted
-// particles give long runs), then into a shared-memory copy of the chunk's
-// bounding box of nodes, which is added to the global accumulator once; when
-// the box is larger than DEP_BOX nodes (unsorted particles) the run sums go
-// straight to global memory. Integer adds commute, so the result does not
-// depend on any of these orders.
+// takes a chunk of DEP_NT*DEP_PPT consecutive particles; warp w of the CTA
+// takes the DEP_PPT*32 consecutive particles starting at w*32*DEP_PPT, 32 at
+// a time (coalesced loads). Each particle's 8 CIC weights are rounded to
+// integers (2^46 per full weight) and summed three ways:
+//  - while a whole warp-load of 32 particles sits in one cell and it is the
+//    same cell as the previous warp-load (sorted particles: a cell holds
+//    hundreds), every lane keeps adding its weights in registers; the warp
+//    sums its lanes once, when the cell changes;
+//  - otherwise runs of equal cell inside the warp-load are summed with a
+//    segmented scan whose length follows the longest run;
+//  - the sums go to a shared-memory copy of the chunk's bounding box of
+//    nodes, added to the global accumulator at the end, or straight to global
+//    memory when the box is larger than DEP_BOX nodes (unsorted particles).
+// Integer adds commute, so rho does not depend on any of these orders.
 constexpr int DEP_NT = 256, DEP_PPT = 16, DEP_BOX = 4096;
 
 __device__ inline bool dep_cell(const double* xp, const double* yp, const double* zp, const double* gaminv,
@@ -60,14 +67,23 @@ __device__ inline bool dep_cell(const double* xp, const double* yp, const double
   return true;
 }
 
+// Adds v to node (i, j, k) of the box or of the global accumulator.
+__device__ inline void dep_add(unsigned long long* box, bool use_box, int ox, int oy, int oz, int bx, int by,
+                               unsigned long long* acc, const GridP& g, int i, int j, int k, unsigned long long v) {
+  if (use_box)
+    atomicAdd(&box[(i - ox) + bx * ((j - oy) + by * (k - oz))], v);
+  else
+    atomicAdd(acc + i + (g.nx + 1) * (j + (g.ny + 1) * k), v);
+}
+
 __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ xp, const double* __restrict__ yp,
                                                     const double* __restrict__ zp,
                                                     const double* __restrict__ gaminv, int64_t np, GridP g,
                                                     unsigned long long* __restrict__ acc) {
   __shared__ unsigned long long box[DEP_BOX];
   __shared__ int bmin[3], bmax[3];
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int64_t base = (int64_t)blockIdx.x * (DEP_NT * DEP_PPT);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t base = (int64_t)blockIdx.x * (DEP_NT * DEP_PPT) + (int64_t)warp * (32 * DEP_PPT) + lane;
   if (tid < 3) {
     bmin[tid] = 0x7fffffff;
     bmax[tid] = -1;
@@ -77,18 +93,21 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
   for (int j = 0; j < DEP_PPT; ++j) {
     int c[3];
     double f1, f2, f3;
-    if (dep_cell(xp, yp, zp, gaminv, base + tid + (int64_t)j * DEP_NT, np, g, c[0], c[1], c[2], f1, f2, f3))
+    if (dep_cell(xp, yp, zp, gaminv, base + 32 * j, np, g, c[0], c[1], c[2], f1, f2, f3))
       for (int d = 0; d < 3; ++d) {
         lo[d] = min(lo[d], c[d]);
         hi[d] = max(hi[d], c[d]);
       }
   }
   for (int d = 0; d < 3; ++d) {
-    if (hi[d] >= 0) {
+    lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+    hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
+  }
+  if (lane == 0 && hi[0] >= 0)
+    for (int d = 0; d < 3; ++d) {
       atomicMin(&bmin[d], lo[d]);
       atomicMax(&bmax[d], hi[d]);
     }
-  }
   __syncthreads();
   // node box [bmin, bmax+1] in each direction
   const int ox = bmin[0], oy = bmin[1], oz = bmin[2];
@@ -99,37 +118,80 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
     for (int i = tid; i < bx * by * bz; i += DEP_NT) box[i] = 0ull;
   __syncthreads();
   if (any) {
-    const int sx = 1, sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+    // register sums of the warp's current uniform cell (ci, cj, ck), or ci < 0
+    unsigned long long s[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) s[n] = 0ull;
+    int ci = -1, cj = 0, ck = 0;
+    auto flush = [&]() {
+      if (ci < 0) return;
+#pragma unroll
+      for (int n = 0; n < 8; ++n) {
+        unsigned long long v = s[n];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        s[n] = v;
+      }
+      // lane n < 8 adds node n
+      unsigned long long mine = 0ull;
+#pragma unroll
+      for (int n = 0; n < 8; ++n)
+        if (lane == n) mine = s[n];
+      if (lane < 8 && mine)
+        dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ci + (lane & 1), cj + ((lane >> 1) & 1), ck + (lane >> 2),
+                mine);
+#pragma unroll
+      for (int n = 0; n < 8; ++n) s[n] = 0ull;
+      ci = -1;
+    };
     for (int j = 0; j < DEP_PPT; ++j) {
       int ii = 0, jj = 0, kk = 0;
       double u1 = 0., v1 = 0., w1 = 0.;
-      const bool live = dep_cell(xp, yp, zp, gaminv, base + tid + (int64_t)j * DEP_NT, np, g, ii, jj, kk, u1, v1, w1);
+      const bool live = dep_cell(xp, yp, zp, gaminv, base + 32 * j, np, g, ii, jj, kk, u1, v1, w1);
       const int key = live ? ii + (g.nx + 1) * (jj + (g.ny + 1) * kk) : -1;
+      const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+      unsigned long long w[8];
+#pragma unroll
+      for (int n = 0; n < 8; ++n) {
+        const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
+        const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
+        w[n] = live ? (unsigned long long)llrint(wgt * kFixScale) : 0ull;
+      }
+      const int key0 = __shfl_sync(0xffffffffu, key, 0);
+      if (__all_sync(0xffffffffu, live && key == key0)) {
+        const int i0 = __shfl_sync(0xffffffffu, ii, 0), j0 = __shfl_sync(0xffffffffu, jj, 0),
+                  k0 = __shfl_sync(0xffffffffu, kk, 0);
+        if (ci != i0 || cj != j0 || ck != k0) {
+          flush();
+          ci = i0;
+          cj = j0;
+          ck = k0;
+        }
+#pragma unroll
+        for (int n = 0; n < 8; ++n) s[n] += w[n];
+        continue;
+      }
+      flush();
+      // runs of equal key inside this warp-load: segmented suffix sums
       const int knext = __shfl_down_sync(0xffffffffu, key, 1);
       const bool tail = (lane == 31) || (knext != key);
       const unsigned tails = __ballot_sync(0xffffffffu, tail);
       const int seg_end = __ffs(tails & (0xffffffffu << lane)) - 1;
       const int kprev = __shfl_up_sync(0xffffffffu, key, 1);
       const bool head = ((lane == 0) || (kprev != key)) && live;
-      const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+      const int runlen = __reduce_max_sync(0xffffffffu, head ? seg_end - lane + 1 : 1);
 #pragma unroll
       for (int n = 0; n < 8; ++n) {
-        const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
-        const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
-        unsigned long long v = live ? (unsigned long long)llrint(wgt * kFixScale) : 0ull;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
+        unsigned long long v = w[n];
+        for (int off = 1; off < runlen; off <<= 1) {
           const unsigned long long t = __shfl_down_sync(0xffffffffu, v, off);
           if (lane + off <= seg_end) v += t;
         }
-        if (head && v) {
-          if (use_box)
-            atomicAdd(&box[(ii + dx - ox) + bx * ((jj + dy - oy) + by * (kk + dz - oz))], v);
-          else
-            atomicAdd(acc + key + dx * sx + dy * sy + dz * sz, v);
-        }
+        if (head && v)
+          dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + (n & 1), jj + ((n >> 1) & 1), kk + (n >> 2), v);
       }
     }
+    flush();
   }
   if (use_box) {
     __syncthreads();
@@ -199,8 +261,11 @@ __device__ inline void gather_e(const double* __restrict__ phi, const GridP& g, 
   cellfrac((y - g.ymmin) * dyi, g.ny, j, v1);
   cellfrac((z - g.zgrid - g.zmmin) * dzi, g.nz, k, w1);
   const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
-  const int nx = g.nx, ny = g.ny;
-  auto P = [&](int a, int b, int c) { return __ldg(phi + pix(nx, ny, a, b, c)); };
+  // phi(i+a, j+b, k+c) through one base pointer and 32-bit offsets (the
+  // padded grid holds fewer than 2^31 nodes)
+  const int sy = g.nx + 3, sz = sy * (g.ny + 3);
+  const double* base = phi + ((i + 1) + sy * (j + 1) + sz * (k + 1));
+  auto P = [&](int a, int b, int c) { return __ldg(base + ((a - i) + (b - j) * sy + (c - k) * sz)); };
   ext = tdxi * (u0 * v0 * w0 * (P(i - 1, j, k) - P(i + 1, j, k)) + u1 * v0 * w0 * (P(i, j, k) - P(i + 2, j, k)) +
                 u0 * v1 * w0 * (P(i - 1, j + 1, k) - P(i + 1, j + 1, k)) +
                 u1 * v1 * w0 * (P(i, j + 1, k) - P(i + 2, j + 1, k)) +
@@ -246,7 +311,7 @@ struct PushP {
 };
 
 // padvnc3d fullv + particleboundaries3d for one particle per thread.
-__global__ void __launch_bounds__(256) k_advance(const double* __restrict__ phi, GridP g, PushP P,
+__global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ phi, GridP g, PushP P,
                                                  double* __restrict__ xp, double* __restrict__ yp,
                                                  double* __restrict__ zp, double* __restrict__ uxp,
                                                  double* __restrict__ uyp, double* __restrict__ uzp,
