@@ -128,6 +128,13 @@ int wg_conductors_export(wg_ctx* ctx, int which, int32_t* indx, double* dels, do
 int wg_solve(wg_ctx* ctx, const wg_solve_opts* opts, wg_solve_stats* stats);
 /* Relative residual of the current phi (same definition as tolkind 1). */
 int wg_relresidual(wg_ctx* ctx, double mgparam, double* out);
+/* Residual field rhs - A phi of the current phi on the finest level, as in
+ * residual3d (f3d_mgrid.F:3094-3598) with the conductor voltages imposed and
+ * without the ppp scaling (the mgform = 2 correction right-hand side,
+ * f3d_mgrid.F:340-358). out: device array in the rho layout; rhs = rho scaled
+ * by mgparam/(2 eps0 (1/dx^2+1/dy^2+1/dz^2)), so out is in volts per SOR
+ * update. Asynchronous on the context's stream. */
+int wg_residual_field(wg_ctx* ctx, double mgparam, double* out);
 
 /* ---- particles -------------------------------------------------------------- */
 

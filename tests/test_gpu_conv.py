@@ -51,9 +51,10 @@ def test_conv3_fwd_offset_and_mask():
     assert np.max(np.abs(got[..., 16:] - ref)) <= 1e-2 * np.max(np.abs(ref)) + 1e-2
 
 
-def test_conv3_dgrad_and_wgrad_match_oracle():
+@pytest.mark.parametrize("cin,cout", [(32, 16), (192, 64)])
+def test_conv3_dgrad_and_wgrad_match_oracle(cin, cout):
     from warp_b200 import unet
-    D, H, W, cin, cout = 6, 5, 20, 32, 16
+    D, H, W = 6, 5, 20
     x = _rand((D, H, W, cin), 7)
     w = _rand((27, cout, cin), 8, 0.2)
     dy = _rand((D, H, W, cout), 9)

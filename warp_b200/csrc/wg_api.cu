@@ -18,6 +18,7 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 
 int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st);
 int relresidual(wg_ctx* c, double mgparam, double* out);
+int residual_field(wg_ctx* c, double mgparam, double* out);
 int deposit(wg_ctx* c, const wg_particles* p, int zero_first);
 int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream);
 int finalize_rho(wg_ctx* c);
@@ -455,6 +456,11 @@ int wg_solve(wg_ctx* c, const wg_solve_opts* opts, wg_solve_stats* stats) {
   if (!c) { set_error("null context"); return WG_EINVAL; }
   if (!c->cond.finalized) { set_error("wg_solve: conductors added but not finalized"); return WG_ESTATE; }
   return solve(c, opts, stats);
+}
+
+int wg_residual_field(wg_ctx* c, double mgparam, double* out) {
+  if (!c || !out) { set_error("null argument"); return WG_EINVAL; }
+  return residual_field(c, mgparam, out);
 }
 
 int wg_relresidual(wg_ctx* c, double mgparam, double* out) {

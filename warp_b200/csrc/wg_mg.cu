@@ -1441,6 +1441,34 @@ int relresidual(wg_ctx* c, double mgparam, double* out) {
   return WG_OK;
 }
 
+// Residual field of the current phi on the finest level into out (rho
+// layout, device memory): rhs - A phi with the conductor voltages imposed,
+// the right-hand side of the correction equation of the residual-correction
+// form (mgform = 2, f3d_mgrid.F:340-358). Zero at conductor and boundary
+// nodes that are not updated.
+int residual_field(wg_ctx* c, double mgparam, double* out) {
+  wg_solve_opts o{mgparam, 0., 0, 101, 1, 1, 1, 0, 1, 0};
+  Solver S{c, &o, {}, c->stream, false};
+  for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
+  cudaStream_t s = c->stream;
+  Level& L0 = c->lv[0];
+  const LevelDims& d = L0.d;
+  double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
+  double reps0c = mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
+  WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
+  WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
+  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
+  S.box<double>(0);
+  WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (L0.n_int) {
+    ++c->nlaunch;
+    k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);
+  }
+  S.residual<double, 2, double>(0, c->phisave, out, true, true, nullptr);
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
 // Shared memory of the fused sweep exceeds the 48 KB default for FP64.
 int configure_kernels() {
   WG_TRY_CUDA(cudaFuncSetAttribute(k_sor_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -371,9 +371,9 @@ int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, con
 
 int wg_conv3_wgrad(const void* xT, const void* dyT, int D, int H, int W, int cin, int cout, float* dw, int* err,
                    void* stream) {
-  if (!xT || !dyT || !dw || !err || D < 1 || H < 1 || W < 1 || cin < 16 || cin % 16 || cin > 128 || cout < 1 ||
+  if (!xT || !dyT || !dw || !err || D < 1 || H < 1 || W < 1 || cin < 16 || cin % 16 || cin > 256 || cout < 1 ||
       cout > 128) {
-    set_error("wg_conv3_wgrad: bad arguments (cin multiple of 16 up to 128, cout <= 128)");
+    set_error("wg_conv3_wgrad: bad arguments (cin multiple of 16 up to 256, cout <= 128)");
     return WG_EINVAL;
   }
   // M = 128 keeps accumulator row m in TMEM lane m (output channels padded with zeros)

@@ -263,6 +263,19 @@ class MultiGridB200(FieldSolver):
         _lib.check(_lib.lib.wg_relresidual(self._h, self.mgparam, ctypes.byref(out)))
         return out.value
 
+    def residual_field(self, out=None):
+        """rhs - A phi of the current phi (conductor voltages imposed), in the
+        rho layout: the right-hand side of the residual-correction equation,
+        in volts per SOR update. Returns a float64 device tensor indexed
+        [ix, iy, iz]."""
+        self._bind_stream()
+        self.getconductorobject()
+        n = (self.nx + 1) * (self.ny + 1) * (self.nz + 1)
+        if out is None:
+            out = torch.empty(n, dtype=torch.float64, device=self.device)
+        _lib.check(_lib.lib.wg_residual_field(self._h, self.mgparam, ctypes.c_void_p(out.data_ptr())))
+        return out.view(self.nz + 1, self.ny + 1, self.nx + 1).permute(2, 1, 0)
+
     def fetche(self, pgroup=None):
         """fetche -> fetchfieldfrompositions -> sete3d (multigrid.py:521-558,
         w3d.F:3963): E at the particles, written to pgroup.ex/ey/ez."""

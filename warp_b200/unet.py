@@ -150,37 +150,64 @@ class UNet3D(torch.nn.Module):
 
 
 class WarmStart:
-    """Scaling around the solver's arrays. The network sees, on the nodes
-    0..nx-1, 0..ny-1, 0..nz-1 (z, y, x order), phi^(n-1)/s and
-    rho * rho_factor / s with s = max|phi^(n-1)|, and predicts
-    out_scale * (phi^n - phi^(n-1)) / s. With rho_factor ~ dx^2/eps0 both
-    inputs are O(1) whatever the beam current."""
+    """The learned guess around the solver's arrays. For a step n the network
+    sees, on the nodes 0..nx-1, 0..ny-1, 0..nz-1 (z, y, x order):
+      channel 0: r / s_r, with r = rhs(rho^n) - A phi^(n-1) the residual
+                 field of the previous potential under the new charge
+                 (MultiGridB200.residual_field) and s_r its rms;
+      channel 1: phi^(n-1) / s_p, with s_p the rms of phi^(n-1).
+    Both are functions of (rho^n, phi^(n-1)) only. It predicts
+    (phi^n - phi^(n-1)) / (s_r * out_scale), which is O(1) because the
+    correction is the residual passed through the inverse Laplacian;
+    out_scale is fixed from the training snapshots."""
 
-    def __init__(self, net, rho_factor, out_scale=30.0):
+    # Low-pass filters applied to the prediction before it is added: the
+    # multigrid judges a guess by its residual, and the bf16 output carries
+    # rounding and fitting noise whose Laplacian is as large as the residual
+    # it removes. "box2": two passes of a 3x3x3 mean; "coarse4": mean over
+    # 4x4x4 blocks, then trilinear interpolation back.
+    SMOOTH = ("none", "box2", "coarse4")
+
+    def __init__(self, net, out_scale=1.0, smooth="coarse4"):
+        if smooth not in self.SMOOTH:
+            raise ValueError("smooth must be one of %s" % (self.SMOOTH,))
         self.net = net
-        self.rho_factor = float(rho_factor)
         self.out_scale = float(out_scale)
+        self.smooth = smooth
 
-    def _core(self, rho, phi):
-        return rho[:-1, :-1, :-1].permute(2, 1, 0), phi[1:-2, 1:-2, 1:-2].permute(2, 1, 0)
+    def lowpass(self, d):
+        """d: [D,H,W] float32 prediction -> filtered copy."""
+        if self.smooth == "none":
+            return d
+        u = d[None, None]
+        if self.smooth == "box2":
+            for _ in range(2):
+                u = torch.nn.functional.avg_pool3d(u, 3, stride=1, padding=1, count_include_pad=False)
+        else:
+            c = torch.nn.functional.avg_pool3d(u, 4, stride=4)
+            u = torch.nn.functional.interpolate(c, size=d.shape, mode="trilinear", align_corners=False)
+        return u[0, 0]
 
-    def inputs(self, rho, phi_prev):
-        """rho: solver.rho [nx+1,ny+1,nz+1] (Fortran view); phi_prev: solver.phi
-        [nx+3,ny+3,nz+3]. Returns ([D,H,W,2] bf16, s)."""
-        r, p = self._core(rho, phi_prev)
-        s = float(p.abs().max().item()) or 1.0
-        x = torch.empty(r.shape + (2,), dtype=torch.bfloat16, device=rho.device)
-        x[..., 0] = (r * (self.rho_factor / s)).to(torch.bfloat16)
-        x[..., 1] = (p / s).to(torch.bfloat16)
-        return x, s
+    @staticmethod
+    def _core_phi(phi):
+        return phi[1:-2, 1:-2, 1:-2].permute(2, 1, 0)
 
-    def pair(self, rho, phi_prev, phi):
-        """Training pair (inputs, target) of one solved step."""
-        x, s = self.inputs(rho, phi_prev)
-        _, p0 = self._core(rho, phi_prev)
-        _, p1 = self._core(rho, phi)
-        y = ((p1 - p0) * (self.out_scale / s)).to(torch.bfloat16).contiguous()
-        return x.contiguous(), y
+    def inputs(self, solver):
+        """([D,H,W,2] bf16 inputs, s_r) from the solver's rho and phi (phi
+        holds phi^(n-1))."""
+        r = solver.residual_field()[:-1, :-1, :-1].permute(2, 1, 0)
+        p = self._core_phi(solver.phi)
+        s_r = float(torch.sqrt(torch.mean(r * r)).item()) or 1.0
+        s_p = float(torch.sqrt(torch.mean(p * p)).item()) or 1.0
+        x = torch.empty(r.shape + (2,), dtype=torch.bfloat16, device=r.device)
+        x[..., 0] = (r * (1.0 / s_r)).to(torch.bfloat16)
+        x[..., 1] = (p * (1.0 / s_p)).to(torch.bfloat16)
+        return x.contiguous(), s_r
+
+    def target(self, phi_prev, phi, s_r):
+        """Training target of one solved step."""
+        d = self._core_phi(phi) - self._core_phi(phi_prev)
+        return (d * (1.0 / (s_r * self.out_scale))).to(torch.bfloat16).contiguous()
 
     @torch.no_grad()
     def predict(self, x2):
@@ -192,8 +219,27 @@ class WarmStart:
     def guess(self, solver):
         """Adds the predicted change to solver.phi (which holds phi^(n-1)) on
         the nodes 0..n-1; the solver's boundary handling sets the rest."""
-        x, s = self.inputs(solver.rho, solver.phi)
-        d = self.predict(x)
+        x, s_r = self.inputs(solver)
+        d = self.lowpass(self.predict(x))
+        # Dirichlet boundary planes keep their values: the solver never
+        # updates them, so a change there would change the problem
+        b = solver.bounds
+        if b[0] == 0:
+            d[:, :, 0] = 0.
+        if b[2] == 0:
+            d[:, 0, :] = 0.
+        if b[4] == 0:
+            d[0, :, :] = 0.
         interior = solver.phi[1:-2, 1:-2, 1:-2]
-        interior.add_((d * (s / self.out_scale)).permute(2, 1, 0).to(torch.float64))
+        interior.add_((d * (s_r * self.out_scale)).permute(2, 1, 0).to(torch.float64))
         check_errors(solver.device)
+
+    def state(self):
+        return {"weights": {k: v.detach().to(torch.bfloat16).cpu() for k, v in self.net.state_dict().items()},
+                "out_scale": self.out_scale, "smooth": self.smooth}
+
+    @classmethod
+    def load(cls, state, device="cuda"):
+        net = UNet3D(device=device)
+        net.load_state_dict({k: v.float().to(device) for k, v in state["weights"].items()})
+        return cls(net, out_scale=state["out_scale"], smooth=state.get("smooth", "coarse4"))

@@ -1,15 +1,25 @@
-"""Training of the learned multigrid warm start on snapshots of the plain
-solver (workload D: 128x128x256 cells over the 8 cm x 8 cm x 1 m box).
+"""Training and evaluation of the learned multigrid warm start.
 
-Each snapshot is one PIC step of a randomized beam -- current uniform in
-1-50 mA, emittance log-uniform in 1-20 mm mrad, envelope mismatch uniform
-in 0-30 % -- taken after the deposit: inputs rho^n and phi^(n-1), target
-phi^n from the FP64 multigrid solved to a 1e-8 relative residual. The
-network is trained on the GPU with the library's tensor-core convolutions
-(forward, data and weight gradients) and Adam; 10 % of the snapshots are
-held out.
+Snapshots come from the plain solver running randomized beams on one of the
+synthetic workloads (by default the 128x128x256-cell grid over the
+8 cm x 8 cm x 1 m box). The beam parameters are drawn as follows:
+- current uniform in 1-50 mA;
+- emittance log-uniform in 1-20 mm mrad;
+- envelope mismatch uniform in 0-30 %.
 
-    python -m warp_b200.warmstart_train --snapshots 400 --epochs 8 --out w.pt
+Each snapshot is one PIC step, taken after the deposit. Its inputs are the
+residual field of phi^(n-1) under rho^n and phi^(n-1) itself. Its target is
+phi^n from the FP64 multigrid solved to a 1e-8 relative residual. The network
+is trained on the GPU with the library's tensor-core convolutions (forward,
+data and weight gradients) and Adam; 10 % of the snapshots are held out.
+
+The evaluation runs fresh beams. At every step it solves to a 1e-6 relative
+residual twice from the same rho^n: once warm-started from phi^(n-1) (the
+plain method), and once from phi^(n-1) plus the network's correction. It
+reports the V-cycles of both, and the relative residual right after each
+start.
+
+    python -m warp_b200.warmstart_train --snapshots 400 --epochs 6 --out ws.pt
 """
 import argparse
 import json
@@ -20,7 +30,6 @@ import numpy as np
 import torch
 
 from . import pic
-from .constants import eps0
 from .particles import semigaussian_device
 from .unet import UNet3D, WarmStart, check_errors
 
@@ -32,46 +41,82 @@ def beam_params(rng):
     return current, emit, mismatch
 
 
-def make_warmstart(net, cfg):
-    dx = (cfg["xmmax"] - cfg["xmmin"]) / cfg["nx"]
-    return WarmStart(net, rho_factor=10.0 * dx * dx / eps0, out_scale=30.0)
+def beam_run(workload, rng, gen, device, npart=None, mgtol=1e-8, sort_interval=4, precision="fp64"):
+    """A plain FP64 run of one randomized beam, with its initial field solved."""
+    current, emit, mismatch = beam_params(rng)
+    cfg = pic.workload(workload, current=current, mismatch=mismatch, angle_rms=emit / (2 * 4e-3),
+                       seed=int(rng.integers(1 << 30)))
+    if npart:
+        cfg["npart"] = npart
+    beam = semigaussian_device(cfg["npart"], gen, radius=cfg["radius"], mismatch=mismatch,
+                               angle_rms=cfg["angle_rms"], device=device)
+    run = pic.ESPIC(cfg, precision=precision, tolkind="relres", mgtol=mgtol, device=device, particles=beam,
+                    sort_interval=sort_interval)
+    run.generate()
+    return run, {"current": current, "emittance": emit, "mismatch": mismatch}
 
 
-def snapshots(n, seed=0, device="cuda", steps_per_beam=4, skip=2, npart=None, log=print):
-    """Returns (inputs [n] of [D,H,W,2] bf16, targets [n] of [D,H,W] bf16,
-    meta list)."""
+def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=4, skip=2, npart=None, log=print):
+    """Returns (inputs [n] of [D,H,W,2] bf16, residual scales s_r [n],
+    raw corrections phi^n - phi^(n-1) [n] of [D,H,W] float32, meta)."""
     rng = np.random.default_rng(seed)
     gen = torch.Generator(device=device).manual_seed(seed)
-    xs, ys, meta = [], [], []
+    ws = WarmStart(None)
+    xs, srs, ds, meta = [], [], [], []
     t0 = time.time()
     while len(xs) < n:
-        current, emit, mismatch = beam_params(rng)
-        cfg = pic.workload("D", current=current, mismatch=mismatch, angle_rms=emit / (2 * 4e-3),
-                           seed=int(rng.integers(1 << 30)))
-        if npart:
-            cfg["npart"] = npart
-        beam = semigaussian_device(cfg["npart"], gen, radius=cfg["radius"], mismatch=mismatch,
-                                   angle_rms=cfg["angle_rms"], device=device)
-        run = pic.ESPIC(cfg, tolkind="relres", mgtol=1e-8, device=device, particles=beam, sort_interval=4)
-        ws = make_warmstart(None, cfg)
-        run.generate()
+        run, m = beam_run(workload, rng, gen, device, npart)
         s = run.solver
         for k in range(skip + steps_per_beam):
-            s.advance(run.pgroup, run.dt, prwall=cfg["pipe_radius"])
+            s.advance(run.pgroup, run.dt, prwall=run.cfg["pipe_radius"])
             s.loadrho()
-            phi_prev = s.phi.clone()
-            s.solve()
             if k >= skip and len(xs) < n:
-                x, y = ws.pair(s.rho, phi_prev, s.phi)
+                x, s_r = ws.inputs(s)
+                phi_prev = s.phi.clone()
+                s.solve()
+                ds.append((WarmStart._core_phi(s.phi) - WarmStart._core_phi(phi_prev)).float().contiguous())
                 xs.append(x)
-                ys.append(y)
-                meta.append({"current": current, "emittance": emit, "mismatch": mismatch, "step": k})
+                srs.append(s_r)
+                meta.append(dict(m, step=k))
+            else:
+                s.solve()
         del run
     log("snapshots: %d in %.1f s" % (len(xs), time.time() - t0))
-    return xs, ys, meta
+    return xs, srs, ds, meta
 
 
-def train(xs, ys, epochs=8, lr=2e-3, seed=0, device="cuda", log=print):
+def fit_out_scale(srs, ds):
+    """Median over snapshots of rms(phi^n - phi^(n-1)) / s_r."""
+    r = [float(torch.sqrt(torch.mean(d * d)).item()) / s for d, s in zip(ds, srs)]
+    return float(np.median(r))
+
+
+def targets(srs, ds, out_scale):
+    return [(d * (1.0 / (s * out_scale))).to(torch.bfloat16).contiguous() for d, s in zip(ds, srs)]
+
+
+def _pad16(x2):
+    x = torch.zeros(x2.shape[:3] + (16,), dtype=torch.bfloat16, device=x2.device)
+    x[..., :2] = x2
+    return x
+
+
+def laplacian(u):
+    """7-point Laplacian (grid units) of [D,H,W] u on the interior nodes."""
+    c = u[1:-1, 1:-1, 1:-1]
+    return (u[:-2, 1:-1, 1:-1] + u[2:, 1:-1, 1:-1] + u[1:-1, :-2, 1:-1] + u[1:-1, 2:, 1:-1] + u[1:-1, 1:-1, :-2] +
+            u[1:-1, 1:-1, 2:] - 6. * c)
+
+
+def guess_loss(pred, y, lap_weight):
+    """MSE of the correction plus lap_weight times the MSE of its Laplacian:
+    the multigrid judges a guess by its residual, which the Laplacian of the
+    error dominates, so high-frequency error costs more than its size."""
+    e = pred - y.float()
+    return torch.mean(e * e) + lap_weight * torch.mean(laplacian(e) ** 2)
+
+
+def train(xs, ys, epochs=6, lr=2e-3, seed=0, device="cuda", lap_weight=1.0, log=print):
     net = UNet3D(seed=seed, device=device)
     opt = torch.optim.Adam(net.parameters(), lr=lr)
     n = len(xs)
@@ -81,10 +126,8 @@ def train(xs, ys, epochs=8, lr=2e-3, seed=0, device="cuda", log=print):
         t0 = time.time()
         tot = 0.0
         for i in rng.permutation(n):
-            x = torch.zeros(xs[i].shape[:3] + (16,), dtype=torch.bfloat16, device=device)
-            x[..., :2] = xs[i]
-            pred = net(x)
-            loss = torch.mean((pred - ys[i].float()) ** 2)
+            pred = net(_pad16(xs[i]))
+            loss = guess_loss(pred, ys[i], lap_weight)
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()
@@ -98,34 +141,89 @@ def train(xs, ys, epochs=8, lr=2e-3, seed=0, device="cuda", log=print):
 
 
 @torch.no_grad()
-def evaluate(net, xs, ys, device="cuda"):
+def evaluate(net, xs, ys):
     """Held-out MSE of the network and of the zero prediction (the plain
     warm start phi^(n-1))."""
     m, m0 = 0.0, 0.0
     for x2, y in zip(xs, ys):
-        x = torch.zeros(x2.shape[:3] + (16,), dtype=torch.bfloat16, device=device)
-        x[..., :2] = x2
-        p = net(x)
+        p = net(_pad16(x2))
         m += float(torch.mean((p - y.float()) ** 2))
         m0 += float(torch.mean(y.float() ** 2))
     return m / len(xs), m0 / len(xs)
 
 
+@torch.no_grad()
+def vcycle_study(ws, workload="D", nbeams=2, steps=6, seed=1000, device="cuda", npart=None, precision="fp64",
+                 mgtol=1e-6):
+    """V-cycles to mgtol from the plain warm start and from the learned
+    guess, on the same rho^n, over fresh randomized beams."""
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device).manual_seed(seed)
+    rows = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(nbeams):
+        run, _m = beam_run(workload, rng, gen, device, npart, mgtol=mgtol, precision=precision)
+        s = run.solver
+        for k in range(steps):
+            s.advance(run.pgroup, run.dt, prwall=run.cfg["pipe_radius"])
+            s.loadrho()
+            phi_prev = s.phi.clone()
+            r_plain = s.relresidual()
+            s.solve()
+            n_plain = s.mgiters
+            s.phi.copy_(phi_prev)
+            e0.record()
+            ws.guess(s)
+            e1.record()
+            torch.cuda.synchronize()
+            r_learned = s.relresidual()
+            s.solve()
+            rows.append({"step": k, "vc_plain": n_plain, "vc_learned": s.mgiters, "relres_start_plain": r_plain,
+                         "relres_start_learned": r_learned, "guess_ms": e0.elapsed_time(e1)})
+        del run
+    vp = float(np.mean([r["vc_plain"] for r in rows]))
+    vl = float(np.mean([r["vc_learned"] for r in rows]))
+    return {"vcycles_plain": vp, "vcycles_learned": vl,
+            "relres_start_plain": float(np.median([r["relres_start_plain"] for r in rows])),
+            "relres_start_learned": float(np.median([r["relres_start_learned"] for r in rows])),
+            "guess_ms": float(np.median([r["guess_ms"] for r in rows])), "steps": len(rows)}
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="D")
     ap.add_argument("--snapshots", type=int, default=400)
-    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--npart", type=int, default=None)
     ap.add_argument("--out", default="warmstart_weights.pt")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--study-beams", type=int, default=2)
+    ap.add_argument("--study-steps", type=int, default=6)
+    ap.add_argument("--lap-weight", type=float, default=1.0)
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     args = ap.parse_args()
     torch.cuda.set_device(0)
-    xs, ys, meta = snapshots(args.snapshots, seed=args.seed, npart=args.npart)
+    xs, srs, ds, meta = snapshots(args.snapshots, workload=args.workload, seed=args.seed, npart=args.npart)
+    out_scale = fit_out_scale(srs, ds)
+    ys = targets(srs, ds, out_scale)
+    del ds
     nval = max(1, len(xs) // 10)
-    net, hist = train(xs[nval:], ys[nval:], epochs=args.epochs, seed=args.seed)
+    t0 = time.time()
+    net, hist = train(xs[nval:], ys[nval:], epochs=args.epochs, seed=args.seed, lap_weight=args.lap_weight)
+    train_s = time.time() - t0
     mse, mse0 = evaluate(net, xs[:nval], ys[:nval])
-    print(json.dumps({"heldout_mse": mse, "heldout_mse_zero_guess": mse0, "ratio": mse / mse0, "train": hist}))
-    torch.save({k: v.detach().cpu() for k, v in net.state_dict().items()}, args.out)
+    study = {}
+    for sm in WarmStart.SMOOTH:
+        ws = WarmStart(net, out_scale=out_scale, smooth=sm)
+        study[sm] = vcycle_study(ws, workload=args.workload, nbeams=args.study_beams, steps=args.study_steps,
+                                 npart=args.npart, precision=args.precision)
+    best = min(study, key=lambda k: study[k]["vcycles_learned"])
+    ws = WarmStart(net, out_scale=out_scale, smooth=best)
+    print(json.dumps({"workload": args.workload, "snapshots": len(xs), "heldout": nval, "epochs": args.epochs,
+                      "lap_weight": args.lap_weight,
+                      "out_scale": out_scale, "train_s": train_s, "heldout_mse": mse,
+                      "heldout_mse_zero_guess": mse0, "ratio": mse / mse0, "train": hist, "study": study}))
+    torch.save(ws.state(), args.out)
 
 
 if __name__ == "__main__":
