@@ -848,7 +848,7 @@ __global__ void __launch_bounds__(256) k_restrict(const T* __restrict__ res, T* 
 // consecutive fine planes per thread, all loads issued before the sums;
 // 32-bit offsets. The weight products keep the reference's left-to-right
 // order, ((wx' * wy') * wz') * q, with the x-y part formed once per thread.
-template <typename T, int ZPT>
+template <typename T, int ZPT, bool ZC>
 __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __restrict__ pc, int nx, int ny,
                                                 int nxc, int nyc, int ixmin, int ixmax, int iymin, int iymax,
                                                 int izmin, int izmax, const int32_t* __restrict__ ej,
@@ -880,10 +880,12 @@ __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __
       q[k][1] = b[1];
       q[k][2] = b[syc];
       q[k][3] = b[syc + 1];
-      q[k][4] = b[szc];
-      q[k][5] = b[szc + 1];
-      q[k][6] = b[szc + syc];
-      q[k][7] = b[szc + syc + 1];
+      if (ZC) {
+        q[k][4] = b[szc];
+        q[k][5] = b[szc + 1];
+        q[k][6] = b[szc + syc];
+        q[k][7] = b[szc + syc + 1];
+      }
       f[k] = phi[f0 + k * sz];
     }
   }
@@ -891,8 +893,11 @@ __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __
   for (int k = 0; k < ZPT; ++k) {
     if (!ok[k]) continue;
     const T z = wz[k], z1 = one - z;
-    phi[f0 + k * sz] = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3] +
-                       a00 * z * q[k][4] + a10 * z * q[k][5] + a01 * z * q[k][6] + a11 * z * q[k][7];
+    if (ZC)
+      phi[f0 + k * sz] = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3] +
+                         a00 * z * q[k][4] + a10 * z * q[k][5] + a01 * z * q[k][6] + a11 * z * q[k][7];
+    else  // z not coarsened: wz = 0 exactly, the z+1 terms add zeros
+      phi[f0 + k * sz] = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3];
   }
 }
 
@@ -1217,8 +1222,12 @@ struct Solver {
       if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin) {
         ++c->nlaunch;
         int pe = prof_begin(l, WG_PROF_EXPAND0, (double)L.nr);
-        k_expand<T, zpt><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny, R.ixmin,
-                                              R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
+        if (dc.nz == d.nz)
+          k_expand<T, zpt, false><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
+                                                       R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
+        else
+          k_expand<T, zpt, true><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
+                                                      R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
         c->prof_end(pe);
       }
       bc<T>(L, Arr<T>::phi(L), false);
