@@ -316,13 +316,14 @@ class MultiGridB200(FieldSolver):
                                            cdb.ctypes.data_as(_lib._dp), nzl, zlmin, dzl))
         self._lattice = (czs, cze, cdb, nzl, zlmin, dzl)
 
-    def advance(self, pgroup, dt, prwall=1.e30, prwallx=0., prwally=0.):
+    def advance(self, pgroup, dt, prwall=1.e30, prwallx=0., prwally=0., start=0, stop=None):
         """One fused fullv particle advance of padvnc3d (w3d.F:1862-1987)
         plus particleboundaries3d: gather E from phi, quad B (if a lattice
         is installed), half E kick, Boris rotation, half E kick, drift,
-        periodic z wrap and the round absorbing pipe of radius prwall."""
+        periodic z wrap and the round absorbing pipe of radius prwall.
+        start/stop restrict it to a range of the group's particles."""
         self._bind_stream()
-        s = pgroup.cstruct()
+        s = pgroup.cstruct(start, stop)
         p = _lib.PushParams(float(dt), float(prwall), float(prwallx), float(prwally),
                             int(self._lattice is not None))
         _lib.check(_lib.lib.wg_advance(self._h, ctypes.byref(s), ctypes.byref(p)))

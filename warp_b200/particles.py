@@ -41,11 +41,13 @@ class ParticleGroup:
     def np(self):
         return int(self.x.shape[0])
 
-    def cstruct(self):
+    def cstruct(self, start=0, stop=None):
+        """C view of particles start..stop-1 (all by default)."""
+        stop = self.np if stop is None else int(stop)
         s = _lib.Particles()
         for f in FIELDS:
-            setattr(s, f, getattr(self, f).data_ptr())
-        s.np = self.np
+            setattr(s, f, getattr(self, f).data_ptr() + 8 * int(start))
+        s.np = stop - int(start)
         s.q, s.m, s.w = self.q, self.m, self.w
         return s
 

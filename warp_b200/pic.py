@@ -108,5 +108,58 @@ class ESPIC:
             self.solver.solve()
             self.it += 1
 
+    def step_host(self, host, nchunks=8):
+        """One step of the drop-in mode in which the host owns the particles
+        (WARP keeps top.pgroup in host memory): `host` maps each of
+        x, y, z, ux, uy, uz, gaminv to a pinned CPU float64 tensor, read at
+        the start of the step and rewritten with the advanced particles.
+
+        The arrays cross PCIe in `nchunks` chunks. Uploads run on one copy
+        stream, and each chunk is advanced as soon as it has landed. The
+        advanced chunks go back on a second copy stream, so downloads overlap
+        the remaining uploads (PCIe is full duplex), the deposit and the
+        field solve. The step returns with the host arrays written; the
+        device state is the same as after step()."""
+        import torch
+        from .particles import FIELDS
+        pg = self.pgroup
+        n = pg.np
+        if self.sort_interval:
+            raise ValueError("step_host: the host owns the particle order; use sort_interval=0")
+        main = torch.cuda.current_stream(pg.device)
+        if not hasattr(self, "_h2d"):
+            self._h2d = torch.cuda.Stream(pg.device)
+            self._d2h = torch.cuda.Stream(pg.device)
+        h2d, d2h = self._h2d, self._d2h
+        edges = [n * k // nchunks for k in range(nchunks + 1)]
+        landed, advanced = [], []
+        h2d.wait_stream(main)
+        with torch.cuda.stream(h2d):
+            for k in range(nchunks):
+                a, b = edges[k], edges[k + 1]
+                for f in FIELDS:
+                    getattr(pg, f)[a:b].copy_(host[f][a:b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(h2d)
+                landed.append(ev)
+        for k in range(nchunks):
+            a, b = edges[k], edges[k + 1]
+            main.wait_event(landed[k])
+            if b > a:
+                self.solver.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], start=a, stop=b)
+            ev = torch.cuda.Event()
+            ev.record(main)
+            advanced.append(ev)
+        with torch.cuda.stream(d2h):
+            for k in range(nchunks):
+                a, b = edges[k], edges[k + 1]
+                d2h.wait_event(advanced[k])
+                for f in FIELDS:
+                    host[f][a:b].copy_(getattr(pg, f)[a:b], non_blocking=True)
+        self.solver.loadrho()
+        self.solver.solve()
+        main.wait_stream(d2h)
+        self.it += 1
+
     def moments(self):
         return self.solver.moments(self.pgroup)
