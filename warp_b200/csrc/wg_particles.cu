@@ -49,8 +49,8 @@ __device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
 //    same cell as the previous warp-load (sorted particles: a cell holds
 //    hundreds), every lane keeps adding its weights in registers; the warp
 //    sums its lanes once, when the cell changes;
-//  - otherwise runs of equal cell inside the warp-load are summed with a
-//    segmented scan whose length follows the longest run;
+//  - otherwise each lane adds its own weights, visiting the 8 nodes in an
+//    order rotated by lane (fewer same-address conflicts);
 //  - the sums go to a shared-memory copy of the chunk's bounding box of
 //    nodes, added to the global accumulator at the end, or straight to global
 //    memory when the box is larger than DEP_BOX nodes (unsorted particles).
@@ -150,15 +150,15 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
       const bool live = dep_cell(xp, yp, zp, gaminv, base + 32 * j, np, g, ii, jj, kk, u1, v1, w1);
       const int key = live ? ii + (g.nx + 1) * (jj + (g.ny + 1) * kk) : -1;
       const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
-      unsigned long long w[8];
-#pragma unroll
-      for (int n = 0; n < 8; ++n) {
-        const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
-        const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
-        w[n] = live ? (unsigned long long)llrint(wgt * kFixScale) : 0ull;
-      }
       const int key0 = __shfl_sync(0xffffffffu, key, 0);
       if (__all_sync(0xffffffffu, live && key == key0)) {
+        unsigned long long w[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+          const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
+          const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
+          w[n] = (unsigned long long)llrint(wgt * kFixScale);
+        }
         const int i0 = __shfl_sync(0xffffffffu, ii, 0), j0 = __shfl_sync(0xffffffffu, jj, 0),
                   k0 = __shfl_sync(0xffffffffu, kk, 0);
         if (ci != i0 || cj != j0 || ck != k0) {
@@ -172,23 +172,18 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
         continue;
       }
       flush();
-      // runs of equal key inside this warp-load: segmented suffix sums
-      const int knext = __shfl_down_sync(0xffffffffu, key, 1);
-      const bool tail = (lane == 31) || (knext != key);
-      const unsigned tails = __ballot_sync(0xffffffffu, tail);
-      const int seg_end = __ffs(tails & (0xffffffffu << lane)) - 1;
-      const int kprev = __shfl_up_sync(0xffffffffu, key, 1);
-      const bool head = ((lane == 0) || (kprev != key)) && live;
-      const int runlen = __reduce_max_sync(0xffffffffu, head ? seg_end - lane + 1 : 1);
+      // mixed cells: each lane adds its own 8 weights, visiting the nodes
+      // in an order rotated by lane so that lanes of one cell hit
+      // different nodes in the same instruction
+      if (live) {
 #pragma unroll
-      for (int n = 0; n < 8; ++n) {
-        unsigned long long v = w[n];
-        for (int off = 1; off < runlen; off <<= 1) {
-          const unsigned long long t = __shfl_down_sync(0xffffffffu, v, off);
-          if (lane + off <= seg_end) v += t;
+        for (int j = 0; j < 8; ++j) {
+          const int n = (j + lane) & 7;
+          const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
+          const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
+          const unsigned long long v = (unsigned long long)llrint(wgt * kFixScale);
+          if (v) dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + dx, jj + dy, kk + dz, v);
         }
-        if (head && v)
-          dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + (n & 1), jj + ((n >> 1) & 1), kk + (n >> 2), v);
       }
     }
     flush();
