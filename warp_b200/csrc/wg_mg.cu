@@ -379,10 +379,12 @@ __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* 
                                                   int ixmin, int ixmax, int iymin, int iymax, int izmin, int izmax,
                                                   int parity, T cx, T cy, T cz, T spm1, int nz, int wtz, int nbz,
                                                   CondArgs<T> C, Bnd B, SorCoef sc, int voltfac_on, int lcndbndy) {
-  // blocks with blockIdx.z >= nbz update the subgrid conductor points of
-  // this colour (condbndymg); they read only nodes of the other colour too
-  if ((int)blockIdx.z >= nbz) {
-    const int i = ((((int)blockIdx.z - nbz) * (int)gridDim.y + (int)blockIdx.y) * (int)gridDim.x + (int)blockIdx.x) *
+  // the first nspz z-slices of blocks update the subgrid conductor points
+  // of this colour (condbndymg); they read only nodes of the other colour
+  // too, and go first so that their dependent loads overlap the bulk blocks
+  const int nspz = (int)gridDim.z - nbz;
+  if ((int)blockIdx.z < nspz) {
+    const int i = (((int)blockIdx.z * (int)gridDim.y + (int)blockIdx.y) * (int)gridDim.x + (int)blockIdx.x) *
                       (int)(blockDim.x * blockDim.y) +
                   (int)(threadIdx.y * blockDim.x + threadIdx.x);
     if (i < (parity ? C.nsub[1] : C.nsub[0])) special_point<T>(phi, nx, ny, nz, C, parity, B, sc, voltfac_on, lcndbndy, i, wtz);
@@ -395,7 +397,7 @@ __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* 
   const int iy = iymin + (int)(blockIdx.y * blockDim.y + threadIdx.y);
   if (iy > iymax) return;
   const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int iz0 = izmin + (int)blockIdx.z * ZPT;
+  const int iz0 = izmin + ((int)blockIdx.z - nspz) * ZPT;
   const int sy = nx + 3, sz = sy * (ny + 3), ry = nx + 1, rz = ry * (ny + 1);
   const int xb = ixmin + 2 * t, odd0 = (ixmin + iy + iz0 + parity) & 1;
   const int p0 = (xb + 1) + sy * (iy + 1) + sz * (iz0 + 1);
