@@ -164,7 +164,7 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
         # by kernel instead of from the captured graph)
         kinds = {"sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE, "deposit": _lib.PROF_DEPOSIT,
                  "resid0": _lib.PROF_RESID0, "restrict0": _lib.PROF_RESTRICT0, "expand0": _lib.PROF_EXPAND0,
-                 "corr": _lib.PROF_CORR}
+                 "corr": _lib.PROF_CORR, "coarse": _lib.PROF_COARSE}
         mask = 0
         for v in kinds.values():
             mask |= 1 << v

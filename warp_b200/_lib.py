@@ -95,6 +95,7 @@ SIGNATURES = {
 }
 
 PROF_SOR0, PROF_DEPOSIT, PROF_ADVANCE, PROF_RESID0, PROF_RESTRICT0, PROF_EXPAND0, PROF_CORR = 0, 1, 2, 3, 4, 5, 6
+PROF_COARSE = 7
 
 
 def _load():

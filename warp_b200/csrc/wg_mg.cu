@@ -1217,7 +1217,9 @@ struct Solver {
       c->prof_end(pr);
       box<T>(l + 1);
       cudaMemsetAsync(Arr<T>::phi(Lc), 0, Lc.np * sizeof(T), s);
+      int pc = (l == 0) ? prof_begin(0, WG_PROF_COARSE, (double)Lc.nr) : -1;
       vcycle<T>(l + 1, false);
+      c->prof_end(pc);
       Ranges R = ranges(d, B.b, false);
       constexpr int zpt = ZPlanes<T>::value;
       dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), cdiv(R.izmax - R.izmin + 1, zpt));
