@@ -135,6 +135,11 @@ int wg_relresidual(wg_ctx* ctx, double mgparam, double* out);
  * by mgparam/(2 eps0 (1/dx^2+1/dy^2+1/dz^2)), so out is in volts per SOR
  * update. Asynchronous on the context's stream. */
 int wg_residual_field(wg_ctx* ctx, double mgparam, double* out);
+/* getese3dfromrhophi (dw3d.F:708-777), no symmetry: the electrostatic energy
+ * dx dy dz / 2 * sum(rho * phi) over the nodes 0..n of the current rho and phi,
+ * summed in the reference's order (bit-identical). *out is a host double;
+ * synchronizes the context's stream. */
+int wg_field_energy(wg_ctx* ctx, double* out);
 
 /* ---- particles -------------------------------------------------------------- */
 

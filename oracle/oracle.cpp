@@ -19,14 +19,80 @@
 // Conductor data uses the ConductorType layout of pywarp90/f3d.v:105-164.
 //
 // Build: see oracle/Makefile (g++ -O2 -ffp-contract=off, no fast-math).
+//
+// Loops whose iterations are independent (the red-black sweeps, residual,
+// restriction, prolongation, gather, push and the maxima) run on all host
+// threads; their results do not depend on the thread count. The deposit runs
+// over z slabs in two phases; its sums on the planes shared by two slabs are
+// ordered by slab, so its last bits depend on the thread count.
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <cstdlib>
+#include <thread>
 #include <vector>
 
 namespace {
+
+// Host threads for the loops whose iterations are independent (the CPU
+// baseline uses every core of the host). ORACLE_THREADS sets the count;
+// default: all hardware threads.
+int nthreads() {
+  static const int n = [] {
+    const char* e = std::getenv("ORACLE_THREADS");
+    int v = e ? std::atoi(e) : 0;
+    if (v <= 0) v = (int)std::thread::hardware_concurrency();
+    return std::max(1, v);
+  }();
+  return n;
+}
+
+// f(i) for i in [lo, hi), split into contiguous ranges over the threads;
+// serial when the loop holds less than kParMin units of work (grain = work
+// units per iteration, e.g. the nodes of a plane).
+constexpr int64_t kParMin = 1 << 17;
+
+template <typename F>
+void par_for(int64_t lo, int64_t hi, F f, int64_t grain = 1) {
+  const int64_t n = hi - lo;
+  int nt = nthreads();
+  if (nt <= 1 || n < 2 || n * grain < kParMin) {
+    for (int64_t i = lo; i < hi; ++i) f(i);
+    return;
+  }
+  nt = (int)std::min<int64_t>(nt, n);
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&, t] {
+      const int64_t a = lo + n * t / nt, b = lo + n * (t + 1) / nt;
+      for (int64_t i = a; i < b; ++i) f(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+// max over i in [lo, hi) of f(i) (non-negative values), in parallel
+template <typename F>
+double par_max(int64_t lo, int64_t hi, F f, int64_t grain = 1) {
+  if ((hi - lo) * grain < kParMin || nthreads() <= 1) {
+    double m = 0.;
+    for (int64_t i = lo; i < hi; ++i) m = std::max(m, f(i));
+    return m;
+  }
+  const int nt = std::max(1, (int)std::min<int64_t>(nthreads(), std::max<int64_t>(1, hi - lo)));
+  std::vector<double> part(nt, 0.);
+  par_for(0, nt, [&](int64_t t) {
+    const int64_t n = hi - lo, a = lo + n * t / nt, b = lo + n * (t + 1) / nt;
+    double m = 0.;
+    for (int64_t i = a; i < b; ++i) m = std::max(m, f(i));
+    part[t] = m;
+  }, kParMin);
+  double m = 0.;
+  for (double v : part) m = std::max(m, v);
+  return m;
+}
 
 const double LARGEPOS = 1.0e36;   // pywarp90/top.h:3
 const double SMALLPOS = 1.0e-36;  // pywarp90/top.h:4
@@ -561,8 +627,9 @@ struct MGParams {
 // cond_potmg, f3d_mgrid.F:2426-2470
 void cond_potmg(const Interior& I, int nx, int ny, double* phi, int mglevel, int mgform, bool mgform2init) {
   bool usev = (mglevel == 0 && (mgform == 1 || mgform2init));
-  for (int ic = I.istart[mglevel]; ic < I.istart[mglevel + 1]; ++ic)
+  par_for(I.istart[mglevel], I.istart[mglevel + 1], [&](int64_t ic) {
     phi[pidx(nx, ny, I.indx[3 * ic], I.indx[3 * ic + 1], I.indx[3 * ic + 2])] = usev ? I.volt[ic] : 0.;
+  });
 }
 
 // handlesubgrid2, f3d_mgrid.F:2628-2764
@@ -629,14 +696,15 @@ void condbndymg(Subgrid& S, int nx, int ny, int nz, double* phi, const double* r
                 int mgform) {
   double dxsqicos = dxsqic / mgparam, dysqicos = dysqic / mgparam, dzsqicos = dzsqic / mgparam;
   double voltfac = (mglevel == 0 && mgform == 1) ? 1. : 0.;
-  for (int ic = S.istart[mglevel]; ic < S.istart[mglevel + 1]; ++ic) {
+  // subgrid points of one colour read only the other colour
+  par_for(S.istart[mglevel], S.istart[mglevel + 1], [&](int64_t ic) {
     int ix = S.indx[3 * ic], iy = S.indx[3 * ic + 1], iz = S.indx[3 * ic + 2];
-    if (ix == 0 && lb[0] < 1) continue;
-    if (ix == nx && lb[1] < 1) continue;
-    if (iy == 0 && lb[2] < 1) continue;
-    if (iy == ny && lb[3] < 1) continue;
-    if (iz == 0 && lb[4] < 1) continue;
-    if (iz == nz && lb[5] < 1) continue;
+    if (ix == 0 && lb[0] < 1) return;
+    if (ix == nx && lb[1] < 1) return;
+    if (iy == 0 && lb[2] < 1) return;
+    if (iy == ny && lb[3] < 1) return;
+    if (iz == 0 && lb[4] < 1) return;
+    if (iz == nz && lb[5] < 1) return;
     double pxm = phi[pidx(nx, ny, ix - 1, iy, iz)], pxp = phi[pidx(nx, ny, ix + 1, iy, iz)];
     double pym = phi[pidx(nx, ny, ix, iy - 1, iz)], pyp = phi[pidx(nx, ny, ix, iy + 1, iz)];
     double pzm = phi[pidx(nx, ny, ix, iy, iz - 1)], pzp = phi[pidx(nx, ny, ix, iy, iz + 1)];
@@ -651,7 +719,7 @@ void condbndymg(Subgrid& S, int nx, int ny, int nz, double* phi, const double* r
           (rho[ridx(nx, ny, ix, iy, iz)] + (pxm + pxp) * dxsqic + (pym + pyp) * dysqic + (pzm + pzp) * dzsqic) / denom +
           spm1 * S.prevphi[ic];
     }
-  }
+  });
 }
 
 // condbndymgint, f3d_mgrid.F:2982-3092 (Neumann subgrid neighbours)
@@ -692,10 +760,13 @@ void sorhalfpass3d(int parity, int mglevel, int nx, int ny, int nz, double* phi,
   if (lb[5] <= 0) izmax = nz - 1;
   Subgrid& S = (parity == 0) ? C.even : C.odd;
   if (P.lcndbndy)
-    for (int ic = S.istart[mglevel]; ic < S.istart[mglevel + 1]; ++ic)
+    par_for(S.istart[mglevel], S.istart[mglevel + 1], [&](int64_t ic) {
       S.prevphi[ic] = phi[pidx(nx, ny, S.indx[3 * ic], S.indx[3 * ic + 1], S.indx[3 * ic + 2])];
+    });
   const size_t sx = 1, sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
-  for (int iz = izmin; iz <= izmax; ++iz)
+  // one colour reads only the other colour: planes are independent
+  par_for(izmin, izmax + 1, [&](int64_t iz64) {
+    const int iz = (int)iz64;
     for (int iy = iymin; iy <= iymax; ++iy) {
       int ix1 = ixmin + (((ixmin + iy + iz + parity) % 2) + 2) % 2;
       for (int ix = ix1; ix <= ixmax; ix += 2) {
@@ -704,6 +775,7 @@ void sorhalfpass3d(int parity, int mglevel, int nx, int ny, int nz, double* phi,
                  (phi[p - sy] + phi[p + sy]) * dysqic + (phi[p - sz] + phi[p + sz]) * dzsqic + spm1 * phi[p];
       }
     }
+  }, (int64_t)(nx + 1) * (ny + 1) / 2);
   if (P.lcndbndy) condbndymg(S, nx, ny, nz, phi, rho, dxsqic, dysqic, dzsqic, spm1, P.mgparam, lb, mglevel, P.mgform);
   cond_potmg(C.interior, nx, ny, phi, mglevel, P.mgform, false);
   condbndymgint(C, nx, ny, nz, phi, lb, mglevel);
@@ -777,15 +849,18 @@ void residual3d(int nx, int ny, int nz, double dxsqi, double dysqi, double dzsqi
   if (lb[3] == 0) iymax = ny - 1;
   if (lb[4] == 0) izmin = 1;
   if (lb[5] == 0) izmax = nz - 1;
-  std::fill(res, res + (size_t)(nx + 3) * (ny + 3) * (nz + 3), 0.);
+  const int64_t npad = (int64_t)(nx + 3) * (ny + 3) * (nz + 3);
+  par_for(0, npad, [&](int64_t i) { res[i] = 0.; });
   const size_t sx = 1, sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
-  for (int iz = izmin; iz <= izmax; ++iz)
+  par_for(izmin, izmax + 1, [&](int64_t iz64) {
+    const int iz = (int)iz64;
     for (int iy = iymin; iy <= iymax; ++iy)
       for (int ix = ixmin; ix <= ixmax; ++ix) {
         size_t p = pidx(nx, ny, ix, iy, iz);
         res[p] = rho[ridx(nx, ny, ix, iy, iz)] + (phi[p - sx] + phi[p + sx]) * dxsqic +
                  (phi[p - sy] + phi[p + sy]) * dysqic + (phi[p - sz] + phi[p + sz]) * dzsqic - phi[p] * P.mgparam;
       }
+  }, (int64_t)(nx + 1) * (ny + 1));
   const Interior& I = C.interior;
   for (int ic = I.istart[mglevel]; ic < I.istart[mglevel + 1]; ++ic)
     res[pidx(nx, ny, I.indx[3 * ic], I.indx[3 * ic + 1], I.indx[3 * ic + 2])] = 0.;
@@ -812,7 +887,8 @@ void restrict3d(int nx, int ny, int nz, const double* res, int nxc, int nyc, int
     lo = std::max(lo0, -1);
     hi = std::min(hi, n + 1);
   };
-  for (int izc = izcmin; izc <= izcmax; ++izc) {
+  par_for(izcmin, izcmax + 1, [&](int64_t izc64) {
+    const int izc = (int)izc64;
     int izmin, izmax, iz0;
     lim(izc, nz, nzc, izmin, izmax, iz0);
     for (int iyc = iycmin; iyc <= iycmax; ++iyc) {
@@ -841,7 +917,7 @@ void restrict3d(int nx, int ny, int nz, const double* res, int nxc, int nyc, int
         }
       }
     }
-  }
+  }, (int64_t)(nxc + 1) * (nyc + 1) * 9);
 }
 
 // expand3d (no precalculated coefficients), f3d_mgrid.F:1777-1947
@@ -853,7 +929,8 @@ void expand3d(int nx, int ny, int nz, double* phi, int nxc, int nyc, int nzc, co
   if (lb[3] == 0) iymax = ny - 1;
   if (lb[4] == 0) izmin = 1;
   if (lb[5] == 0) izmax = nz - 1;
-  for (int iz = izmin; iz <= izmax; ++iz) {
+  par_for(izmin, izmax + 1, [&](int64_t iz64) {
+    const int iz = (int)iz64;
     int jz = (iz * nzc) / nz;
     double wz = 1. * (iz * nzc) / nz - jz;
     for (int iy = iymin; iy <= iymax; ++iy) {
@@ -873,7 +950,7 @@ void expand3d(int nx, int ny, int nz, double* phi, int nxc, int nyc, int nzc, co
             wx * wy * wz * phic[pidx(nxc, nyc, jx + 1, jy + 1, jz + 1)];
       }
     }
-  }
+  }, (int64_t)(nx + 1) * (ny + 1));
 }
 
 // vcycle, f3d_mgrid.F:1101-1591 (serial; recursive)
@@ -1040,16 +1117,18 @@ int or_mgsolve(int nx, int ny, int nz, double dx, double dy, double dz, const in
     }
     vcycle(0, lv, phi, rhs.data(), bounds, P, *C);
     if (mgform == 2) {
-      for (size_t i = 0; i < np; ++i) phi[i] = phi[i] + phisave[i];
+      par_for(0, (int64_t)np, [&](int64_t i) { phi[i] = phi[i] + phisave[i]; });
       applybc(nx, ny, nz, 1, phi, bounds, false, false);
     }
-    mgerror = 0.;
-    for (int iz = 0; iz <= nz; ++iz)
+    mgerror = par_max(0, nz + 1, [&](int64_t iz) {
+      double m = 0.;
       for (int iy = 0; iy <= ny; ++iy)
         for (int ix = 0; ix <= nx; ++ix) {
-          size_t p = pidx(nx, ny, ix, iy, iz);
-          mgerror = std::max(mgerror, std::fabs(phisave[p] - phi[p]));
+          size_t p = pidx(nx, ny, ix, iy, (int)iz);
+          m = std::max(m, std::fabs(phisave[p] - phi[p]));
         }
+      return m;
+    }, (int64_t)(nx + 1) * (ny + 1));
   }
   applybc(nx, ny, nz, 1, phi, bounds, true, false);
   *mgiters_out = mgiters;
@@ -1082,13 +1161,18 @@ double or_relresidual(int nx, int ny, int nz, double dx, double dy, double dz, c
   // level-0 residual3d with mgform = 1, so rows next to conductors carry
   // the ppp = min(dels) scaling of condbndyres
   residual3d(nx, ny, nz, dxsqi, dysqi, dzsqi, ph.data(), rhs.data(), res.data(), 0, bounds, P, false, *C);
-  double rmax = 0., bmax = 0.;
-  for (int iz = 0; iz <= nz; ++iz)
+  const double rmax = par_max(0, nz + 1, [&](int64_t iz) {
+    double m = 0.;
     for (int iy = 0; iy <= ny; ++iy)
-      for (int ix = 0; ix <= nx; ++ix) {
-        rmax = std::max(rmax, std::fabs(res[pidx(nx, ny, ix, iy, iz)]));
-        bmax = std::max(bmax, std::fabs(rhs[ridx(nx, ny, ix, iy, iz)]));
-      }
+      for (int ix = 0; ix <= nx; ++ix) m = std::max(m, std::fabs(res[pidx(nx, ny, ix, iy, (int)iz)]));
+    return m;
+  }, (int64_t)(nx + 1) * (ny + 1));
+  const double bmax = par_max(0, nz + 1, [&](int64_t iz) {
+    double m = 0.;
+    for (int iy = 0; iy <= ny; ++iy)
+      for (int ix = 0; ix <= nx; ++ix) m = std::max(m, std::fabs(rhs[ridx(nx, ny, ix, iy, (int)iz)]));
+    return m;
+  }, (int64_t)(nx + 1) * (ny + 1));
   return bmax > 0. ? rmax / bmax : rmax;
 }
 
@@ -1102,8 +1186,8 @@ void or_setrho(int nx, int ny, int nz, double dx, double dy, double dz, double x
   g = g / dy;
   g = g / dz;
   double dxi = 1. / dx, dyi = 1. / dy, dzi = 1. / dz;
-  for (int64_t ip = 0; ip < np; ++ip) {
-    if (gaminv && gaminv[ip] == 0.) continue;
+  auto deposit = [&](int64_t ip) {
+    if (gaminv && gaminv[ip] == 0.) return;
     int ii, jj, kk;
     double u1, v1, w1;
     cellfrac((xp[ip] - xmmin) * dxi, nx, ii, u1);
@@ -1118,7 +1202,35 @@ void or_setrho(int nx, int ny, int nz, double dx, double dy, double dz, double x
     rho[ridx(nx, ny, ii + 1, jj, kk + 1)] += u1 * v0 * w1 * g;
     rho[ridx(nx, ny, ii, jj + 1, kk + 1)] += u0 * v1 * w1 * g;
     rho[ridx(nx, ny, ii + 1, jj + 1, kk + 1)] += u1 * v1 * w1 * g;
+  };
+  const int nt = nthreads();
+  if (nt <= 1 || np < kParMin || nz < 2) {
+    for (int64_t ip = 0; ip < np; ++ip) deposit(ip);
+    return;
   }
+  // Parallel over z slabs of cells. A particle in cell kk writes node planes
+  // kk and kk + 1, so slabs two apart never share a plane: the even slabs
+  // run at once, then the odd ones. Within a slab the particles keep their
+  // order, so the result is fixed for a given thread count; it differs from
+  // the serial loop only by the order of the adds on the shared planes.
+  const int nslab = std::min(2 * nt, nz);
+  std::vector<int> slab(np);
+  par_for(0, np, [&](int64_t ip) {
+    int kk;
+    double w1;
+    cellfrac((zp[ip] - zgrid - zmmin) * dzi, nz, kk, w1);
+    slab[ip] = (int)((int64_t)kk * nslab / nz);
+  });
+  std::vector<int64_t> start(nslab + 1, 0);
+  for (int64_t ip = 0; ip < np; ++ip) ++start[slab[ip] + 1];
+  for (int b = 0; b < nslab; ++b) start[b + 1] += start[b];
+  std::vector<int64_t> order(np), fill(start.begin(), start.end() - 1);
+  for (int64_t ip = 0; ip < np; ++ip) order[fill[slab[ip]]++] = ip;
+  for (int phase = 0; phase < 2; ++phase)
+    par_for(0, (nslab - phase + 1) / 2, [&](int64_t h) {
+      const int b = 2 * (int)h + phase;
+      for (int64_t t = start[b]; t < start[b + 1]; ++t) deposit(order[t]);
+    }, kParMin);
 }
 
 // applyrhoboundaryconditions3d (serial, nguardrho = 0), w3d.F:2660-2750
@@ -1145,7 +1257,8 @@ void or_sete(int nx, int ny, int nz, double dx, double dy, double dz, double xmm
   double tdxi = 1. / (2. * dx), tdyi = 1. / (2. * dy), tdzi = 1. / (2. * dz);
   double dxi = 1. / dx, dyi = 1. / dy, dzi = 1. / dz;
   auto P = [&](int ix, int iy, int iz) { return phi[pidx(nx, ny, ix, iy, iz)]; };
-  for (int64_t ip = 0; ip < np; ++ip) {
+  // particles are independent
+  par_for(0, np, [&](int64_t ip) {
     int i, j, k;
     double u1, v1, w1;
     cellfrac((xp[ip] - xmmin) * dxi, nx, i, u1);
@@ -1174,7 +1287,7 @@ void or_sete(int nx, int ny, int nz, double dx, double dy, double dz, double xmm
     ex[ip] = ex[ip] + ext;
     ey[ip] = ey[ip] + eyt;
     ez[ip] = ez[ip] + ezt;
-  }
+  });
 }
 
 // Per-lattice-cell quad tables as built by setlattzt (top_lattice.F:1852-2030)
@@ -1222,8 +1335,9 @@ void or_push_fullv(int64_t np, double* xp, double* yp, double* zp, double* uxp, 
                    double dzl, double zmmin, double zmmax, double prwall, double prwallx, double prwally) {
   const double halfdt = 0.5 * dt, dtl = -halfdt, dtr = halfdt;
   const double dzli = 1. / dzl;
-  for (int64_t ip = 0; ip < np; ++ip) {
-    if (gaminv[ip] == 0.) continue;
+  // particles are independent
+  par_for(0, np, [&](int64_t ip) {
+    if (gaminv[ip] == 0.) return;
     double bx = 0., by = 0., bz = 0.;
     if (czs) {
       double vz = uzp[ip] * gaminv[ip];
@@ -1275,7 +1389,7 @@ void or_push_fullv(int64_t np, double* xp, double* yp, double* zp, double* uxp, 
     // stckxy3d, round aperture (prwelip = 1)
     double rx = xp[ip] - prwallx, ry = yp[ip] - prwally;
     if (rx * rx + ry * ry >= prwall * prwall) gaminv[ip] = 0.;
-  }
+  });
 }
 
 // Global moments of the live particles (getzmmnt, top.F:521-1444). out[]:
@@ -1308,6 +1422,29 @@ void or_moments(int64_t np, const double* xp, const double* yp, const double* ux
   out[6] = 4. * std::sqrt(std::max(0., dysq * dypsq - dyyp * dyyp));
 }
 
+// getese3dfromrhophi (dw3d.F:708-777), no symmetry: ese = dx dy dz / 2 times
+// the sum of rho*phi over nodes 0..n, summed over z per (x, y) column first,
+// then over y into row 0, then over x, in that order.
+double or_ese(int nx, int ny, int nz, const double* rho, const double* phi, double dx, double dy, double dz) {
+  std::vector<double> scr((size_t)(nx + 1) * (ny + 1), 0.);
+  const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3);
+  for (int iz = 0; iz <= nz; ++iz)
+    for (int iy = 0; iy <= ny; ++iy)
+      for (int ix = 0; ix <= nx; ++ix) {
+        const double r = rho[ix + (size_t)(nx + 1) * (iy + (size_t)(ny + 1) * iz)];
+        const double p = phi[(ix + 1) + sy * (iy + 1) + sz * (iz + 1)];
+        double& c = scr[ix + (size_t)(nx + 1) * iy];
+        c = c + r * p;
+      }
+  for (int iy = 1; iy <= ny; ++iy)
+    for (int ix = 0; ix <= nx; ++ix) scr[ix] = scr[ix] + scr[ix + (size_t)(nx + 1) * iy];
+  double ese = 0.;
+  for (int ix = 0; ix <= nx; ++ix) ese = ese + scr[ix];
+  return dx * dy * dz * 0.5 * ese;
+}
+
 double or_eps0() { return EPS0; }
+
+int or_threads() { return nthreads(); }
 
 }  // extern "C"

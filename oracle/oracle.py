@@ -60,6 +60,9 @@ def lib():
             [ctypes.c_int] + [ctypes.c_double] * 7
         L.or_moments.argtypes = [ctypes.c_int64] + [_dp] * 6 + [_dp]
         L.or_eps0.restype = ctypes.c_double
+        L.or_threads.restype = ctypes.c_int
+        L.or_ese.argtypes = [ctypes.c_int] * 3 + [_dp, _dp] + [ctypes.c_double] * 3
+        L.or_ese.restype = ctypes.c_double
         _LIB = L
     return _LIB
 
@@ -233,3 +236,17 @@ def moments(p):
                      _d(p["gaminv"]), _d(out))
     return {"n": out[0], "xbar": out[1], "ybar": out[2], "xrms": out[3], "yrms": out[4], "epsx": out[5],
             "epsy": out[6]}
+
+
+def ese(rho, phi, dx, dy, dz):
+    """Field energy of getese3dfromrhophi (dw3d.F:708-777): rho (nx+1, ny+1,
+    nz+1) and phi (nx+3, ny+3, nz+3), both Fortran-ordered."""
+    rho = np.asfortranarray(rho, dtype=np.float64)
+    phi = np.asfortranarray(phi, dtype=np.float64)
+    nx, ny, nz = (n - 1 for n in rho.shape)
+    return lib().or_ese(nx, ny, nz, _d(rho), _d(phi), dx, dy, dz)
+
+
+def threads():
+    """Host threads the oracle's parallel loops use (ORACLE_THREADS)."""
+    return lib().or_threads()

@@ -67,3 +67,16 @@ def test_semigaussian_statistics():
     assert np.std(p["ux"] / p["uz"]) == pytest.approx(5e-3, rel=0.02)
     q = semigaussian(1000, seed=0)
     assert np.array_equal(q["x"], semigaussian(1000, seed=0)["x"])
+
+
+def test_oracle_field_energy_matches_direct_sum():
+    """or_ese (getese3dfromrhophi) equals dx dy dz / 2 * sum(rho * phi) on the
+    nodes, to rounding."""
+    import numpy as np
+    from oracle import oracle
+    rng = np.random.default_rng(4)
+    rho = np.asfortranarray(rng.standard_normal((9, 7, 12)))
+    phi = np.asfortranarray(rng.standard_normal((11, 9, 14)))
+    e = oracle.ese(rho, phi, 0.1, 0.2, 0.05)
+    ref = 0.1 * 0.2 * 0.05 * 0.5 * np.sum(rho * phi[1:-1, 1:-1, 1:-1])
+    assert abs(e - ref) <= 1e-12 * np.sum(np.abs(rho * phi[1:-1, 1:-1, 1:-1]))

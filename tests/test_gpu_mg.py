@@ -130,3 +130,15 @@ def test_gpu_graph_replay_equals_eager(precision):
         out.append((sv.phi.cpu().numpy(), sv.mgiters))
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
+
+
+def test_gpu_field_energy_bitexact():
+    """getese3dfromrhophi: the GPU sum in the reference's order equals the
+    oracle bit for bit, on a solved field."""
+    s, shapes, rho = _conductor_case()
+    s.rho = rho
+    s.solve()
+    e = s.getese()
+    ref = oracle.ese(rho, s.phi.cpu().numpy(), s.dx, s.dy, s.dz)
+    assert e == ref
+    assert e != 0.0

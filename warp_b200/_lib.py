@@ -77,6 +77,7 @@ SIGNATURES = {
     "wg_solve": [_vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats)],
     "wg_relresidual": [_vp, _c.c_double, _dp],
     "wg_residual_field": [_vp, _c.c_double, _vp],
+    "wg_field_energy": [_vp, _dp],
     "wg_deposit": [_vp, ctypes.POINTER(Particles), _c.c_int],
     "wg_deposit_noalloc": [ctypes.POINTER(Grid), ctypes.POINTER(Particles), _vp, _c.c_int, _vp],
     "wg_finalize_rho": [_vp],

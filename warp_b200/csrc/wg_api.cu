@@ -19,6 +19,7 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st);
 int relresidual(wg_ctx* c, double mgparam, double* out);
 int residual_field(wg_ctx* c, double mgparam, double* out);
+int field_energy(wg_ctx* c, double* out);
 int deposit(wg_ctx* c, const wg_particles* p, int zero_first);
 int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream);
 int finalize_rho(wg_ctx* c);
@@ -185,6 +186,7 @@ void free_all(wg_ctx* c) {
   dfree(c->dred);
   dfree(c->dslot);
   dfree(c->dmom);
+  dfree(c->dese);
   dfree(c->czs);
   dfree(c->cze);
   dfree(c->cdb);
@@ -312,6 +314,7 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
   if (rc == WG_OK) rc = dalloc(&c->rho, L0.nr);
   if (rc == WG_OK) rc = dalloc(&c->racc, L0.nr);
   if (rc == WG_OK) rc = dalloc(&c->dred, (size_t)4);
+  if (rc == WG_OK) rc = dalloc(&c->dese, (size_t)(G.nx + 1) * (G.ny + 1) + 1);
   if (rc == WG_OK) rc = dalloc(&c->dslot, (size_t)3 * 32 * 16);
   if (rc == WG_OK) {
     cudaDeviceProp prop;
@@ -456,6 +459,11 @@ int wg_solve(wg_ctx* c, const wg_solve_opts* opts, wg_solve_stats* stats) {
   if (!c) { set_error("null context"); return WG_EINVAL; }
   if (!c->cond.finalized) { set_error("wg_solve: conductors added but not finalized"); return WG_ESTATE; }
   return solve(c, opts, stats);
+}
+
+int wg_field_energy(wg_ctx* c, double* out) {
+  if (!c || !out) { set_error("null argument"); return WG_EINVAL; }
+  return field_energy(c, out);
 }
 
 int wg_residual_field(wg_ctx* c, double mgparam, double* out) {

@@ -122,6 +122,7 @@ struct wg_ctx {
   unsigned long long* dslot = nullptr; // per-block max slots of [0..2], folded into dred
   unsigned long long* hred = nullptr;  // pinned host copy
   double* dmom = nullptr;              // moment partial sums
+  double* dese = nullptr;              // field-energy row sums ((nx+1)(ny+1) + 1)
   int mom_blocks = 0;
   // lattice tables
   double* czs = nullptr;

@@ -1482,6 +1482,49 @@ int residual_field(wg_ctx* c, double mgparam, double* out) {
   return WG_OK;
 }
 
+// getese3dfromrhophi (dw3d.F:708-777) without symmetry, in the reference's
+// summation order: per (x, y) column over z, then over y into row 0, then
+// over x; the result is bit-identical to the serial loops.
+__global__ void k_ese_cols(const double* __restrict__ rho, const double* __restrict__ phi, int nx, int ny, int nz,
+                           double* __restrict__ scr) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y;
+  if (ix > nx) return;
+  const size_t sy = nx + 3, sz = (size_t)(nx + 3) * (ny + 3), rz = (size_t)(nx + 1) * (ny + 1);
+  const double* r = rho + ix + (size_t)(nx + 1) * iy;
+  const double* p = phi + (ix + 1) + sy * (iy + 1) + sz;
+  double c = 0.;
+  for (int iz = 0; iz <= nz; ++iz) c = c + r[rz * iz] * p[sz * iz];
+  scr[ix + (size_t)(nx + 1) * iy] = c;
+}
+
+__global__ void k_ese_rows(double* __restrict__ scr, int nx, int ny, double dvol, double* __restrict__ out) {
+  for (int ix = threadIdx.x; ix <= nx; ix += blockDim.x) {
+    double c = scr[ix];
+    for (int iy = 1; iy <= ny; ++iy) c = c + scr[ix + (size_t)(nx + 1) * iy];
+    scr[ix] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ese = 0.;
+    for (int ix = 0; ix <= nx; ++ix) ese = ese + scr[ix];
+    *out = dvol * 0.5 * ese;
+  }
+}
+
+int field_energy(wg_ctx* c, double* out) {
+  cudaStream_t s = c->stream;
+  const LevelDims& d = c->lv[0].d;
+  ++c->nlaunch;
+  k_ese_cols<<<dim3(cdiv(d.nx + 1, 128), d.ny + 1), 128, 0, s>>>(c->rho, c->lv[0].phi, d.nx, d.ny, d.nz, c->dese);
+  ++c->nlaunch;
+  k_ese_rows<<<1, 256, 0, s>>>(c->dese, d.nx, d.ny, c->dx * c->dy * c->dz, c->dese + (size_t)(d.nx + 1) * (d.ny + 1));
+  WG_TRY_CUDA(cudaGetLastError());
+  WG_TRY_CUDA(cudaMemcpyAsync(out, c->dese + (size_t)(d.nx + 1) * (d.ny + 1), sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  WG_TRY_CUDA(cudaStreamSynchronize(s));
+  return WG_OK;
+}
+
 // Shared memory of the fused sweep exceeds the 48 KB default for FP64.
 int configure_kernels() {
   WG_TRY_CUDA(cudaFuncSetAttribute(k_sor_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,

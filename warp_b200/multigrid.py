@@ -263,6 +263,15 @@ class MultiGridB200(FieldSolver):
         _lib.check(_lib.lib.wg_relresidual(self._h, self.mgparam, ctypes.byref(out)))
         return out.value
 
+    def getese(self):
+        """Electrostatic energy dx dy dz / 2 * sum(rho * phi) over the nodes
+        (MultiGrid3D.getese -> getese3dfromrhophi, multigrid.py:447-469,
+        dw3d.F:708-777). Returns a float (the reference stores it in top.ese)."""
+        self._bind_stream()
+        out = ctypes.c_double()
+        _lib.check(_lib.lib.wg_field_energy(self._h, ctypes.byref(out)))
+        return out.value
+
     def residual_field(self, out=None):
         """rhs - A phi of the current phi (conductor voltages imposed), in the
         rho layout: the right-hand side of the residual-correction equation,
