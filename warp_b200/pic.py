@@ -20,6 +20,8 @@ Workloads (synthetic, seeded):
 """
 import math
 
+import numpy as np
+
 from . import conductors as cond
 from .constants import clight, echarge, proton_mass
 from .fieldsolver import registersolver
@@ -163,3 +165,40 @@ class ESPIC:
 
     def moments(self):
         return self.solver.moments(self.pgroup)
+
+    def dump(self, filename=None, prefix="", runid="espic", suffix=""):
+        """Restartable dump of the run (the dump/restart pair of
+        scripts/warp.py:950-1121, as one .npz file): the workload, the solver
+        options, the step counter, the particle arrays and phi with its guard
+        cells. rho is not saved: every step deposits it afresh. The default
+        name follows the reference's prefix + runid + '%06d' % it + suffix +
+        '.dump'. Returns the file name."""
+        import json
+        if filename is None:
+            filename = "%s%s%06d%s.dump.npz" % (prefix, runid, self.it, suffix)
+        s, pg = self.solver, self.pgroup
+        arrays = {"p_" + k: v for k, v in pg.to_numpy().items()}
+        meta = {"cfg": self.cfg, "it": self.it, "sort_interval": self.sort_interval, "precision": s.precision,
+                "tolkind": s.tolkind, "mgtol": s.mgtol, "mgmaxiters": s.mgmaxiters, "q": pg.q, "m": pg.m,
+                "w": pg.w}
+        with open(filename, "wb") as f:
+            np.savez(f, meta=np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8),
+                     phi=s.phi.cpu().numpy(), **arrays)
+        return filename
+
+
+def restart(filename, device="cuda"):
+    """Rebuilds an ESPIC run from ESPIC.dump: same workload, options, step
+    counter, particles and phi, so the following steps reproduce the run
+    that wrote the dump bit for bit."""
+    import json
+    with np.load(filename) as d:
+        meta = json.loads(bytes(d["meta"]).decode())
+        parts = {k[2:]: d[k] for k in d.files if k.startswith("p_")}
+        phi = d["phi"]
+    run = ESPIC(meta["cfg"], precision=meta["precision"], tolkind=meta["tolkind"], mgtol=meta["mgtol"],
+                mgmaxiters=meta["mgmaxiters"], device=device, particles=parts, sort_interval=meta["sort_interval"])
+    run.pgroup.q, run.pgroup.m, run.pgroup.w = meta["q"], meta["m"], meta["w"]
+    run.solver.phi = np.asfortranarray(phi)
+    run.it = meta["it"]
+    return run
