@@ -55,7 +55,23 @@ __device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
 //    nodes, added to the global accumulator at the end, or straight to global
 //    memory when the box is larger than DEP_BOX nodes (unsorted particles).
 // Integer adds commute, so rho does not depend on any of these orders.
-constexpr int DEP_NT = 256, DEP_PPT = 16, DEP_BOX = 4096;
+constexpr int DEP_NT = 256, DEP_PPT = 16, DEP_BOX = 3072;
+
+// A box node holds its fixed-point sum as three 32-bit parts (bits 0-15,
+// 16-31 and 32 up), so every shared-memory add is a 32-bit atomic: 64-bit
+// shared atomics are several times slower. A chunk adds at most
+// DEP_NT*DEP_PPT = 4096 contributions to a node, so the two 16-bit parts sum
+// below 2^28 and the high part below 2^26 (total below 2^58): no part
+// overflows, and the recombined 64-bit value is exact.
+struct DepBox {
+  unsigned lo[DEP_BOX], mid[DEP_BOX], hi[DEP_BOX];
+};
+__device__ inline void box_add(DepBox& b, int n, unsigned long long v) {
+  const unsigned l = (unsigned)(v & 0xFFFFull), m = (unsigned)((v >> 16) & 0xFFFFull), h = (unsigned)(v >> 32);
+  if (l) atomicAdd(&b.lo[n], l);
+  if (m) atomicAdd(&b.mid[n], m);
+  if (h) atomicAdd(&b.hi[n], h);
+}
 
 __device__ inline bool dep_cell(const double* xp, const double* yp, const double* zp, const double* gaminv,
                                 int64_t i, int64_t np, const GridP& g, int& ii, int& jj, int& kk, double& u1,
@@ -68,10 +84,10 @@ __device__ inline bool dep_cell(const double* xp, const double* yp, const double
 }
 
 // Adds v to node (i, j, k) of the box or of the global accumulator.
-__device__ inline void dep_add(unsigned long long* box, bool use_box, int ox, int oy, int oz, int bx, int by,
+__device__ inline void dep_add(DepBox& box, bool use_box, int ox, int oy, int oz, int bx, int by,
                                unsigned long long* acc, const GridP& g, int i, int j, int k, unsigned long long v) {
   if (use_box)
-    atomicAdd(&box[(i - ox) + bx * ((j - oy) + by * (k - oz))], v);
+    box_add(box, (i - ox) + bx * ((j - oy) + by * (k - oz)), v);
   else
     atomicAdd(acc + i + (g.nx + 1) * (j + (g.ny + 1) * k), v);
 }
@@ -80,7 +96,7 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
                                                     const double* __restrict__ zp,
                                                     const double* __restrict__ gaminv, int64_t np, GridP g,
                                                     unsigned long long* __restrict__ acc) {
-  __shared__ unsigned long long box[DEP_BOX];
+  __shared__ DepBox box;
   __shared__ int bmin[3], bmax[3];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t base = (int64_t)blockIdx.x * (DEP_NT * DEP_PPT) + (int64_t)warp * (32 * DEP_PPT) + lane;
@@ -115,7 +131,11 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
   const bool any = bmax[0] >= 0;
   const bool use_box = any && (long long)bx * by * bz <= DEP_BOX;
   if (use_box)
-    for (int i = tid; i < bx * by * bz; i += DEP_NT) box[i] = 0ull;
+    for (int i = tid; i < bx * by * bz; i += DEP_NT) {
+      box.lo[i] = 0u;
+      box.mid[i] = 0u;
+      box.hi[i] = 0u;
+    }
   __syncthreads();
   if (any) {
     // register sums of the warp's current uniform cell (ci, cj, ck), or ci < 0
@@ -191,7 +211,8 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
   if (use_box) {
     __syncthreads();
     for (int i = tid; i < bx * by * bz; i += DEP_NT) {
-      const unsigned long long v = box[i];
+      const unsigned long long v =
+          ((unsigned long long)box.hi[i] << 32) + ((unsigned long long)box.mid[i] << 16) + box.lo[i];
       if (v) {
         const int lx = i % bx, ly = (i / bx) % by, lz = i / (bx * by);
         atomicAdd(acc + (ox + lx) + (g.nx + 1) * ((oy + ly) + (g.ny + 1) * (oz + lz)), v);
