@@ -34,9 +34,10 @@ DEFAULT_REF_VCYCLES = 6
 # particles are re-sorted by cell every SORT_INTERVAL steps (inside the timed steps)
 SORT_INTERVAL = 10
 # DRAM bytes (read + write) per finest-level node of one k_sor_bulk<float>
-# half sweep, from an ncu --set full capture of one launch on the
-# 257x257x513-node level: 271.7 MB read + 91.6 MB written
-SOR_F32_TRAFFIC_PER_NODE = (271.714048e6 + 91.577344e6) / (257 * 257 * 513)
+# half sweep (bulk nodes and the colour's subgrid points), from an ncu
+# --set full capture of one launch on the 257x257x513-node level:
+# 311.2 MB read + 94.6 MB written
+SOR_F32_TRAFFIC_PER_NODE = (311.19488e6 + 94.622976e6) / (257 * 257 * 513)
 
 
 def parse():
