@@ -75,12 +75,21 @@ typedef struct {
   double q, m, w; /* charge, mass, macroparticle weight (sq, sm, sw) */
 } wg_particles;
 
-/* Parameters of one fullv particle advance (padvnc3d, w3d.F:1862-1987). */
+/* Parameters of one particle advance (padvnc3d, w3d.F:1575). */
 typedef struct {
   double dt;
   double prwall, prwallx, prwally; /* round absorbing aperture (top.prwall) */
   int use_lattice;                 /* apply the hard-edge quad tables */
+  int center;                      /* WG_CENTER_* below; 0 = fullv */
 } wg_push_params;
+
+/* padvnc3d's `center` argument. During a run the velocities are half a step
+ * ahead of the positions. Right after loading both are at t, so the first
+ * step is HALFV and the steps after it FULLV; SYNCHV brings the velocities
+ * back in step with the positions for diagnostics. */
+#define WG_CENTER_FULLV 0  /* v t-dt/2 -> t+dt/2, x t -> t+dt (w3d.F:1862-1987) */
+#define WG_CENTER_HALFV 1  /* v t -> t+dt/2, x t -> t+dt (w3d.F:1989-2125) */
+#define WG_CENTER_SYNCHV 2 /* v t-dt/2 -> t, x unchanged (w3d.F:2187-2310) */
 
 /* ---- context ----------------------------------------------------------- */
 
@@ -174,11 +183,12 @@ int wg_fetch_e(wg_ctx* ctx, const double* x, const double* y, const double* z, d
  * Host arrays of length nzl+1. */
 int wg_set_lattice(wg_ctx* ctx, const double* czs, const double* cze, const double* cdb, int nzl,
                    double zlmin, double dzl);
-/* One fused fullv step of padvnc3d (w3d.F:1862-1987) followed by
- * particleboundaries3d (w3d.F:11292): gather E (sete_from_phi_linear3d),
- * quad B (applyquad), epush3d/bpush3d(ibpush=1)/epush3d/xpush3d
- * (w3d.F:2752,2834,3070), periz (top.F:4015) and the round-pipe absorber
- * (stckxy3d, w3d.F:11473). */
+/* One fused step of padvnc3d (w3d.F:1575) followed by particleboundaries3d
+ * (w3d.F:11292): gather E (sete_from_phi_linear3d), quad B (applyquad),
+ * epush3d/bpush3d(ibpush=1)/epush3d/xpush3d (w3d.F:2752,2834,3070) as
+ * prm->center selects, periz (top.F:4015) and the round-pipe absorber
+ * (stckxy3d, w3d.F:11473). A SYNCHV step pushes no position and applies no
+ * boundary. An unknown center is WG_EINVAL. */
 int wg_advance(wg_ctx* ctx, const wg_particles* p, const wg_push_params* prm);
 /* getzmmnt global moments (top.F:521-1444): out[0] live count, 1 xbar,
  * 2 ybar, 3 xrms, 4 yrms, 5 epsx, 6 epsy (x' = ux/uz), 7 reserved. FP64,

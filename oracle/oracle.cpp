@@ -1322,18 +1322,26 @@ void or_quad_table(int nquad, const double* zs, const double* ze, const double* 
   }
 }
 
-// One "fullv" particle advance followed by the particle boundaries, as done by
-// padvnc3d(center="fullv") (w3d.F:1862-1987) and particleboundaries3d:
-//   E (already gathered, passed in ex,ey,ez), B from applyquad
-//   (top_lattice.F:2985-3120; dtl=-dt/2, dtr=+dt/2), epush3d half step,
-//   bpush3d (ibpush = 1), epush3d half step, xpush3d (gaminv fixed: lrelativ
-//   false), periz (top.F:4015-4035), stckxy3d round pipe (w3d.F:11520-11535).
+// One particle advance of padvnc3d followed by the particle boundaries.
+// center 0, "fullv" (w3d.F:1862-1987): E (already gathered, passed in
+//   ex,ey,ez), B from applyquad (top_lattice.F:2985-3120) over the residence
+//   window (-dt/2, +dt/2), epush3d half step, bpush3d (ibpush = 1) full step,
+//   epush3d half step, xpush3d (gaminv fixed: lrelativ false), periz
+//   (top.F:4015-4035), stckxy3d round pipe (w3d.F:11520-11535).
+// center 1, "halfv" (w3d.F:1989-2125), the first step after loading, which
+//   takes velocities from t to t+dt/2: window (0, +dt/2), bpush3d half step,
+//   epush3d half step, then the same xpush3d, periz and pipe.
+// center 2, "synchv" (w3d.F:2187-2310), which takes velocities from t-dt/2
+//   back to t for diagnostics: window (-dt/2, 0), epush3d half step, bpush3d
+//   half step; positions are not pushed and no boundary is applied.
 // Lost particles get gaminv = 0 and are skipped.
-void or_push_fullv(int64_t np, double* xp, double* yp, double* zp, double* uxp, double* uyp, double* uzp,
-                   double* gaminv, const double* ex, const double* ey, const double* ez, double q, double m,
-                   double dt, const double* czs, const double* cze, const double* cdb, int nzl, double zlmin,
-                   double dzl, double zmmin, double zmmax, double prwall, double prwallx, double prwally) {
-  const double halfdt = 0.5 * dt, dtl = -halfdt, dtr = halfdt;
+void or_push(int center, int64_t np, double* xp, double* yp, double* zp, double* uxp, double* uyp, double* uzp,
+             double* gaminv, const double* ex, const double* ey, const double* ez, double q, double m, double dt,
+             const double* czs, const double* cze, const double* cdb, int nzl, double zlmin, double dzl,
+             double zmmin, double zmmax, double prwall, double prwallx, double prwally) {
+  const double halfdt = 0.5 * dt;
+  const double dtl = center == 1 ? 0. : -halfdt, dtr = center == 2 ? 0. : halfdt;
+  const double bdt = center == 0 ? dt : halfdt;
   const double dzli = 1. / dzl;
   // particles are independent
   par_for(0, np, [&](int64_t ip) {
@@ -1358,13 +1366,15 @@ void or_push_fullv(int64_t np, double* xp, double* yp, double* zp, double* uxp, 
         by = by + cdb[iz] * frac * xp[ip];
       }
     }
-    // epush3d, half step
-    double cst = q * halfdt / m;
-    uxp[ip] = uxp[ip] + ex[ip] * cst;
-    uyp[ip] = uyp[ip] + ey[ip] * cst;
-    uzp[ip] = uzp[ip] + ez[ip] * cst;
+    const double cst = q * halfdt / m;
+    if (center != 1) {
+      // epush3d, half step
+      uxp[ip] = uxp[ip] + ex[ip] * cst;
+      uyp[ip] = uyp[ip] + ey[ip] * cst;
+      uzp[ip] = uzp[ip] + ez[ip] * cst;
+    }
     // bpush3d, ibpush = 1
-    double cb = q * dt * 0.5 / m;
+    double cb = q * bdt * 0.5 / m;
     double tx = gaminv[ip] * bx * cb, ty = gaminv[ip] * by * cb, tz = gaminv[ip] * bz * cb;
     double tsqi = 2. / (1. + tx * tx + ty * ty + tz * tz);
     double sx = tx * tsqi, sy = ty * tsqi, sz = tz * tsqi;
@@ -1374,6 +1384,7 @@ void or_push_fullv(int64_t np, double* xp, double* yp, double* zp, double* uxp, 
     uxp[ip] = uxp[ip] + uyppr * sz - uzppr * sy;
     uyp[ip] = uyp[ip] + uzppr * sx - uxppr * sz;
     uzp[ip] = uzp[ip] + uxppr * sy - uyppr * sx;
+    if (center == 2) return;
     // epush3d, half step
     uxp[ip] = uxp[ip] + ex[ip] * cst;
     uyp[ip] = uyp[ip] + ey[ip] * cst;

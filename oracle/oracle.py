@@ -56,7 +56,7 @@ def lib():
         L.or_rhobc.argtypes = [ctypes.c_int] * 3 + [_dp, _ip]
         L.or_sete.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 7 + [_dp, ctypes.c_int64] + [_dp] * 6
         L.or_quad_table.argtypes = [ctypes.c_int, _dp, _dp, _dp] + [ctypes.c_double] * 4 + [ctypes.c_int] + [_dp] * 3
-        L.or_push_fullv.argtypes = [ctypes.c_int64] + [_dp] * 10 + [ctypes.c_double] * 3 + [_dp] * 3 + \
+        L.or_push.argtypes = [ctypes.c_int, ctypes.c_int64] + [_dp] * 10 + [ctypes.c_double] * 3 + [_dp] * 3 + \
             [ctypes.c_int] + [ctypes.c_double] * 7
         L.or_moments.argtypes = [ctypes.c_int64] + [_dp] * 6 + [_dp]
         L.or_eps0.restype = ctypes.c_double
@@ -214,8 +214,14 @@ def quad_tables(zs, ze, db, zlatperi, zlatstrt, zlmin, dzl, nzl):
     return czs, cze, cdb
 
 
-def push_fullv(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall, prwallx=0.0, prwally=0.0):
-    """p: dict of float64 arrays x,y,z,ux,uy,uz,gaminv (modified in place)."""
+_CENTERS = {"fullv": 0, "halfv": 1, "synchv": 2}
+
+
+def push(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall, prwallx=0.0, prwally=0.0,
+         center="fullv"):
+    """One padvnc3d advance (center "fullv", "halfv" or "synchv") of the
+    particles in p, a dict of float64 arrays x,y,z,ux,uy,uz,gaminv
+    (modified in place), with E already gathered into ex, ey, ez."""
     n = len(p["x"])
     if tables is None:
         czs = cze = cdb = None
@@ -223,11 +229,15 @@ def push_fullv(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall
     else:
         czs, cze, cdb = tables
         nzl = len(czs) - 1
-    lib().or_push_fullv(n, _d(p["x"]), _d(p["y"]), _d(p["z"]), _d(p["ux"]), _d(p["uy"]), _d(p["uz"]),
-                        _d(p["gaminv"]), _d(ex), _d(ey), _d(ez), q, m, dt,
-                        _d(czs) if czs is not None else None, _d(cze) if cze is not None else None,
-                        _d(cdb) if cdb is not None else None, nzl, zlmin, dzl, zmmin, zmmax, prwall, prwallx,
-                        prwally)
+    lib().or_push(_CENTERS[center], n, _d(p["x"]), _d(p["y"]), _d(p["z"]), _d(p["ux"]), _d(p["uy"]),
+                  _d(p["uz"]), _d(p["gaminv"]), _d(ex), _d(ey), _d(ez), q, m, dt,
+                  _d(czs) if czs is not None else None, _d(cze) if cze is not None else None,
+                  _d(cdb) if cdb is not None else None, nzl, zlmin, dzl, zmmin, zmmax, prwall, prwallx, prwally)
+
+
+def push_fullv(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall, prwallx=0.0, prwally=0.0):
+    """The fullv advance of push()."""
+    push(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall, prwallx, prwally, "fullv")
 
 
 def moments(p):

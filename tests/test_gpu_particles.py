@@ -1,6 +1,7 @@
 """GPU particle kernels against the oracle: fixed-point CIC deposition
 (within the fixed-point rounding, bit-identical under any particle order),
-the field gather and the fused fullv advance (bit for bit), and moments."""
+the field gather and the fused advance in its fullv, halfv and synchv forms
+(bit for bit), and moments."""
 import numpy as np
 import pytest
 import torch
@@ -109,6 +110,66 @@ def test_advance_bitexact_with_quads_and_pipe():
     for k in ("x", "y", "z", "ux", "uy", "uz"):
         # lost particles are frozen at the step they were lost
         assert np.array_equal(got[k], p2[k]), k
+
+
+def test_halfv_fullv_synchv_sequence_bitexact():
+    """A run as padvnc3d orders it: halfv after loading, fullv steps, and a
+    synchv that brings the velocities back to the positions' time."""
+    from warp_b200 import pic
+    from warp_b200.lattice import fodo
+    from warp_b200.particles import ParticleGroup
+    cfg, s, p, _ = _setup(50_000)
+    rng = np.random.default_rng(12)
+    phi = np.asfortranarray(1e3 * rng.standard_normal((s.nx + 3, s.ny + 3, s.nz + 3)))
+    s.phi = phi
+    s.setlattice(fodo(cfg["quad_gradient"], cfg["quad_length"], cfg["period"]))
+    czs, cze, cdb, nzl, zlmin, dzl = s._lattice
+    dt = pic.timestep(cfg)
+    p2 = {k: v.copy() for k, v in p.items()}
+    pg = ParticleGroup(p2, w=1.0)
+    for center in ("halfv", "fullv", "fullv", "synchv"):
+        ex, ey, ez = oracle.sete(phi, p2["x"], p2["y"], p2["z"], s.dx, s.dy, s.dz, s.xmmin, s.ymmin, s.zmmin)
+        oracle.push(p2, ex, ey, ez, pg.q, pg.m, dt, (czs, cze, cdb), zlmin, dzl, s.zmmin, s.zmmax,
+                    cfg["pipe_radius"], center=center)
+        s.advance(pg, dt, prwall=cfg["pipe_radius"], center=center)
+        got = pg.to_numpy()
+        for k in ("x", "y", "z", "ux", "uy", "uz", "gaminv"):
+            assert np.array_equal(got[k], p2[k]), (center, k)
+    # synchv moves no particle
+    x = pg.x.clone()
+    s.advance(pg, dt, center="synchv")
+    assert torch.equal(pg.x, x)
+
+
+def test_halfv_then_synchv_is_one_half_kick_each_way():
+    """With E only (no lattice): halfv with dt = 0 changes nothing, and
+    synchv is exactly one half E kick u + E q (dt/2) / m."""
+    from warp_b200 import pic
+    from warp_b200.particles import ParticleGroup
+    cfg, s, p, _ = _setup(20_000)
+    rng = np.random.default_rng(13)
+    s.phi = np.asfortranarray(1e3 * rng.standard_normal((s.nx + 3, s.ny + 3, s.nz + 3)))
+    dt = pic.timestep(cfg)
+    pg = ParticleGroup({k: v.copy() for k, v in p.items()}, w=1.0, with_fields=True)
+    s.fetche(pg)
+    e0 = (pg.ex.clone(), pg.ey.clone())
+    u0 = (pg.ux.clone(), pg.uy.clone())
+    s.advance(pg, 0.0, center="halfv")  # dt = 0: no kick, no drift
+    assert torch.equal(pg.ux, u0[0]) and torch.equal(pg.uy, u0[1])
+    s.advance(pg, dt, center="synchv")  # half kick at the unchanged positions
+    cst = pg.q * (0.5 * dt) / pg.m
+    assert torch.equal(pg.ux, u0[0] + e0[0] * cst) and torch.equal(pg.uy, u0[1] + e0[1] * cst)
+
+
+def test_unknown_center_is_rejected():
+    cfg, s, p, pg = _setup(1000)
+    with pytest.raises(ValueError):
+        s.advance(pg, 1e-9, center="gen")
+    from warp_b200 import _lib
+    import ctypes
+    prm = _lib.PushParams(1e-9, 1e30, 0., 0., 0, 7)
+    st = pg.cstruct()
+    assert _lib.lib.wg_advance(s._h, ctypes.byref(st), ctypes.byref(prm)) == -1
 
 
 def test_moments_match_oracle():

@@ -52,7 +52,11 @@ class Particles(ctypes.Structure):
 
 class PushParams(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("prwall", ctypes.c_double), ("prwallx", ctypes.c_double),
-                ("prwally", ctypes.c_double), ("use_lattice", ctypes.c_int)]
+                ("prwally", ctypes.c_double), ("use_lattice", ctypes.c_int), ("center", ctypes.c_int)]
+
+
+CENTER_FULLV, CENTER_HALFV, CENTER_SYNCHV = 0, 1, 2
+CENTERS = {"fullv": CENTER_FULLV, "halfv": CENTER_HALFV, "synchv": CENTER_SYNCHV}
 
 
 _c = ctypes

@@ -326,7 +326,14 @@ struct PushP {
   double zlmin, dzl;
 };
 
-// padvnc3d fullv + particleboundaries3d for one particle per thread.
+// padvnc3d + particleboundaries3d for one particle per thread. CENTER 0 is
+// "fullv" (w3d.F:1862-1987): quad window (-dt/2, dt/2), half E kick, full-dt
+// Boris rotation, half E kick, drift. CENTER 1 is "halfv" (w3d.F:1989-2125),
+// the first step after loading, velocities from t to t+dt/2: window
+// (0, dt/2), half-dt rotation, half E kick, drift. CENTER 2 is "synchv"
+// (w3d.F:2187-2310), velocities from t-dt/2 to t: window (-dt/2, 0), half E
+// kick, half-dt rotation; no drift and no boundaries.
+template <int CENTER>
 __global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ phi, GridP g, PushP P,
                                                  double* __restrict__ xp, double* __restrict__ yp,
                                                  double* __restrict__ zp, double* __restrict__ uxp,
@@ -344,7 +351,7 @@ __global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ p
   ey = 0. + ey;
   ez = 0. + ez;
   double bx = 0., by = 0., bz = 0.;
-  const double halfdt = 0.5 * P.dt, dtl = -halfdt, dtr = halfdt;
+  const double halfdt = 0.5 * P.dt, dtl = CENTER == 1 ? 0. : -halfdt, dtr = CENTER == 2 ? 0. : halfdt;
   if (P.czs) {
     // applyquad (top_lattice.F:2985-3120), one overlap level
     const double vz = uz * gi;
@@ -369,10 +376,12 @@ __global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ p
   }
   // epush3d (half step), bpush3d (ibpush = 1), epush3d (half step)
   const double cst = P.q * halfdt / P.m;
-  ux = ux + ex * cst;
-  uy = uy + ey * cst;
-  uz = uz + ez * cst;
-  const double cb = P.q * P.dt * 0.5 / P.m;
+  if (CENTER != 1) {
+    ux = ux + ex * cst;
+    uy = uy + ey * cst;
+    uz = uz + ez * cst;
+  }
+  const double cb = P.q * (CENTER == 0 ? P.dt : halfdt) * 0.5 / P.m;
   const double tx = gi * bx * cb, ty = gi * by * cb, tz = gi * bz * cb;
   const double tsqi = 2. / (1. + tx * tx + ty * ty + tz * tz);
   const double sx = tx * tsqi, sy = ty * tsqi, sz = tz * tsqi;
@@ -382,6 +391,12 @@ __global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ p
   ux = ux + uyppr * sz - uzppr * sy;
   uy = uy + uzppr * sx - uxppr * sz;
   uz = uz + uxppr * sy - uyppr * sx;
+  if (CENTER == 2) {
+    uxp[i] = ux;
+    uyp[i] = uy;
+    uzp[i] = uz;
+    return;
+  }
   ux = ux + ex * cst;
   uy = uy + ey * cst;
   uz = uz + ez * cst;
@@ -575,11 +590,17 @@ int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
     set_error("wg_advance: use_lattice set but no lattice installed (wg_set_lattice)");
     return WG_ESTATE;
   }
+  if (prm->center != WG_CENTER_FULLV && prm->center != WG_CENTER_HALFV && prm->center != WG_CENTER_SYNCHV) {
+    set_error("wg_advance: center must be WG_CENTER_FULLV, WG_CENTER_HALFV or WG_CENTER_SYNCHV");
+    return WG_EINVAL;
+  }
   if (p->np == 0) return WG_OK;
   PushP P{p->q, p->m, prm->dt, c->grid.zmmin, c->grid.zmmax, prm->prwall, prm->prwallx, prm->prwally,
           prm->use_lattice ? c->czs : nullptr, c->cze, c->cdb, c->nzl, c->zlmin, c->dzl};
-  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); k_advance<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, p->x, p->y, p->z, p->ux, p->uy,
-                                                       p->uz, p->gaminv, p->np); c->prof_end(pe); }
+  auto kern = prm->center == WG_CENTER_HALFV ? k_advance<1> : prm->center == WG_CENTER_SYNCHV ? k_advance<2>
+                                                                                               : k_advance<0>;
+  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, p->x, p->y, p->z, p->ux, p->uy,
+                                                  p->uz, p->gaminv, p->np); c->prof_end(pe); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }

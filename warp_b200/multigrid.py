@@ -325,16 +325,24 @@ class MultiGridB200(FieldSolver):
                                            cdb.ctypes.data_as(_lib._dp), nzl, zlmin, dzl))
         self._lattice = (czs, cze, cdb, nzl, zlmin, dzl)
 
-    def advance(self, pgroup, dt, prwall=1.e30, prwallx=0., prwally=0., start=0, stop=None):
-        """One fused fullv particle advance of padvnc3d (w3d.F:1862-1987)
-        plus particleboundaries3d: gather E from phi, quad B (if a lattice
-        is installed), half E kick, Boris rotation, half E kick, drift,
+    def advance(self, pgroup, dt, prwall=1.e30, prwallx=0., prwally=0., start=0, stop=None, center="fullv"):
+        """One fused particle advance of padvnc3d (w3d.F:1575) plus
+        particleboundaries3d: gather E from phi, quad B (if a lattice is
+        installed), the velocity push and drift that center selects, the
         periodic z wrap and the round absorbing pipe of radius prwall.
-        start/stop restrict it to a range of the group's particles."""
+        center "fullv" (w3d.F:1862-1987): half E kick, Boris rotation, half
+        E kick, drift. "halfv" (w3d.F:1989-2125), the first step after
+        loading, when velocities are still at the positions' time: half-dt
+        rotation, half E kick, drift. "synchv" (w3d.F:2187-2310): half E kick
+        and half-dt rotation only, bringing velocities back to the
+        positions' time. start/stop restrict it to a range of the group's
+        particles."""
+        if center not in _lib.CENTERS:
+            raise ValueError("center must be one of %s" % sorted(_lib.CENTERS))
         self._bind_stream()
         s = pgroup.cstruct(start, stop)
         p = _lib.PushParams(float(dt), float(prwall), float(prwallx), float(prwally),
-                            int(self._lattice is not None))
+                            int(self._lattice is not None), _lib.CENTERS[center])
         _lib.check(_lib.lib.wg_advance(self._h, ctypes.byref(s), ctypes.byref(p)))
 
     def moments(self, pgroup):

@@ -140,3 +140,61 @@ def beam_weight(current, length, n, ekin_ev=1e6, mass=proton_mass, charge=echarg
     gamma = 1. + ekin_ev * echarge / (mass * clight * clight)
     v = math.sqrt(1. - 1. / (gamma * gamma)) * clight
     return current * length / (charge * v * n)
+
+
+def semigaussian_matched(n, generator, z, a, b, ap, bp, emitx, emity, zmin, zmax, v, device="cuda"):
+    """Semi-Gaussian beam that follows an envelope, as the reference loads
+    it from its env package (w3d.distrbtn = "semigaus"): z uniform in
+    [zmin, zmax); at each particle's z the envelope (a, b, a', b', given on
+    the grid z and interpolated linearly) sets a uniform density in the
+    ellipse (x/a)^2 + (y/b)^2 <= 1, the slope x' = (a'/a) x plus a Gaussian
+    spread of rms emitx / (2 a) (so the 4 x rms emittance is emitx), and
+    likewise in y. uz = v (non-relativistic, gaminv = 1)."""
+    kw = dict(generator=generator, device=device, dtype=torch.float64)
+    zt = torch.as_tensor(np.asarray(z, dtype=np.float64), device=device)
+
+    def interp(f):
+        ft = torch.as_tensor(np.asarray(f, dtype=np.float64), device=device)
+        idx = torch.clamp(torch.searchsorted(zt, zp) - 1, 0, zt.numel() - 2)
+        t = (zp - zt[idx]) / (zt[idx + 1] - zt[idx])
+        return ft[idx] + t * (ft[idx + 1] - ft[idx])
+
+    zp = zmin + (zmax - zmin) * torch.rand(n, **kw)
+    aa, bb, aap, bbp = interp(a), interp(b), interp(ap), interp(bp)
+    r = torch.sqrt(torch.rand(n, **kw))
+    th = 2. * math.pi * torch.rand(n, **kw)
+    x = aa * r * torch.cos(th)
+    y = bb * r * torch.sin(th)
+    xp = aap / aa * x + emitx / (2. * aa) * torch.randn(n, **kw)
+    yp = bbp / bb * y + emity / (2. * bb) * torch.randn(n, **kw)
+    return {"x": x, "y": y, "z": zp, "ux": xp * v, "uy": yp * v,
+            "uz": torch.full((n,), float(v), device=device, dtype=torch.float64),
+            "gaminv": torch.ones(n, device=device, dtype=torch.float64)}
+
+
+def rms_along_z(pgroup, zmin, zmax, nz, periodic=True):
+    """rms x and y sizes of the live particles on the z grid nodes
+    zmin + k (zmax - zmin) / nz, k = 0..nz, with linear weighting in z (the
+    z moments of getzmmnt, top.F:521-1444, xrmsz and yrmsz). With periodic z
+    the end nodes share their particles. Returns two numpy arrays."""
+    import torch as _t
+    live = pgroup.gaminv != 0
+    x, y, z = pgroup.x[live], pgroup.y[live], pgroup.z[live]
+    dz = (zmax - zmin) / nz
+    s = (z - zmin) / dz
+    k = _t.clamp(_t.floor(s).long(), 0, nz - 1)
+    f = s - k
+    n0 = _t.zeros(nz + 1, dtype=_t.float64, device=x.device)
+    sums = [n0.clone() for _ in range(5)]
+    for arr, val in zip(sums, (_t.ones_like(x), x, y, x * x, y * y)):
+        arr.index_add_(0, k, (1. - f) * val)
+        arr.index_add_(0, k + 1, f * val)
+    if periodic:
+        for arr in sums:
+            arr[0] += arr[nz]
+            arr[nz] = arr[0]
+    w, sx, sy, sxx, syy = sums
+    w = _t.clamp(w, min=1e-300)
+    xr = _t.sqrt(_t.clamp(sxx / w - (sx / w) ** 2, min=0.))
+    yr = _t.sqrt(_t.clamp(syy / w - (sy / w) ** 2, min=0.))
+    return xr.cpu().numpy(), yr.cpu().numpy()
