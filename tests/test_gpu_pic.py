@@ -1,6 +1,7 @@
 """End-to-end PIC parity on the 32x32x64 / 2e5-proton workload: the B200
 path (fixed-point deposit, FP64 multigrid with the pipe conductor, fused
-fullv advance) against the FP64 oracle stepping the same seeded beam.
+advance: halfv on the first step, fullv after it, and a final synchv)
+against the FP64 oracle stepping the same seeded beam.
 
 Tolerance: the deposit differs from an FP64 running sum by the 2^-46
 fixed-point rounding of each weight (about 1e-15 relative on rho); over the
@@ -19,15 +20,22 @@ NSTEPS = 8
 TOL = 1e-9
 
 
-def _oracle_step(state, cfg, oc, tables, dt, q, m, w, first=False):
+def _oracle_push(state, cfg, tables, dt, q, m, center):
     phi, p = state["phi"], state["p"]
     dx, dy, dz = state["d"]
     mins = (cfg["xmmin"], cfg["ymmin"], cfg["zmmin"])
-    if not first:
-        ex, ey, ez = oracle.sete(phi, p["x"], p["y"], p["z"], dx, dy, dz, *mins)
-        czs, cze, cdb, nzl, zlmin, dzl = tables
-        oracle.push_fullv(p, ex, ey, ez, q, m, dt, (czs, cze, cdb), zlmin, dzl, cfg["zmmin"], cfg["zmmax"],
-                          cfg["pipe_radius"])
+    ex, ey, ez = oracle.sete(phi, p["x"], p["y"], p["z"], dx, dy, dz, *mins)
+    czs, cze, cdb, nzl, zlmin, dzl = tables
+    oracle.push(p, ex, ey, ez, q, m, dt, (czs, cze, cdb), zlmin, dzl, cfg["zmmin"], cfg["zmmax"],
+                cfg["pipe_radius"], center=center)
+
+
+def _oracle_step(state, cfg, oc, tables, dt, q, m, w, center=None):
+    phi, p = state["phi"], state["p"]
+    dx, dy, dz = state["d"]
+    mins = (cfg["xmmin"], cfg["ymmin"], cfg["zmmin"])
+    if center is not None:
+        _oracle_push(state, cfg, tables, dt, q, m, center)
     rho = np.zeros((cfg["nx"] + 1, cfg["ny"] + 1, cfg["nz"] + 1), order="F")
     oracle.setrho(rho, p["x"], p["y"], p["z"], q, w, dx, dy, dz, *mins, gaminv=p["gaminv"])
     oracle.rhobc(rho, (0, 0, 0, 0, 2, 2))
@@ -46,12 +54,14 @@ def test_pic_workload_A_matches_oracle():
     oc = H.oracle_conductors(s, shapes)
     state = {"phi": np.zeros((s.nx + 3, s.ny + 3, s.nz + 3), order="F"), "p": p0, "d": (s.dx, s.dy, s.dz)}
     pg = run.pgroup
-    it = _oracle_step(state, cfg, oc, s._lattice, run.dt, pg.q, pg.m, pg.w, first=True)
+    it = _oracle_step(state, cfg, oc, s._lattice, run.dt, pg.q, pg.m, pg.w)
     assert it == s.mgiters
     for n in range(NSTEPS):
         run.step()
-        it = _oracle_step(state, cfg, oc, s._lattice, run.dt, pg.q, pg.m, pg.w)
+        it = _oracle_step(state, cfg, oc, s._lattice, run.dt, pg.q, pg.m, pg.w, "halfv" if n == 0 else "fullv")
         assert it == s.mgiters, "step %d: V-cycles %d vs %d" % (n, s.mgiters, it)
+    run.synchv()
+    _oracle_push(state, cfg, s._lattice, run.dt, pg.q, pg.m, "synchv")
     gphi = s.phi.cpu().numpy()
     scale = np.max(np.abs(state["phi"]))
     assert np.max(np.abs(gphi - state["phi"])) <= TOL * scale
@@ -151,7 +161,7 @@ def test_dump_and_restart_continue_bit_for_bit(tmp_path):
     fname = run.dump(str(tmp_path / "run.dump.npz"))
     run.step(3)
     again = pic.restart(fname)
-    assert again.it == 4
+    assert again.it == 4 and again.vsync is False
     again.step(3)
     torch.cuda.synchronize()
     for k in FIELDS:

@@ -3,10 +3,12 @@
 MultiGridB200.
 
 Order inside one step (step3d): particle advance with the field of the
-previous solve (padvnc3d fullv: gather, quads, leapfrog/Boris, drift),
-particle boundaries (periodic z, absorbing pipe), charge deposition
-(loadrho), field solve. Loaded velocities are taken as time-centred at
-t - dt/2, so every step is a fullv step.
+previous solve (padvnc3d: gather, quads, leapfrog/Boris, drift), particle
+boundaries (periodic z, absorbing pipe), charge deposition (loadrho), field
+solve. Loaded velocities are at the positions' time, so the first step is
+halfv (w3d.F:780 with lspecial at it == 0) and the steps after it fullv;
+ESPIC.synchv() brings the velocities back to the positions' time for
+diagnostics, after which the next step is halfv again.
 
 Workloads (synthetic, seeded):
   WORKLOADS["A"]: 32x32x64 cells over 8 cm x 8 cm x 1 m, 2e5 protons at
@@ -92,6 +94,8 @@ class ESPIC:
         self.solver.addpgroup(self.pgroup)
         self.sort_interval = int(sort_interval)
         self.it = 0
+        # velocities at the positions' time (true after loading and synchv)
+        self.vsync = True
 
     def generate(self):
         """Initial deposit and field solve (w3dgen -> step3d("w3dgen"))."""
@@ -100,9 +104,13 @@ class ESPIC:
         self.solver.loadrho()
         self.solver.solve()
 
+    def _center(self):
+        return "halfv" if self.vsync else "fullv"
+
     def step(self, n=1):
         for _ in range(n):
-            self.solver.advance(self.pgroup, self.dt, prwall=self.cfg["pipe_radius"])
+            self.solver.advance(self.pgroup, self.dt, prwall=self.cfg["pipe_radius"], center=self._center())
+            self.vsync = False
             if self.sort_interval > 0 and (self.it + 1) % self.sort_interval == 0:
                 # re-sort by cell (and drop lost particles) every sort_interval steps
                 self.pgroup.sort(self.solver)
@@ -134,6 +142,7 @@ class ESPIC:
             self._d2h = torch.cuda.Stream(pg.device)
         h2d, d2h = self._h2d, self._d2h
         edges = [n * k // nchunks for k in range(nchunks + 1)]
+        center = self._center()
         landed, advanced = [], []
         h2d.wait_stream(main)
         with torch.cuda.stream(h2d):
@@ -148,7 +157,7 @@ class ESPIC:
             a, b = edges[k], edges[k + 1]
             main.wait_event(landed[k])
             if b > a:
-                self.solver.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], start=a, stop=b)
+                self.solver.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], start=a, stop=b, center=center)
             ev = torch.cuda.Event()
             ev.record(main)
             advanced.append(ev)
@@ -161,9 +170,21 @@ class ESPIC:
         self.solver.loadrho()
         self.solver.solve()
         main.wait_stream(d2h)
+        self.vsync = False
         self.it += 1
 
+    def synchv(self):
+        """padvnc3d("synchv") at the end of a special step (w3d.F:975): a
+        half kick with the field of the last solve takes the velocities from
+        t - dt/2 to t, where the positions are. The next step is then halfv.
+        Does nothing when the velocities are already in step."""
+        if not self.vsync:
+            self.solver.advance(self.pgroup, self.dt, prwall=self.cfg["pipe_radius"], center="synchv")
+            self.vsync = True
+
     def moments(self):
+        """Moments of the particles as they are; call synchv() first for
+        velocities at the positions' time (the reference's special step)."""
         return self.solver.moments(self.pgroup)
 
     def dump(self, filename=None, prefix="", runid="espic", suffix=""):
@@ -178,7 +199,8 @@ class ESPIC:
             filename = "%s%s%06d%s.dump.npz" % (prefix, runid, self.it, suffix)
         s, pg = self.solver, self.pgroup
         arrays = {"p_" + k: v for k, v in pg.to_numpy().items()}
-        meta = {"cfg": self.cfg, "it": self.it, "sort_interval": self.sort_interval, "precision": s.precision,
+        meta = {"cfg": self.cfg, "it": self.it, "vsync": self.vsync, "sort_interval": self.sort_interval,
+                "precision": s.precision,
                 "tolkind": s.tolkind, "mgtol": s.mgtol, "mgmaxiters": s.mgmaxiters, "q": pg.q, "m": pg.m,
                 "w": pg.w}
         with open(filename, "wb") as f:
@@ -201,4 +223,5 @@ def restart(filename, device="cuda"):
     run.pgroup.q, run.pgroup.m, run.pgroup.w = meta["q"], meta["m"], meta["w"]
     run.solver.phi = np.asfortranarray(phi)
     run.it = meta["it"]
+    run.vsync = meta["vsync"]
     return run
