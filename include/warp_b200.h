@@ -183,6 +183,15 @@ int wg_fetch_e(wg_ctx* ctx, const double* x, const double* y, const double* z, d
  * Host arrays of length nzl+1. */
 int wg_set_lattice(wg_ctx* ctx, const double* czs, const double* cze, const double* cdb, int nzl,
                    double zlmin, double dzl);
+/* lcorrectede (f3d.v:152 Conductor3d.lcorrectede; used by
+ * MultiGrid3D.fetchfieldfrompositions, scripts/multigrid.py:528-546): when
+ * on, wg_fetch_e and wg_advance gather E with sete3dwithconductor, efetch = 1
+ * (f3d_mgrid.F:4774-5220). Next to a conductor the field then comes from the
+ * subgrid points' dels and volt (getefieldatconductorsubgrid, :4635-4735,
+ * recomputed from the current phi at each call, over an icgrid built as
+ * setupconductorfielddata, :4581-4632, does), and particles outside the grid
+ * get no field. Off by default, as in the reference. */
+int wg_set_correctede(wg_ctx* ctx, int on);
 /* One fused step of padvnc3d (w3d.F:1575) followed by particleboundaries3d
  * (w3d.F:11292): gather E (sete_from_phi_linear3d), quad B (applyquad),
  * epush3d/bpush3d(ibpush=1)/epush3d/xpush3d (w3d.F:2752,2834,3070) as

@@ -1403,6 +1403,167 @@ void or_push(int center, int64_t np, double* xp, double* yp, double* zp, double*
   });
 }
 
+// lcorrectede: E at particles next to conductors from the subgrid data.
+// 1. icgrid over the level-0 nodes (setupconductorfielddata,
+//    f3d_mgrid.F:4581-4632): 0 in vacuum, nmax+1 at level-0 interior points,
+//    then the 1-based list index at even subgrid points and minus it at odd
+//    ones, written in that order.
+// 2. At every level-0 subgrid point, efield0 (centred, one per axis) and
+//    efieldd (one-sided, one per direction, only towards an interior
+//    neighbour) from phi and the conductor's dels/volt
+//    (getefieldatconductorsubgrid and SETEE, f3d_mgrid.F:4635-4735). Nothing is
+//    computed unless both subgrid lists are non-empty; the fields stay 0.
+// 3. The efetch = 1 gather of sete3dwithconductor (f3d_mgrid.F:4774-5020,
+//    GETEEFROME :5160-5220): particles outside the grid get nothing; cells
+//    whose 8 nodes are all vacuum use centred differences with each term
+//    scaled by 1/(2 dx); other cells weight, per edge of the cell, the
+//    vacuum differences and the conductor points' fields by the particle's
+//    weights, normalized by the weights used.
+// A particle on an upper grid face uses the last cell with fraction 1 (the
+// reference reads one node past the array there). E is ADDED to ex,ey,ez.
+void or_sete_cond(or_conductors* hc, int nx, int ny, int nz, double dx, double dy, double dz, double xmmin,
+                  double ymmin, double zmmin, double zgrid, const double* phi, int64_t np, const double* xp,
+                  const double* yp, const double* zp, double* ex, double* ey, double* ez) {
+  const Conductors& C = *reinterpret_cast<Conductors*>(hc);
+  auto P = [&](int ix, int iy, int iz) { return phi[pidx(nx, ny, ix, iy, iz)]; };
+  const int nmax = (int)std::max(C.even.n(), C.odd.n());
+  std::vector<int> icgrid((size_t)(nx + 1) * (ny + 1) * (nz + 1), 0);
+  auto ICG = [&](int ix, int iy, int iz) -> int& { return icgrid[ridx(nx, ny, ix, iy, iz)]; };
+  const Interior& I = C.interior;
+  for (int ic = I.istart[0]; ic < I.istart[1]; ++ic) ICG(I.indx[3 * ic], I.indx[3 * ic + 1], I.indx[3 * ic + 2]) = nmax + 1;
+  for (int ie = C.even.istart[0]; ie < C.even.istart[1]; ++ie)
+    ICG(C.even.indx[3 * ie], C.even.indx[3 * ie + 1], C.even.indx[3 * ie + 2]) = ie + 1;
+  for (int io = C.odd.istart[0]; io < C.odd.istart[1]; ++io)
+    ICG(C.odd.indx[3 * io], C.odd.indx[3 * io + 1], C.odd.indx[3 * io + 2]) = -(io + 1);
+
+  std::vector<double> e0[2], ed[2];
+  const Subgrid* L[2] = {&C.even, &C.odd};
+  for (int s = 0; s < 2; ++s) {
+    e0[s].assign(3 * L[s]->n(), 0.);
+    ed[s].assign(6 * L[s]->n(), 0.);
+  }
+  if (C.even.n() > 0 && C.odd.n() > 0) {
+    for (int s = 0; s < 2; ++s) {
+      const Subgrid& S = *L[s];
+      for (int ic = S.istart[0]; ic < S.istart[1]; ++ic) {
+        const int ix = S.indx[3 * ic], iy = S.indx[3 * ic + 1], iz = S.indx[3 * ic + 2];
+        const double* dels = &S.dels[6 * ic];
+        const double* volt = &S.volt[6 * ic];
+        for (int id = 0; id < 3; ++id) {
+          const int mx = id == 0 ? -1 : 0, my = id == 1 ? -1 : 0, mz = id == 2 ? -1 : 0;
+          const int px = -mx, py = -my, pz = -mz;
+          const double di = id == 0 ? 1. / dx : id == 1 ? 1. / dy : 1. / dz;
+          const int im = 2 * id, ip = 2 * id + 1;
+          double vv0, dd0, vv1, dd1;
+          if (0. < dels[im] && dels[im] <= 1.) { vv0 = volt[im]; dd0 = dels[im]; }
+          else { vv0 = P(ix + mx, iy + my, iz + mz); dd0 = 1.; }
+          if (0. < dels[ip] && dels[ip] <= 1.) { vv1 = volt[ip]; dd1 = dels[ip]; }
+          else { vv1 = P(ix + px, iy + py, iz + pz); dd1 = 1.; }
+          const double ppp = P(ix, iy, iz);
+          e0[s][3 * ic + id] = (dd1 / (dd0 + dd1) * (vv0 - ppp) / dd0 + dd0 / (dd0 + dd1) * (ppp - vv1) / dd1) * di;
+          if (ix + mx >= 0 && iy + my >= 0 && iz + mz >= 0 && ICG(ix + mx, iy + my, iz + mz) > nmax)
+            ed[s][6 * ic + im] = ((vv0 - ppp) / dd0 - (2. - dd0) / (2. + dd1) * (ppp - vv1) / dd1) *
+                                 ((2. + dd1) / (dd1 + dd0)) * di;
+          if (ix + px <= nx && iy + py <= ny && iz + pz <= nz && ICG(ix + px, iy + py, iz + pz) > nmax)
+            ed[s][6 * ic + ip] = ((ppp - vv1) / dd1 - (2. - dd1) / (2. + dd0) * (vv0 - ppp) / dd0) *
+                                 ((2. + dd0) / (dd0 + dd1)) * di;
+        }
+      }
+    }
+  }
+  auto E0 = [&](int ic, int id) { return ic < 0 ? e0[1][3 * (-ic - 1) + id] : e0[0][3 * (ic - 1) + id]; };
+  auto ED = [&](int ic, int k) { return ic < 0 ? ed[1][6 * (-ic - 1) + k] : ed[0][6 * (ic - 1) + k]; };
+
+  const double tdxi = 1. / (2. * dx), tdyi = 1. / (2. * dy), tdzi = 1. / (2. * dz);
+  const double dxi = 1. / dx, dyi = 1. / dy, dzi = 1. / dz;
+  // particles are independent
+  par_for(0, np, [&](int64_t ip) {
+    const double xi = (xp[ip] - xmmin) * dxi, yj = (yp[ip] - ymmin) * dyi, zk = (zp[ip] - zgrid - zmmin) * dzi;
+    if (xi < 0. || xi > nx || yj < 0. || yj > ny || zk < 0. || zk > nz) return;
+    int i, j, k;
+    double u1, v1, w1;
+    cellfrac(xi, nx, i, u1);
+    cellfrac(yj, ny, j, v1);
+    cellfrac(zk, nz, k, w1);
+    const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+    double ext, eyt, ezt;
+    if (ICG(i, j, k) == 0 && ICG(i + 1, j, k) == 0 && ICG(i, j + 1, k) == 0 && ICG(i + 1, j + 1, k) == 0 &&
+        ICG(i, j, k + 1) == 0 && ICG(i + 1, j, k + 1) == 0 && ICG(i, j + 1, k + 1) == 0 &&
+        ICG(i + 1, j + 1, k + 1) == 0) {
+      ext = u0 * v0 * w0 * (P(i - 1, j, k) - P(i + 1, j, k)) * tdxi + u1 * v0 * w0 * (P(i, j, k) - P(i + 2, j, k)) * tdxi +
+            u0 * v1 * w0 * (P(i - 1, j + 1, k) - P(i + 1, j + 1, k)) * tdxi +
+            u1 * v1 * w0 * (P(i, j + 1, k) - P(i + 2, j + 1, k)) * tdxi +
+            u0 * v0 * w1 * (P(i - 1, j, k + 1) - P(i + 1, j, k + 1)) * tdxi +
+            u1 * v0 * w1 * (P(i, j, k + 1) - P(i + 2, j, k + 1)) * tdxi +
+            u0 * v1 * w1 * (P(i - 1, j + 1, k + 1) - P(i + 1, j + 1, k + 1)) * tdxi +
+            u1 * v1 * w1 * (P(i, j + 1, k + 1) - P(i + 2, j + 1, k + 1)) * tdxi;
+      eyt = u0 * v0 * w0 * (P(i, j - 1, k) - P(i, j + 1, k)) * tdyi + u1 * v0 * w0 * (P(i + 1, j - 1, k) - P(i + 1, j + 1, k)) * tdyi +
+            u0 * v1 * w0 * (P(i, j, k) - P(i, j + 2, k)) * tdyi + u1 * v1 * w0 * (P(i + 1, j, k) - P(i + 1, j + 2, k)) * tdyi +
+            u0 * v0 * w1 * (P(i, j - 1, k + 1) - P(i, j + 1, k + 1)) * tdyi +
+            u1 * v0 * w1 * (P(i + 1, j - 1, k + 1) - P(i + 1, j + 1, k + 1)) * tdyi +
+            u0 * v1 * w1 * (P(i, j, k + 1) - P(i, j + 2, k + 1)) * tdyi +
+            u1 * v1 * w1 * (P(i + 1, j, k + 1) - P(i + 1, j + 2, k + 1)) * tdyi;
+      ezt = u0 * v0 * w0 * (P(i, j, k - 1) - P(i, j, k + 1)) * tdzi + u1 * v0 * w0 * (P(i + 1, j, k - 1) - P(i + 1, j, k + 1)) * tdzi +
+            u0 * v1 * w0 * (P(i, j + 1, k - 1) - P(i, j + 1, k + 1)) * tdzi +
+            u1 * v1 * w0 * (P(i + 1, j + 1, k - 1) - P(i + 1, j + 1, k + 1)) * tdzi +
+            u0 * v0 * w1 * (P(i, j, k) - P(i, j, k + 2)) * tdzi + u1 * v0 * w1 * (P(i + 1, j, k) - P(i + 1, j, k + 2)) * tdzi +
+            u0 * v1 * w1 * (P(i, j + 1, k) - P(i, j + 1, k + 2)) * tdzi +
+            u1 * v1 * w1 * (P(i + 1, j + 1, k) - P(i + 1, j + 1, k + 2)) * tdzi;
+    } else {
+      double ee[3] = {0., 0., 0.}, ww[3] = {0., 0., 0.};
+      // GETEEFROME: the cell edge from node a = (i+ox, j+oy, k+oz) to a + p
+      auto edge = [&](int id, int ox, int oy, int oz, int px, int py, int pz, double di, double wm, double wp) {
+        const int ax = i + ox, ay = j + oy, az = k + oz;
+        int ic = ICG(ax, ay, az);
+        if (ic == 0) {
+          ee[id] = ee[id] + wm * (P(ax - px, ay - py, az - pz) - P(ax + px, ay + py, az + pz)) * 0.5 * di;
+          ww[id] = ww[id] + wm;
+        } else if (ic < nmax + 1) {
+          ee[id] = ee[id] + wm * E0(ic, id);
+          ww[id] = ww[id] + wm;
+          if (ICG(ax + px, ay + py, az + pz) > nmax) {
+            ee[id] = ee[id] + wp * ED(ic, 2 * id + 1);
+            ww[id] = ww[id] + wp;
+          }
+        }
+        ic = ICG(ax + px, ay + py, az + pz);
+        if (ic == 0) {
+          ee[id] = ee[id] + wp * (P(ax, ay, az) - P(ax + 2 * px, ay + 2 * py, az + 2 * pz)) * 0.5 * di;
+          ww[id] = ww[id] + wp;
+        } else if (ic < nmax + 1) {
+          ee[id] = ee[id] + wp * E0(ic, id);
+          ww[id] = ww[id] + wp;
+          if (ICG(ax, ay, az) > nmax) {
+            ee[id] = ee[id] + wm * ED(ic, 2 * id);
+            ww[id] = ww[id] + wm;
+          }
+        }
+      };
+      edge(0, 0, 0, 0, 1, 0, 0, dxi, u0 * v0 * w0, u1 * v0 * w0);
+      edge(0, 0, 1, 0, 1, 0, 0, dxi, u0 * v1 * w0, u1 * v1 * w0);
+      edge(0, 0, 0, 1, 1, 0, 0, dxi, u0 * v0 * w1, u1 * v0 * w1);
+      edge(0, 0, 1, 1, 1, 0, 0, dxi, u0 * v1 * w1, u1 * v1 * w1);
+      if (ww[0] != 0.) ww[0] = 1. / ww[0];
+      edge(1, 0, 0, 0, 0, 1, 0, dyi, u0 * v0 * w0, u0 * v1 * w0);
+      edge(1, 1, 0, 0, 0, 1, 0, dyi, u1 * v0 * w0, u1 * v1 * w0);
+      edge(1, 0, 0, 1, 0, 1, 0, dyi, u0 * v0 * w1, u0 * v1 * w1);
+      edge(1, 1, 0, 1, 0, 1, 0, dyi, u1 * v0 * w1, u1 * v1 * w1);
+      if (ww[1] != 0.) ww[1] = 1. / ww[1];
+      edge(2, 0, 0, 0, 0, 0, 1, dzi, u0 * v0 * w0, u0 * v0 * w1);
+      edge(2, 1, 0, 0, 0, 0, 1, dzi, u1 * v0 * w0, u1 * v0 * w1);
+      edge(2, 0, 1, 0, 0, 0, 1, dzi, u0 * v1 * w0, u0 * v1 * w1);
+      edge(2, 1, 1, 0, 0, 0, 1, dzi, u1 * v1 * w0, u1 * v1 * w1);
+      if (ww[2] != 0.) ww[2] = 1. / ww[2];
+      ext = ee[0] * ww[0];
+      eyt = ee[1] * ww[1];
+      ezt = ee[2] * ww[2];
+    }
+    ex[ip] = ex[ip] + ext;
+    ey[ip] = ey[ip] + eyt;
+    ez[ip] = ez[ip] + ezt;
+  });
+}
+
 // Global moments of the live particles (getzmmnt, top.F:521-1444). out[]:
 // 0 n, 1 xbar, 2 ybar, 3 xrms, 4 yrms, 5 epsx, 6 epsy (x' = ux/uz).
 void or_moments(int64_t np, const double* xp, const double* yp, const double* uxp, const double* uyp,

@@ -59,6 +59,8 @@ def lib():
         L.or_push.argtypes = [ctypes.c_int, ctypes.c_int64] + [_dp] * 10 + [ctypes.c_double] * 3 + [_dp] * 3 + \
             [ctypes.c_int] + [ctypes.c_double] * 7
         L.or_moments.argtypes = [ctypes.c_int64] + [_dp] * 6 + [_dp]
+        L.or_sete_cond.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 3 + [ctypes.c_double] * 7 + \
+            [_dp, ctypes.c_int64] + [_dp] * 6
         L.or_eps0.restype = ctypes.c_double
         L.or_threads.restype = ctypes.c_int
         L.or_ese.argtypes = [ctypes.c_int] * 3 + [_dp, _dp] + [ctypes.c_double] * 3
@@ -212,6 +214,21 @@ def quad_tables(zs, ze, db, zlatperi, zlatstrt, zlmin, dzl, nzl):
     lib().or_quad_table(len(zs), _d(zs), _d(ze), _d(db), zlatperi, zlatstrt, zlmin, dzl, nzl, _d(czs), _d(cze),
                         _d(cdb))
     return czs, cze, cdb
+
+
+def sete_cond(conductors, phi, x, y, z, dx, dy, dz, xmmin, ymmin, zmmin, zgrid=0.0):
+    """E at the particles with the conductor correction (lcorrectede) of
+    sete3dwithconductor, efetch = 1; conductors is a finalized Conductors
+    of the same grid. Returns new arrays ex, ey, ez (zero for particles
+    outside the grid)."""
+    nx, ny, nz = (s - 3 for s in phi.shape)
+    phi = np.asfortranarray(phi, dtype=np.float64)
+    n = len(x)
+    ex, ey, ez = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib().or_sete_cond(conductors.h, nx, ny, nz, dx, dy, dz, xmmin, ymmin, zmmin, zgrid, _d(phi), n,
+                       _d(np.ascontiguousarray(x, np.float64)), _d(np.ascontiguousarray(y, np.float64)),
+                       _d(np.ascontiguousarray(z, np.float64)), _d(ex), _d(ey), _d(ez))
+    return ex, ey, ez
 
 
 _CENTERS = {"fullv": 0, "halfv": 1, "synchv": 2}

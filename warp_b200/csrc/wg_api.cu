@@ -190,6 +190,11 @@ void free_all(wg_ctx* c) {
   dfree(c->czs);
   dfree(c->cze);
   dfree(c->cdb);
+  dfree(c->icgrid);
+  for (int s = 0; s < 2; ++s) {
+    dfree(c->ef0[s]);
+    dfree(c->efd[s]);
+  }
   if (c->hred) cudaFreeHost(c->hred);
   c->hred = nullptr;
 }
@@ -511,6 +516,12 @@ int wg_set_lattice(wg_ctx* c, const double* czs, const double* cze, const double
   c->nzl = nzl;
   c->zlmin = zlmin;
   c->dzl = dzl;
+  return WG_OK;
+}
+
+int wg_set_correctede(wg_ctx* c, int on) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  c->correctede = on ? 1 : 0;
   return WG_OK;
 }
 

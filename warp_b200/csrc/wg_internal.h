@@ -95,6 +95,8 @@ struct Level {
 };
 
 constexpr int kRestrictTaps = 4;
+// icgrid value of a level-0 conductor interior node (the reference's nmax+1)
+constexpr int kIcInterior = 0x7fffffff;
 
 std::vector<LevelDims> mglevels(int nx, int ny, int nz, double dx, double dy, double dz);
 
@@ -131,6 +133,12 @@ struct wg_ctx {
   int nzl = -1;
   double zlmin = 0., dzl = 1.;
   bool have_fp32 = false;
+  // lcorrectede: E next to conductors from the subgrid data
+  int correctede = 0;
+  int* icgrid = nullptr;                 // level-0 nodes: 0 vacuum, kIcInterior, +/- (subgrid index + 1)
+  double* ef0[2] = {nullptr, nullptr};   // efield0 of the level-0 even/odd subgrid points, 3 per point
+  double* efd[2] = {nullptr, nullptr};   // efieldd, 6 per point
+  long long icgrid_version = 0;          // cond_version the icgrid was built for
   // kernels launched by this context (cumulative; a graph replay counts its kernels)
   long long nlaunch = 0;
   // captured V-cycles (index 0: FP64, 1: FP32), valid for vgraph_key

@@ -303,6 +303,192 @@ __device__ inline void gather_e(const double* __restrict__ phi, const GridP& g, 
                 u1 * v1 * w1 * (P(i + 1, j + 1, k) - P(i + 1, j + 1, k + 2)));
 }
 
+// ---- lcorrectede: E next to conductors (sete3dwithconductor) -------------
+
+// Level-0 conductor data read by the corrected gather.
+struct CondE {
+  const int* icg;   // icgrid over the level-0 nodes
+  const double* e0e;  // efield0 of the even subgrid points, 3 per point
+  const double* e0o;  // odd
+  const double* ede;  // efieldd of the even points, 6 per point
+  const double* edo;  // odd
+};
+
+// setupconductorfielddata (f3d_mgrid.F:4581-4632): one list into icgrid.
+// value 0 writes kIcInterior; +1/-1 write +/-(list index + 1).
+__global__ void k_icgrid_fill(const int32_t* __restrict__ ijk, int n, int value, int nx, int ny, int nz,
+                              int* __restrict__ icg) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int ix = ijk[3 * t], iy = ijk[3 * t + 1], iz = ijk[3 * t + 2];
+  if (ix < 0 || ix > nx || iy < 0 || iy > ny || iz < 0 || iz > nz) return;
+  icg[(size_t)ix + (size_t)(nx + 1) * ((size_t)iy + (size_t)(ny + 1) * iz)] = value == 0 ? kIcInterior : value * (t + 1);
+}
+
+// getefieldatconductorsubgrid / SETEE (f3d_mgrid.F:4635-4735) at the level-0
+// subgrid points of one list: efield0 per axis from the two sides (the
+// conductor surface at dels with its volt, or the neighbour node), and
+// efieldd towards each neighbour that is an interior node.
+__global__ void k_efield_sub(const double* __restrict__ phi, GridP g, const int32_t* __restrict__ ijk,
+                             const double* __restrict__ dels, const double* __restrict__ volt, int n,
+                             const int* __restrict__ icg, double* __restrict__ e0, double* __restrict__ ed) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int ix = ijk[3 * t], iy = ijk[3 * t + 1], iz = ijk[3 * t + 2];
+  if (ix < 0 || ix > g.nx || iy < 0 || iy > g.ny || iz < 0 || iz > g.nz) return;
+  const int sy = g.nx + 3, sz = sy * (g.ny + 3);
+  const double* p0 = phi + ((ix + 1) + sy * (iy + 1) + sz * (iz + 1));
+  const int cy = g.nx + 1, cz = cy * (g.ny + 1);
+  const int* c0 = icg + ((size_t)ix + (size_t)cy * iy + (size_t)cz * iz);
+  const double ppp = p0[0];
+#pragma unroll
+  for (int id = 0; id < 3; ++id) {
+    const int so = id == 0 ? 1 : id == 1 ? sy : sz;
+    const int co = id == 0 ? 1 : id == 1 ? cy : cz;
+    const int coord = id == 0 ? ix : id == 1 ? iy : iz;
+    const int nmaxc = id == 0 ? g.nx : id == 1 ? g.ny : g.nz;
+    const double di = id == 0 ? 1. / g.dx : id == 1 ? 1. / g.dy : 1. / g.dz;
+    const double dm = dels[6 * t + 2 * id], dp = dels[6 * t + 2 * id + 1];
+    double vv0, dd0, vv1, dd1;
+    if (0. < dm && dm <= 1.) {
+      vv0 = volt[6 * t + 2 * id];
+      dd0 = dm;
+    } else {
+      vv0 = p0[-so];
+      dd0 = 1.;
+    }
+    if (0. < dp && dp <= 1.) {
+      vv1 = volt[6 * t + 2 * id + 1];
+      dd1 = dp;
+    } else {
+      vv1 = p0[so];
+      dd1 = 1.;
+    }
+    e0[3 * t + id] = (dd1 / (dd0 + dd1) * (vv0 - ppp) / dd0 + dd0 / (dd0 + dd1) * (ppp - vv1) / dd1) * di;
+    if (coord - 1 >= 0 && c0[-co] == kIcInterior)
+      ed[6 * t + 2 * id] = ((vv0 - ppp) / dd0 - (2. - dd0) / (2. + dd1) * (ppp - vv1) / dd1) *
+                           ((2. + dd1) / (dd1 + dd0)) * di;
+    if (coord + 1 <= nmaxc && c0[co] == kIcInterior)
+      ed[6 * t + 2 * id + 1] = ((ppp - vv1) / dd1 - (2. - dd1) / (2. + dd0) * (vv0 - ppp) / dd0) *
+                               ((2. + dd0) / (dd0 + dd1)) * di;
+  }
+}
+
+__device__ __forceinline__ double cond_e0(const CondE& ce, int ic, int id) {
+  return ic > 0 ? __ldg(ce.e0e + 3 * (ic - 1) + id) : __ldg(ce.e0o + 3 * (-ic - 1) + id);
+}
+__device__ __forceinline__ double cond_ed(const CondE& ce, int ic, int k) {
+  return ic > 0 ? __ldg(ce.ede + 6 * (ic - 1) + k) : __ldg(ce.edo + 6 * (-ic - 1) + k);
+}
+
+// GETEEFROME (f3d_mgrid.F:5160-5220): the cell edge from node a (phi at pa,
+// icgrid value ca) to node a+p (icgrid value cb); ps is the phi stride of p.
+__device__ __forceinline__ void cond_edge(const double* __restrict__ pa, int ps, int ca, int cb, const CondE& ce,
+                                          int id, double di, double wm, double wp, double& ee, double& ww) {
+  if (ca == 0) {
+    ee = ee + wm * (__ldg(pa - ps) - __ldg(pa + ps)) * 0.5 * di;
+    ww = ww + wm;
+  } else if (ca != kIcInterior) {
+    ee = ee + wm * cond_e0(ce, ca, id);
+    ww = ww + wm;
+    if (cb == kIcInterior) {
+      ee = ee + wp * cond_ed(ce, ca, 2 * id + 1);
+      ww = ww + wp;
+    }
+  }
+  if (cb == 0) {
+    ee = ee + wp * (__ldg(pa) - __ldg(pa + 2 * ps)) * 0.5 * di;
+    ww = ww + wp;
+  } else if (cb != kIcInterior) {
+    ee = ee + wp * cond_e0(ce, cb, id);
+    ww = ww + wp;
+    if (ca == kIcInterior) {
+      ee = ee + wm * cond_ed(ce, cb, 2 * id);
+      ww = ww + wm;
+    }
+  }
+}
+
+// sete3dwithconductor, efetch = 1 (f3d_mgrid.F:4774-5020). Returns false for
+// a particle outside the grid, which gets no field. All-vacuum cells use
+// centred differences with each term scaled by 1/(2 dx); other cells weight
+// the vacuum differences and the conductor points' fields per cell edge,
+// normalized by the weights used. A particle on an upper face uses the last
+// cell with fraction 1.
+__device__ inline bool gather_e_cond(const double* __restrict__ phi, const GridP& g, const CondE& ce, double x,
+                                     double y, double z, double& ext, double& eyt, double& ezt) {
+  const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
+  const double dxi = 1. / g.dx, dyi = 1. / g.dy, dzi = 1. / g.dz;
+  const double xi = (x - g.xmmin) * dxi, yj = (y - g.ymmin) * dyi, zk = (z - g.zgrid - g.zmmin) * dzi;
+  if (xi < 0. || xi > g.nx || yj < 0. || yj > g.ny || zk < 0. || zk > g.nz) return false;
+  int i, j, k;
+  double u1, v1, w1;
+  cellfrac(xi, g.nx, i, u1);
+  cellfrac(yj, g.ny, j, v1);
+  cellfrac(zk, g.nz, k, w1);
+  const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+  const int sy = g.nx + 3, sz = sy * (g.ny + 3);
+  const double* b = phi + ((i + 1) + sy * (j + 1) + sz * (k + 1));
+  auto P = [&](int a, int bb, int c) { return __ldg(b + (a + bb * sy + c * sz)); };
+  const int cy = g.nx + 1, cz = cy * (g.ny + 1);
+  const int* cb = ce.icg + ((size_t)i + (size_t)cy * j + (size_t)cz * k);
+  const int c000 = __ldg(cb), c100 = __ldg(cb + 1), c010 = __ldg(cb + cy), c110 = __ldg(cb + 1 + cy);
+  const int c001 = __ldg(cb + cz), c101 = __ldg(cb + 1 + cz), c011 = __ldg(cb + cy + cz),
+            c111 = __ldg(cb + 1 + cy + cz);
+  if ((c000 | c100 | c010 | c110 | c001 | c101 | c011 | c111) == 0) {
+    ext = u0 * v0 * w0 * (P(-1, 0, 0) - P(1, 0, 0)) * tdxi + u1 * v0 * w0 * (P(0, 0, 0) - P(2, 0, 0)) * tdxi +
+          u0 * v1 * w0 * (P(-1, 1, 0) - P(1, 1, 0)) * tdxi + u1 * v1 * w0 * (P(0, 1, 0) - P(2, 1, 0)) * tdxi +
+          u0 * v0 * w1 * (P(-1, 0, 1) - P(1, 0, 1)) * tdxi + u1 * v0 * w1 * (P(0, 0, 1) - P(2, 0, 1)) * tdxi +
+          u0 * v1 * w1 * (P(-1, 1, 1) - P(1, 1, 1)) * tdxi + u1 * v1 * w1 * (P(0, 1, 1) - P(2, 1, 1)) * tdxi;
+    eyt = u0 * v0 * w0 * (P(0, -1, 0) - P(0, 1, 0)) * tdyi + u1 * v0 * w0 * (P(1, -1, 0) - P(1, 1, 0)) * tdyi +
+          u0 * v1 * w0 * (P(0, 0, 0) - P(0, 2, 0)) * tdyi + u1 * v1 * w0 * (P(1, 0, 0) - P(1, 2, 0)) * tdyi +
+          u0 * v0 * w1 * (P(0, -1, 1) - P(0, 1, 1)) * tdyi + u1 * v0 * w1 * (P(1, -1, 1) - P(1, 1, 1)) * tdyi +
+          u0 * v1 * w1 * (P(0, 0, 1) - P(0, 2, 1)) * tdyi + u1 * v1 * w1 * (P(1, 0, 1) - P(1, 2, 1)) * tdyi;
+    ezt = u0 * v0 * w0 * (P(0, 0, -1) - P(0, 0, 1)) * tdzi + u1 * v0 * w0 * (P(1, 0, -1) - P(1, 0, 1)) * tdzi +
+          u0 * v1 * w0 * (P(0, 1, -1) - P(0, 1, 1)) * tdzi + u1 * v1 * w0 * (P(1, 1, -1) - P(1, 1, 1)) * tdzi +
+          u0 * v0 * w1 * (P(0, 0, 0) - P(0, 0, 2)) * tdzi + u1 * v0 * w1 * (P(1, 0, 0) - P(1, 0, 2)) * tdzi +
+          u0 * v1 * w1 * (P(0, 1, 0) - P(0, 1, 2)) * tdzi + u1 * v1 * w1 * (P(1, 1, 0) - P(1, 1, 2)) * tdzi;
+    return true;
+  }
+  double ee = 0., ww = 0.;
+  cond_edge(b, 1, c000, c100, ce, 0, dxi, u0 * v0 * w0, u1 * v0 * w0, ee, ww);
+  cond_edge(b + sy, 1, c010, c110, ce, 0, dxi, u0 * v1 * w0, u1 * v1 * w0, ee, ww);
+  cond_edge(b + sz, 1, c001, c101, ce, 0, dxi, u0 * v0 * w1, u1 * v0 * w1, ee, ww);
+  cond_edge(b + sy + sz, 1, c011, c111, ce, 0, dxi, u0 * v1 * w1, u1 * v1 * w1, ee, ww);
+  if (ww != 0.) ww = 1. / ww;
+  ext = ee * ww;
+  ee = 0.;
+  ww = 0.;
+  cond_edge(b, sy, c000, c010, ce, 1, dyi, u0 * v0 * w0, u0 * v1 * w0, ee, ww);
+  cond_edge(b + 1, sy, c100, c110, ce, 1, dyi, u1 * v0 * w0, u1 * v1 * w0, ee, ww);
+  cond_edge(b + sz, sy, c001, c011, ce, 1, dyi, u0 * v0 * w1, u0 * v1 * w1, ee, ww);
+  cond_edge(b + 1 + sz, sy, c101, c111, ce, 1, dyi, u1 * v0 * w1, u1 * v1 * w1, ee, ww);
+  if (ww != 0.) ww = 1. / ww;
+  eyt = ee * ww;
+  ee = 0.;
+  ww = 0.;
+  cond_edge(b, sz, c000, c001, ce, 2, dzi, u0 * v0 * w0, u0 * v0 * w1, ee, ww);
+  cond_edge(b + 1, sz, c100, c101, ce, 2, dzi, u1 * v0 * w0, u1 * v0 * w1, ee, ww);
+  cond_edge(b + sy, sz, c010, c011, ce, 2, dzi, u0 * v1 * w0, u0 * v1 * w1, ee, ww);
+  cond_edge(b + 1 + sy, sz, c110, c111, ce, 2, dzi, u1 * v1 * w0, u1 * v1 * w1, ee, ww);
+  if (ww != 0.) ww = 1. / ww;
+  ezt = ee * ww;
+  return true;
+}
+
+__global__ void k_fetch_e_cond(const double* __restrict__ phi, GridP g, CondE ce, const double* __restrict__ xp,
+                               const double* __restrict__ yp, const double* __restrict__ zp,
+                               double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez,
+                               int64_t np) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  double a, b, c;
+  if (!gather_e_cond(phi, g, ce, xp[i], yp[i], zp[i], a, b, c)) return;
+  ex[i] = ex[i] + a;
+  ey[i] = ey[i] + b;
+  ez[i] = ez[i] + c;
+}
+
 __global__ void k_fetch_e(const double* __restrict__ phi, GridP g, const double* __restrict__ xp,
                           const double* __restrict__ yp, const double* __restrict__ zp, double* __restrict__ ex,
                           double* __restrict__ ey, double* __restrict__ ez, int64_t np) {
@@ -333,8 +519,10 @@ struct PushP {
 // (0, dt/2), half-dt rotation, half E kick, drift. CENTER 2 is "synchv"
 // (w3d.F:2187-2310), velocities from t-dt/2 to t: window (-dt/2, 0), half E
 // kick, half-dt rotation; no drift and no boundaries.
-template <int CENTER>
-__global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ phi, GridP g, PushP P,
+// COND selects the conductor-corrected gather (lcorrectede), which leaves E
+// at 0 for a particle outside the grid.
+template <int CENTER, bool COND>
+__global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ phi, GridP g, PushP P, CondE ce,
                                                  double* __restrict__ xp, double* __restrict__ yp,
                                                  double* __restrict__ zp, double* __restrict__ uxp,
                                                  double* __restrict__ uyp, double* __restrict__ uzp,
@@ -345,7 +533,11 @@ __global__ void __launch_bounds__(256, 3) k_advance(const double* __restrict__ p
   if (gi == 0.) return;
   double x = xp[i], y = yp[i], z = zp[i], ux = uxp[i], uy = uyp[i], uz = uzp[i];
   double ex, ey, ez;
-  gather_e(phi, g, x, y, z, ex, ey, ez);
+  if (COND) {
+    if (!gather_e_cond(phi, g, ce, x, y, z, ex, ey, ez)) ex = ey = ez = 0.;
+  } else {
+    gather_e(phi, g, x, y, z, ex, ey, ez);
+  }
   // fetche3d zeroes E before the gather (w3d.F:11015): E = 0 + gathered
   ex = 0. + ex;
   ey = 0. + ey;
@@ -568,6 +760,54 @@ int finalize_rho(wg_ctx* c) {
   return WG_OK;
 }
 
+// lcorrectede setup before a corrected gather: rebuilds icgrid and the
+// per-point field arrays when the conductors changed, then recomputes
+// efield0/efieldd from the current phi (the reference does this after every
+// solve, multigrid.py:602-616). Nothing is computed unless both subgrid
+// lists (all levels) are non-empty, as in getefieldatconductorsubgrid; the
+// fields then stay 0.
+int prepare_correctede(wg_ctx* c, CondE* ce) {
+  Level& L = c->lv[0];
+  const LevelDims& d = L.d;
+  cudaStream_t s = c->stream;
+  const size_t nodes = (size_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+  if (c->icgrid_version != c->cond_version || !c->icgrid) {
+    if (!c->icgrid) WG_TRY_CUDA(cudaMalloc((void**)&c->icgrid, nodes * sizeof(int)));
+    for (int p = 0; p < 2; ++p) {
+      if (c->ef0[p]) cudaFree(c->ef0[p]);
+      if (c->efd[p]) cudaFree(c->efd[p]);
+      c->ef0[p] = c->efd[p] = nullptr;
+      const size_t n = (size_t)L.sub[p].n;
+      if (n) {
+        WG_TRY_CUDA(cudaMalloc((void**)&c->ef0[p], 3 * n * sizeof(double)));
+        WG_TRY_CUDA(cudaMalloc((void**)&c->efd[p], 6 * n * sizeof(double)));
+        WG_TRY_CUDA(cudaMemsetAsync(c->ef0[p], 0, 3 * n * sizeof(double), s));
+        WG_TRY_CUDA(cudaMemsetAsync(c->efd[p], 0, 6 * n * sizeof(double), s));
+      }
+    }
+    WG_TRY_CUDA(cudaMemsetAsync(c->icgrid, 0, nodes * sizeof(int), s));
+    if (L.n_int) { ++c->nlaunch; k_icgrid_fill<<<(L.n_int + 255) / 256, 256, 0, s>>>(L.int_ijk, L.n_int, 0, d.nx, d.ny, d.nz, c->icgrid); }
+    if (L.sub[0].n) { ++c->nlaunch; k_icgrid_fill<<<(L.sub[0].n + 255) / 256, 256, 0, s>>>(L.sub[0].ijk, L.sub[0].n, 1, d.nx, d.ny, d.nz, c->icgrid); }
+    if (L.sub[1].n) { ++c->nlaunch; k_icgrid_fill<<<(L.sub[1].n + 255) / 256, 256, 0, s>>>(L.sub[1].ijk, L.sub[1].n, -1, d.nx, d.ny, d.nz, c->icgrid); }
+    WG_TRY_CUDA(cudaGetLastError());
+    c->icgrid_version = c->cond_version;
+  }
+  if (!c->cond.even_indx.empty() && !c->cond.odd_indx.empty()) {
+    for (int p = 0; p < 2; ++p) {
+      const DevSubgrid& S = L.sub[p];
+      if (!S.n) continue;
+      { ++c->nlaunch; k_efield_sub<<<(S.n + 255) / 256, 256, 0, s>>>(L.phi, gridp(c), S.ijk, S.dels, S.volt, S.n, c->icgrid, c->ef0[p], c->efd[p]); }
+    }
+    WG_TRY_CUDA(cudaGetLastError());
+  }
+  ce->icg = c->icgrid;
+  ce->e0e = c->ef0[0];
+  ce->e0o = c->ef0[1];
+  ce->ede = c->efd[0];
+  ce->edo = c->efd[1];
+  return WG_OK;
+}
+
 int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double* ex, double* ey, double* ez,
             int64_t np) {
   if (np < 0 || (np > 0 && (!x || !y || !z || !ex || !ey || !ez))) {
@@ -575,6 +815,13 @@ int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double
     return WG_EINVAL;
   }
   if (np == 0) return WG_OK;
+  if (c->correctede) {
+    CondE ce{};
+    WG_TRY(prepare_correctede(c, &ce));
+    { ++c->nlaunch; k_fetch_e_cond<<<cdiv64(np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), ce, x, y, z, ex, ey, ez, np); }
+    WG_TRY_CUDA(cudaGetLastError());
+    return WG_OK;
+  }
   { ++c->nlaunch; k_fetch_e<<<cdiv64(np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), x, y, z, ex, ey, ez, np); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
@@ -597,9 +844,16 @@ int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
   if (p->np == 0) return WG_OK;
   PushP P{p->q, p->m, prm->dt, c->grid.zmmin, c->grid.zmmax, prm->prwall, prm->prwallx, prm->prwally,
           prm->use_lattice ? c->czs : nullptr, c->cze, c->cdb, c->nzl, c->zlmin, c->dzl};
-  auto kern = prm->center == WG_CENTER_HALFV ? k_advance<1> : prm->center == WG_CENTER_SYNCHV ? k_advance<2>
-                                                                                               : k_advance<0>;
-  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, p->x, p->y, p->z, p->ux, p->uy,
+  CondE ce{};
+  if (c->correctede) WG_TRY(prepare_correctede(c, &ce));
+  auto kern = c->correctede
+                  ? (prm->center == WG_CENTER_HALFV    ? k_advance<1, true>
+                     : prm->center == WG_CENTER_SYNCHV ? k_advance<2, true>
+                                                       : k_advance<0, true>)
+                  : (prm->center == WG_CENTER_HALFV    ? k_advance<1, false>
+                     : prm->center == WG_CENTER_SYNCHV ? k_advance<2, false>
+                                                       : k_advance<0, false>);
+  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, ce, p->x, p->y, p->z, p->ux, p->uy,
                                                   p->uz, p->gaminv, p->np); c->prof_end(pe); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;

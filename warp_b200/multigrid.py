@@ -88,6 +88,7 @@ class MultiGridB200(FieldSolver):
         self._phi = _device_view(pphi.value, (self.nx + 3, self.ny + 3, self.nz + 3), self.device)
         self._rho = _device_view(prho.value, (self.nx + 1, self.ny + 1, self.nz + 1), self.device)
         self._lattice = None
+        self._lcorrectede = False
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -115,6 +116,19 @@ class MultiGridB200(FieldSolver):
     @rho.setter
     def rho(self, value):
         self._rho.copy_(torch.as_tensor(value, dtype=torch.float64, device=self.device))
+
+    @property
+    def lcorrectede(self):
+        """f3d.lcorrectede (f3d.v:152): when True, fetche and advance gather E
+        next to conductors from the subgrid data (sete3dwithconductor,
+        f3d_mgrid.F:4774-5220) instead of plain centred differences, and
+        particles outside the grid get no field. Default False."""
+        return self._lcorrectede
+
+    @lcorrectede.setter
+    def lcorrectede(self, on):
+        _lib.check(_lib.lib.wg_set_correctede(self._h, int(bool(on))))
+        self._lcorrectede = bool(on)
 
     def getphi(self):
         """Host copy of phi on the nodes 0..nx, 0..ny, 0..nz (getphi)."""
@@ -289,6 +303,8 @@ class MultiGridB200(FieldSolver):
         """fetche -> fetchfieldfrompositions -> sete3d (multigrid.py:521-558,
         w3d.F:3963): E at the particles, written to pgroup.ex/ey/ez."""
         self._bind_stream()
+        if self._lcorrectede:
+            self.getconductorobject()
         groups = self.pgroups if pgroup is None else [pgroup]
         for pg in groups:
             pg.ex.zero_()
@@ -305,6 +321,8 @@ class MultiGridB200(FieldSolver):
         fetchfieldfrompositions (multigrid.py:521-558) makes. Positions are
         copied in, the gather runs on the device, the fields are copied out."""
         self._bind_stream()
+        if self._lcorrectede:
+            self.getconductorobject()
         pos = [torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(self.device) for a in (x, y, z)]
         n = int(pos[0].shape[0])
         e = torch.zeros((3, n), dtype=torch.float64, device=self.device)
@@ -340,6 +358,8 @@ class MultiGridB200(FieldSolver):
         if center not in _lib.CENTERS:
             raise ValueError("center must be one of %s" % sorted(_lib.CENTERS))
         self._bind_stream()
+        if self._lcorrectede:
+            self.getconductorobject()
         s = pgroup.cstruct(start, stop)
         p = _lib.PushParams(float(dt), float(prwall), float(prwallx), float(prwally),
                             int(self._lattice is not None), _lib.CENTERS[center])
