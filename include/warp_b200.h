@@ -55,6 +55,11 @@ typedef struct {
   int tolkind;     /* 0: mgerror = max|dphi| in volts (reference criterion)
                       1: relative residual max|rhs-A phi|/max|rhs| */
   int flags;       /* WG_SOLVE_* bits below */
+  int mgmaxvcycles; /* > 0: full multigrid (fullmultigrid3dsolve,
+                       f3d_mgrid.F:502-945; FullMultiGrid3D default 2): the
+                       coarse levels, solved first from the restricted rho
+                       with this many V-cycles each, give the starting phi
+                       (the warm start is not used); 0: multigrid3dsolve */
 } wg_solve_opts;
 
 #define WG_SOLVE_GRAPH 1  /* replay each V-cycle from a captured CUDA graph */

@@ -870,8 +870,14 @@ void residual3d(int nx, int ny, int nz, double dxsqi, double dysqi, double dzsqi
 }
 
 // restrict3d, f3d_mgrid.F:1593-1775 (serial: offsets 0, nguardres = 1)
+// The source has `ng` guard cells (1 for the V-cycle's residual, 0 for rho
+// in the full multigrid) and is passed in the padded layout. Windows are
+// clipped to the guard; the weights stay indexed from the unclipped window
+// start, as the reference's precalculated wxa/wya/wza are, so a window
+// clipped at its low end takes the weights of the taps below it. (With
+// ng = 1 and coarsening ratios up to 2 no window is clipped.)
 void restrict3d(int nx, int ny, int nz, const double* res, int nxc, int nyc, int nzc, double* rhoc, double ff,
-                const int* lbc) {
+                const int* lbc, int ng = 1) {
   int ixcmin = 0, ixcmax = nxc, iycmin = 0, iycmax = nyc, izcmin = 0, izcmax = nzc;
   if (lbc[0] == 0) ixcmin = 1;
   if (lbc[1] == 0) ixcmax = nxc - 1;
@@ -881,11 +887,11 @@ void restrict3d(int nx, int ny, int nz, const double* res, int nxc, int nyc, int
   if (lbc[5] == 0) izcmax = nzc - 1;
   double dxi = 1. * nxc / nx, dyi = 1. * nyc / ny, dzi = 1. * nzc / nz;
   std::fill(rhoc, rhoc + (size_t)(nxc + 1) * (nyc + 1) * (nzc + 1), 0.);
-  auto lim = [](int ic, int n, int nc, int& lo, int& hi, int& lo0) {
+  auto lim = [ng](int ic, int n, int nc, int& lo, int& hi, int& lo0) {
     lo0 = ((ic - 1) * n + 4 * nc) / nc - 3;
     hi = ((ic + 1) * n - 1) / nc;
-    lo = std::max(lo0, -1);
-    hi = std::min(hi, n + 1);
+    lo = std::max(lo0, -ng);
+    hi = std::min(hi, n + ng);
   };
   par_for(izcmin, izcmax + 1, [&](int64_t izc64) {
     const int izc = (int)izc64;
@@ -899,11 +905,11 @@ void restrict3d(int nx, int ny, int nz, const double* res, int nxc, int nyc, int
         lim(ixc, nx, nxc, ixmin, ixmax, ix0);
         double r = 0., w = 0.;
         for (int iz = izmin; iz <= izmax; ++iz) {
-          double wz = 1. - std::fabs(izc - (iz + 0.) * dzi);
+          double wz = 1. - std::fabs(izc - (iz0 + (iz - izmin) + 0.) * dzi);
           for (int iy = iymin; iy <= iymax; ++iy) {
-            double wy = 1. - std::fabs(iyc - (iy + 0.) * dyi);
+            double wy = 1. - std::fabs(iyc - (iy0 + (iy - iymin) + 0.) * dyi);
             for (int ix = ixmin; ix <= ixmax; ++ix) {
-              double wx = 1. - std::fabs(ixc - (ix + 0.) * dxi);
+              double wx = 1. - std::fabs(ixc - (ix0 + (ix - ixmin) + 0.) * dxi);
               r = r + wx * wy * wz * res[pidx(nx, ny, ix, iy, iz)];
               w = w + wx * wy * wz;
             }
@@ -974,6 +980,38 @@ void vcycle(int mglevel, const std::vector<Level>& lv, double* phi, const double
     applybc(nx, ny, nz, 1, phi, bounds, false, false);
   }
   for (int i = 0; i < P.uppasses; ++i) sorpass3d(mglevel, nx, ny, nz, phi, rho, dxsqi, dysqi, dzsqi, bounds, P, C);
+}
+
+// fullmultigrid3dsolve below the finest level (f3d_mgrid.F:502-945): rho is
+// this level's source (already scaled), phi its potential. Coarser levels are
+// solved first from the restricted rho (ghost width 0), their phi expanded
+// into a zeroed phi here; a coarse level then does mgmaxvcycles V-cycles
+// without a convergence test. Level 0 stops after the expansion: the caller
+// iterates it to convergence.
+void fmg_level(int mglevel, const std::vector<Level>& lv, double* phi, const double* rho, const int* bounds,
+               const MGParams& P, Conductors& C, int mgmaxvcycles) {
+  const Level& L = lv[mglevel];
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  if (nx >= 4 && ny >= 4 && nz >= 4 && mglevel < P.mgmaxlevels && mglevel + 1 < (int)lv.size()) {
+    const Level& Lc = lv[mglevel + 1];
+    double dxsqi = 1. / (L.dx * L.dx), dysqi = 1. / (L.dy * L.dy), dzsqi = 1. / (L.dz * L.dz);
+    double dxcsqi = 1. / (Lc.dx * Lc.dx), dycsqi = 1. / (Lc.dy * Lc.dy), dzcsqi = 1. / (Lc.dz * Lc.dz);
+    double ff = (dxsqi + dysqi + dzsqi) / (dxcsqi + dycsqi + dzcsqi);
+    std::vector<double> rpad((size_t)(nx + 3) * (ny + 3) * (nz + 3), 0.);
+    for (int iz = 0; iz <= nz; ++iz)
+      for (int iy = 0; iy <= ny; ++iy)
+        for (int ix = 0; ix <= nx; ++ix) rpad[pidx(nx, ny, ix, iy, iz)] = rho[ridx(nx, ny, ix, iy, iz)];
+    std::vector<double> rhoc((size_t)(Lc.nx + 1) * (Lc.ny + 1) * (Lc.nz + 1), 0.);
+    restrict3d(nx, ny, nz, rpad.data(), Lc.nx, Lc.ny, Lc.nz, rhoc.data(), ff, bounds, 0);
+    std::vector<double> phic((size_t)(Lc.nx + 3) * (Lc.ny + 3) * (Lc.nz + 3), 0.);
+    fmg_level(mglevel + 1, lv, phic.data(), rhoc.data(), bounds, P, C, mgmaxvcycles);
+    std::fill(phi, phi + (size_t)(nx + 3) * (ny + 3) * (nz + 3), 0.);
+    expand3d(nx, ny, nz, phi, Lc.nx, Lc.ny, Lc.nz, phic.data(), bounds);
+  }
+  applybc(nx, ny, nz, 1, phi, bounds, false, false);
+  if (mglevel == 0) return;
+  for (int it = 0; it < mgmaxvcycles; ++it) vcycle(mglevel, lv, phi, rho, bounds, P, C);
+  applybc(nx, ny, nz, 1, phi, bounds, true, false);
 }
 
 }  // namespace
@@ -1074,10 +1112,13 @@ void or_cond_export(or_conductors* c, int which, int* indx, double* dels, double
 // coefficients; mgform 1 or 2). phi is (nx+3)(ny+3)(nz+3) with guards, rho is
 // (nx+1)(ny+1)(nz+1). rho is not modified (the reference scales it in place
 // and unscales it afterwards). cond may be NULL.
+// multigrid3dsolve (f3d_mgrid.F:83-500), or with mgmaxvcycles > 0 the full
+// multigrid fullmultigrid3dsolve (:502-945, mgform 1 only): the coarse
+// levels give the starting phi, then level 0 iterates as multigrid3dsolve.
 int or_mgsolve(int nx, int ny, int nz, double dx, double dy, double dz, const int* bounds, double* phi,
                const double* rho, or_conductors* cond, double mgparam, double mgtol, int mgmaxiters,
                int mgmaxlevels, int downpasses, int uppasses, int mgform, int lcndbndy, int* mgiters_out,
-               double* mgerror_out) {
+               double* mgerror_out, int mgmaxvcycles) {
   Conductors empty;
   Conductors* C = cond ? reinterpret_cast<Conductors*>(cond) : &empty;
   std::vector<Level> lv = mglevels(nx, ny, nz, dx, dy, dz);
@@ -1097,7 +1138,12 @@ int or_mgsolve(int nx, int ny, int nz, double dx, double dy, double dz, const in
   const size_t np = (size_t)(nx + 3) * (ny + 3) * (nz + 3);
   std::vector<double> rhs(nr);
   for (size_t i = 0; i < nr; ++i) rhs[i] = rho[i] * reps0c;
-  applybc(nx, ny, nz, 1, phi, bounds, false, false);
+  if (mgmaxvcycles > 0) {
+    if (mgform != 1) return -4;
+    fmg_level(0, lv, phi, rhs.data(), bounds, P, *C, mgmaxvcycles);
+  } else {
+    applybc(nx, ny, nz, 1, phi, bounds, false, false);
+  }
   std::vector<double> rhosave, res;
   if (mgform == 2) { rhosave = rhs; res.resize(np); }
   std::vector<double> phisave(np);

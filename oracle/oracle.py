@@ -47,7 +47,7 @@ def lib():
         L.or_cond_export.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _dp, _dp, _ip]
         L.or_mgsolve.restype = ctypes.c_int
         L.or_mgsolve.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [_ip, _dp, _dp, ctypes.c_void_p,
-                                 ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 6 + [_ip, _dp]
+                                 ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 6 + [_ip, _dp, ctypes.c_int]
         L.or_relresidual.restype = ctypes.c_double
         L.or_relresidual.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [_ip, _dp, _dp, ctypes.c_void_p,
                                      ctypes.c_double]
@@ -158,8 +158,10 @@ class Conductors:
 
 
 def mgsolve(phi, rho, dx, dy, dz, bounds, conductors=None, mgparam=1.2, mgtol=1e-6, mgmaxiters=100,
-            mgmaxlevels=101, downpasses=1, uppasses=1, mgform=1, lcndbndy=True):
-    """multigrid3dsolve on the CPU; phi updated in place. Returns (iters, err)."""
+            mgmaxlevels=101, downpasses=1, uppasses=1, mgform=1, lcndbndy=True, mgmaxvcycles=0):
+    """multigrid3dsolve on the CPU; phi updated in place. Returns (iters, err).
+    mgmaxvcycles > 0 selects fullmultigrid3dsolve with that many V-cycles
+    per coarse level (FullMultiGrid3D's default is 2)."""
     nx, ny, nz = rho.shape[0] - 1, rho.shape[1] - 1, rho.shape[2] - 1
     assert phi.shape == (nx + 3, ny + 3, nz + 3) and phi.flags.f_contiguous and rho.flags.f_contiguous
     b = np.ascontiguousarray(bounds, np.int32)
@@ -168,7 +170,7 @@ def mgsolve(phi, rho, dx, dy, dz, bounds, conductors=None, mgparam=1.2, mgtol=1e
     rc = lib().or_mgsolve(nx, ny, nz, dx, dy, dz, _i(b), _d(phi), _d(rho),
                           conductors.h if conductors is not None else None, mgparam, mgtol, mgmaxiters,
                           mgmaxlevels, downpasses, uppasses, mgform, int(lcndbndy), ctypes.byref(it),
-                          ctypes.byref(err))
+                          ctypes.byref(err), int(mgmaxvcycles))
     if rc != 0:
         raise RuntimeError("oracle mgsolve failed: %d" % rc)
     return it.value, err.value

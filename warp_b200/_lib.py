@@ -33,7 +33,7 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("mgparam", ctypes.c_double), ("mgtol", ctypes.c_double), ("mgmaxiters", ctypes.c_int),
                 ("mgmaxlevels", ctypes.c_int), ("downpasses", ctypes.c_int), ("uppasses", ctypes.c_int),
                 ("lcndbndy", ctypes.c_int), ("precision", ctypes.c_int), ("tolkind", ctypes.c_int),
-                ("flags", ctypes.c_int)]
+                ("flags", ctypes.c_int), ("mgmaxvcycles", ctypes.c_int)]
 
 
 SOLVE_GRAPH, SOLVE_FUSED = 1, 2

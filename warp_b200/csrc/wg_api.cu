@@ -117,19 +117,26 @@ int expand_tables(Level& L, const LevelDims& dc) {
 
 // Window and weight tables of restrict3d (f3d_mgrid.F:1593-1775) from level
 // L into coarse level dc, with the reference's per-node expressions.
-int restrict_tables(Level& L, const LevelDims& dc) {
-  const int n[3] = {L.d.nx, L.d.ny, L.d.nz}, nc[3] = {dc.nx, dc.ny, dc.nz};
+// Index and weight tables of restrict3d (f3d_mgrid.F:1593-1775) from level L
+// into coarse level dc, for a source with ng guard cells: ng = 1 for the
+// V-cycle's residual, ng = 0 for rho in the full multigrid. A window clipped
+// at its low end keeps the weights indexed from its unclipped start, as the
+// reference's precalculated wxa/wya/wza are.
+int restrict_tables_ng(const LevelDims& d, const LevelDims& dc, int ng, int32_t** dlo, int32_t** dn, double** dw,
+                       int* rmax) {
+  const int n[3] = {d.nx, d.ny, d.nz}, nc[3] = {dc.nx, dc.ny, dc.nz};
   const size_t tot = (size_t)(nc[0] + 1) + (nc[1] + 1) + (nc[2] + 1);
   std::vector<int32_t> lo(tot), cnt(tot);
   std::vector<double> w(tot * kRestrictTaps, 0.);
   size_t o = 0;
+  *rmax = 0;
   for (int a = 0; a < 3; ++a) {
     const double dci = 1. * nc[a] / n[a];
     for (int ic = 0; ic <= nc[a]; ++ic, ++o) {
-      int l = ((ic - 1) * n[a] + 4 * nc[a]) / nc[a] - 3;
+      const int l0 = ((ic - 1) * n[a] + 4 * nc[a]) / nc[a] - 3;
       int h = ((ic + 1) * n[a] - 1) / nc[a];
-      l = std::max(l, -1);
-      h = std::min(h, n[a] + 1);
+      const int l = std::max(l0, -ng);
+      h = std::min(h, n[a] + ng);
       const int k = std::max(0, h - l + 1);
       if (k > kRestrictTaps) {
         set_error("wg_create: restriction window wider than 4 fine cells (coarsening ratio above 2)");
@@ -137,17 +144,22 @@ int restrict_tables(Level& L, const LevelDims& dc) {
       }
       lo[o] = l;
       cnt[o] = k;
-      if (a < 2) L.rmax = std::max(L.rmax, k);
-      for (int t = 0; t < k; ++t) w[o * kRestrictTaps + t] = 1. - std::fabs(ic - (l + t + 0.) * dci);
+      if (a < 2) *rmax = std::max(*rmax, k);
+      for (int t = 0; t < k; ++t) w[o * kRestrictTaps + t] = 1. - std::fabs(ic - (l0 + t + 0.) * dci);
     }
   }
-  WG_TRY(dalloc(&L.rlo, tot));
-  WG_TRY(dalloc(&L.rn, tot));
-  WG_TRY(dalloc(&L.rw, tot * kRestrictTaps));
-  WG_TRY_CUDA(cudaMemcpy(L.rlo, lo.data(), tot * sizeof(int32_t), cudaMemcpyHostToDevice));
-  WG_TRY_CUDA(cudaMemcpy(L.rn, cnt.data(), tot * sizeof(int32_t), cudaMemcpyHostToDevice));
-  WG_TRY_CUDA(cudaMemcpy(L.rw, w.data(), tot * kRestrictTaps * sizeof(double), cudaMemcpyHostToDevice));
+  WG_TRY(dalloc(dlo, tot));
+  WG_TRY(dalloc(dn, tot));
+  WG_TRY(dalloc(dw, tot * kRestrictTaps));
+  WG_TRY_CUDA(cudaMemcpy(*dlo, lo.data(), tot * sizeof(int32_t), cudaMemcpyHostToDevice));
+  WG_TRY_CUDA(cudaMemcpy(*dn, cnt.data(), tot * sizeof(int32_t), cudaMemcpyHostToDevice));
+  WG_TRY_CUDA(cudaMemcpy(*dw, w.data(), tot * kRestrictTaps * sizeof(double), cudaMemcpyHostToDevice));
   return WG_OK;
+}
+
+int restrict_tables(Level& L, const LevelDims& dc) {
+  WG_TRY(restrict_tables_ng(L.d, dc, 1, &L.rlo, &L.rn, &L.rw, &L.rmax));
+  return restrict_tables_ng(L.d, dc, 0, &L.rlo0, &L.rn0, &L.rw0, &L.rmax0);
 }
 
 void free_graphs(wg_ctx* c) {
@@ -179,6 +191,9 @@ void free_all(wg_ctx* c) {
     dfree(L.rlo);
     dfree(L.rn);
     dfree(L.rw);
+    dfree(L.rlo0);
+    dfree(L.rn0);
+    dfree(L.rw0);
   }
   dfree(c->phisave);
   dfree(c->rho);

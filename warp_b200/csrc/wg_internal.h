@@ -92,6 +92,11 @@ struct Level {
   int32_t* rn = nullptr;
   double* rw = nullptr;
   int rmax = 0;  // widest x or y window
+  // the same for a source without guard cells (rho in the full multigrid)
+  int32_t* rlo0 = nullptr;
+  int32_t* rn0 = nullptr;
+  double* rw0 = nullptr;
+  int rmax0 = 0;
 };
 
 constexpr int kRestrictTaps = 4;

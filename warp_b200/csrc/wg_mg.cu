@@ -919,6 +919,15 @@ __global__ void k_maxdiff(const double* __restrict__ a, const double* __restrict
 }
 
 // rhs = rho * reps0c (f3d_mgrid.F:223) and max|rhs|; flags a non-finite rho.
+// rhs (node layout) into the interior of a padded array: the source of the
+// full multigrid's restriction of rho, whose windows stay inside 0..n.
+__global__ void k_pad_copy(const double* __restrict__ src, double* __restrict__ dst, int nx, int ny) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y, iz = blockIdx.z;
+  if (ix > nx || iy > ny) return;
+  dst[(size_t)(ix + 1) + (size_t)(nx + 3) * ((size_t)(iy + 1) + (size_t)(ny + 3) * (iz + 1))] =
+      src[(size_t)ix + (size_t)(nx + 1) * ((size_t)iy + (size_t)(ny + 1) * iz)];
+}
+
 __global__ void k_scale_rhs(const double* __restrict__ rho, double* __restrict__ rhs, size_t n, double s,
                             unsigned long long* maxout, unsigned long long* flag) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1220,23 +1229,98 @@ struct Solver {
       int pc = (l == 0) ? prof_begin(0, WG_PROF_COARSE, (double)Lc.nr) : -1;
       vcycle<T>(l + 1, false);
       c->prof_end(pc);
-      Ranges R = ranges(d, B.b, false);
-      constexpr int zpt = ZPlanes<T>::value;
-      dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), cdiv(R.izmax - R.izmin + 1, zpt));
-      if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin) {
-        ++c->nlaunch;
-        int pe = prof_begin(l, WG_PROF_EXPAND0, (double)L.nr);
-        if (dc.nz == d.nz)
-          k_expand<T, zpt, false><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
-                                                       R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
-        else
-          k_expand<T, zpt, true><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
-                                                      R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
-        c->prof_end(pe);
-      }
+      expand<T>(l);
       bc<T>(L, Arr<T>::phi(L), false);
     }
     for (int i = 0; i < o->uppasses; ++i) sorpass<T>(l, usev);
+  }
+
+  // expand3d (f3d_mgrid.F:1777-1947): adds level l+1's phi, interpolated,
+  // to level l's phi
+  template <typename T>
+  void expand(int l) {
+    Level& L = c->lv[l];
+    Level& Lc = c->lv[l + 1];
+    const LevelDims& d = L.d;
+    const LevelDims& dc = Lc.d;
+    Ranges R = ranges(d, B.b, false);
+    constexpr int zpt = ZPlanes<T>::value;
+    dim3 blk(32, 8);
+    dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), cdiv(R.izmax - R.izmin + 1, zpt));
+    if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin) {
+      ++c->nlaunch;
+      int pe = prof_begin(l, WG_PROF_EXPAND0, (double)L.nr);
+      if (dc.nz == d.nz)
+        k_expand<T, zpt, false><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
+                                                     R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
+      else
+        k_expand<T, zpt, true><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
+                                                    R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
+      c->prof_end(pe);
+    }
+  }
+
+  // The deepest level the recursion of vcycle and fullmultigrid3dsolve
+  // reaches from level 0.
+  int deepest() const {
+    int l = 0;
+    for (;;) {
+      const LevelDims& d = c->lv[l].d;
+      if (d.nx >= 4 && d.ny >= 4 && d.nz >= 4 && l < o->mgmaxlevels && l + 1 < (int)c->lv.size())
+        ++l;
+      else
+        return l;
+    }
+  }
+
+  // fullmultigrid3dsolve (f3d_mgrid.F:502-945), downward part: the source of
+  // every level down to lmax, restricted from the scaled rho of level 0
+  // (rho has no guard cells there, hence the ng = 0 tables).
+  void fmg_restrict(int lmax) {
+    for (int l = 0; l < lmax; ++l) {
+      Level& L = c->lv[l];
+      Level& Lc = c->lv[l + 1];
+      const LevelDims& d = L.d;
+      const LevelDims& dc = Lc.d;
+      dim3 blk(32, 8);
+      { ++c->nlaunch; k_pad_copy<<<dim3(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1), blk, 0, s>>>(L.rhs, L.res, d.nx, d.ny); }
+      double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
+      double dxcsqi = 1. / (dc.dx * dc.dx), dycsqi = 1. / (dc.dy * dc.dy), dzcsqi = 1. / (dc.dz * dc.dz);
+      double ff = (dxsqi + dysqi + dzsqi) / (dxcsqi + dycsqi + dzcsqi);
+      Ranges Rc = ranges(dc, B.b, false);
+      dim3 grd(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), dc.nz + 1);
+      ++c->nlaunch;
+      if (L.rmax0 <= 3)
+        k_restrict<double, 3><<<grd, blk, 0, s>>>(L.res, Lc.rhs, d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin, Rc.ixmax,
+                                                  Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax, L.rlo0, L.rn0, L.rw0, ff);
+      else
+        k_restrict<double, kRestrictTaps><<<grd, blk, 0, s>>>(L.res, Lc.rhs, d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin,
+                                                              Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
+                                                              L.rlo0, L.rn0, L.rw0, ff);
+    }
+  }
+
+  // Upward part: from the coarsest level (phi = 0) to level 1, each level's
+  // phi is the expanded phi of the next coarser one followed by nvc
+  // V-cycles without a convergence test (voltages zero below level 0, as in
+  // every V-cycle); level 0 gets the expansion only. With a single level
+  // phi is left as it is.
+  int fmg_up(int lmax, int nvc) {
+    for (int l = lmax; l >= 0; --l) {
+      Level& L = c->lv[l];
+      if (l < lmax) {
+        WG_TRY_CUDA(cudaMemsetAsync(L.phi, 0, L.np * sizeof(double), s));
+        expand<double>(l);
+      } else if (l > 0) {
+        WG_TRY_CUDA(cudaMemsetAsync(L.phi, 0, L.np * sizeof(double), s));
+      }
+      bc<double>(L, L.phi, false);
+      if (l == 0) break;
+      box<double>(l);
+      for (int it = 0; it < nvc; ++it) vcycle<double>(l, false);
+      bc<double>(L, L.phi, true);
+    }
+    return WG_OK;
   }
 
   // reduction slot area of quantity q: 0 max|dphi|, 1 max|res|, 2 max|rhs|
@@ -1322,7 +1406,7 @@ int ensure_fp32(wg_ctx* c);
 int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   if (!o || !st) { set_error("wg_solve: null options or stats"); return WG_EINVAL; }
   if (!(o->mgparam > 0. && o->mgparam < 2.) || o->mgmaxiters < 0 || o->downpasses < 0 || o->uppasses < 0 ||
-      (o->precision != 0 && o->precision != 1) || (o->tolkind != 0 && o->tolkind != 1)) {
+      (o->precision != 0 && o->precision != 1) || (o->tolkind != 0 && o->tolkind != 1) || o->mgmaxvcycles < 0) {
     set_error("wg_solve: invalid options");
     return WG_EINVAL;
   }
@@ -1347,6 +1431,9 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
   WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
   { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
+  const bool fmg = o->mgmaxvcycles > 0;
+  const int lmax = fmg ? S.deepest() : 0;
+  if (fmg) S.fmg_restrict(lmax);
   S.box<double>(0);
   S.bc<double>(L0, L0.phi, false);
   dim3 blk(32, 8), grdn(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1);
@@ -1359,6 +1446,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
     set_error("wg_solve: rho contains NaN or Inf");
     return WG_EINVAL;
   }
+  if (fmg) WG_TRY(S.fmg_up(lmax, o->mgmaxvcycles));
   if (o->precision == 0) {
     for (;;) {
       if (o->tolkind == 1) {

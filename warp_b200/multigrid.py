@@ -249,7 +249,7 @@ class MultiGridB200(FieldSolver):
         flags = (_lib.SOLVE_GRAPH if self.use_graphs else 0) | (_lib.SOLVE_FUSED if self.fused_sweep else 0)
         return _lib.SolveOpts(self.mgparam, self.mgtol, self.mgmaxiters, self.mgmaxlevels, self.downpasses,
                               self.uppasses, int(self.lcndbndy), _PRECISION[self.precision],
-                              _TOLKIND[self.tolkind], flags)
+                              _TOLKIND[self.tolkind], flags, int(getattr(self, "mgmaxvcycles", 0)))
 
     def solve(self, iwhich=0):
         """dosolve -> multigrid3dsolve (multigrid.py:846-917,
@@ -377,3 +377,21 @@ class MultiGridB200(FieldSolver):
 
 
 MultiGrid3D = MultiGridB200
+
+
+class FullMultiGridB200(MultiGridB200):
+    """FullMultiGrid3D (scripts/multigrid.py:957-1020): each solve is a full
+    multigrid (fullmultigrid3dsolve, f3d_mgrid.F:502-945). The source is
+    restricted to every level, the coarsest level is solved first, and each
+    finer level starts from the expanded coarse phi and does mgmaxvcycles
+    V-cycles (default 2); the finest level then iterates to mgtol as
+    MultiGrid3D does. The previous phi is not used as a starting point."""
+
+    def __init__(self, *args, mgmaxvcycles=2, **kw):
+        if int(mgmaxvcycles) < 1:
+            raise ValueError("mgmaxvcycles must be at least 1")
+        self.mgmaxvcycles = int(mgmaxvcycles)
+        super().__init__(*args, **kw)
+
+
+FullMultiGrid3D = FullMultiGridB200
