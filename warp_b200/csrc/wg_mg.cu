@@ -126,8 +126,24 @@ __device__ inline void block_max_to(unsigned long long* base, double v) {
 }
 
 // out[q] = max over the slots of reduction q (q < nq).
+// Programmatic dependent launch: wait until the grid this one depends on
+// has finished and its writes are visible, then let the next grid of the
+// stream be scheduled, so that its launch overlaps this grid's run. Both are
+// no-ops for a grid launched without the attribute.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename T>
+__global__ void k_zero(T* __restrict__ u, size_t n) {
+  pdl_entry();
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) u[i] = (T)0.;
+}
+
 __global__ void k_fold_max(const unsigned long long* __restrict__ slots, unsigned long long* __restrict__ out,
                            int nq) {
+  pdl_entry();
   const int q = threadIdx.x / 32, lane = threadIdx.x & 31;
   if (q >= nq) return;
   unsigned long long v = slots[q * kRedQ + kRedStride * lane];
@@ -144,6 +160,7 @@ __global__ void k_fold_max(const unsigned long long* __restrict__ slots, unsigne
 // phase over all x and y, exactly as the reference orders them.
 template <typename T>
 __global__ void k_bc_xy(T* __restrict__ u, int nx, int ny, Bnd B, int lwithdirichlet) {
+  pdl_entry();
   const int iz = blockIdx.x;
   const size_t sy = nx + 3;
   const size_t base = (size_t)(ny + 3) * sy * (size_t)(iz + 1);
@@ -181,6 +198,7 @@ __global__ void k_bc_xy(T* __restrict__ u, int nx, int ny, Bnd B, int lwithdiric
 
 template <typename T>
 __global__ void k_bc_z(T* __restrict__ u, int nx, int ny, int nz, Bnd B, int lwithdirichlet) {
+  pdl_entry();
   const size_t nxy = (size_t)(nx + 3) * (ny + 3);
   size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nxy) return;
@@ -311,6 +329,7 @@ __device__ __noinline__ T subgrid_value(const CondArgs<T>& C, int par, int i, T 
 template <typename T>
 __global__ void k_box(T* __restrict__ rhs, int nx, int ny, CondArgs<T> C, T* __restrict__ srhs0,
                       T* __restrict__ srhs1) {
+  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < C.nint) {
     rhs[rix(nx, ny, C.iijk[3 * i], C.iijk[3 * i + 1], C.iijk[3 * i + 2])] = Box<T>::make(true, (uint32_t)i);
@@ -379,6 +398,7 @@ __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* 
                                                   int ixmin, int ixmax, int iymin, int iymax, int izmin, int izmax,
                                                   int parity, T cx, T cy, T cz, T spm1, int nz, int wtz, int nbz,
                                                   CondArgs<T> C, Bnd B, SorCoef sc, int voltfac_on, int lcndbndy) {
+  pdl_entry();
   // the first nspz z-slices of blocks update the subgrid conductor points
   // of this colour (condbndymg); they read only nodes of the other colour
   // too, and go first so that their dependent loads overlap the bulk blocks
@@ -433,6 +453,7 @@ __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* 
 template <typename T>
 __global__ void k_special_sor(T* __restrict__ phi, int nx, int ny, int nz, CondArgs<T> C, int par, Bnd B, SorCoef c,
                               int voltfac_on, int usev, int lcndbndy) {
+  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nsub = par ? C.nsub[1] : C.nsub[0];
   if (i < nsub) {
@@ -447,6 +468,7 @@ __global__ void k_special_sor(T* __restrict__ phi, int nx, int ny, int nz, CondA
 template <typename T>
 __global__ void k_interior(T* __restrict__ phi, int nx, int ny, const int32_t* __restrict__ iijk,
                            const double* __restrict__ ivolt, int nint, int usev, int nz = 0, int wtz = 0) {
+  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nint) return;
   const int ix = iijk[3 * i], iy = iijk[3 * i + 1], iz = iijk[3 * i + 2];
@@ -460,6 +482,7 @@ __global__ void k_interior(T* __restrict__ phi, int nx, int ny, const int32_t* _
 template <typename T>
 __global__ void k_condbndymgint(T* __restrict__ phi, int nx, int ny, int nz, const int32_t* __restrict__ ijk,
                                 const double* __restrict__ dels, int n, Bnd B) {
+  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int ix = ijk[3 * i], iy = ijk[3 * i + 1], iz = ijk[3 * i + 2];
@@ -545,6 +568,7 @@ __device__ inline void fused_relax(T* __restrict__ pc, const T* __restrict__ pm,
 
 template <typename T>
 __global__ void __launch_bounds__(FNT, 3) k_sor_fused(FusedArgs<T> a) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sp = reinterpret_cast<T*>(smraw);  // [4][FPL] phi planes
   T* sr = sp + 4 * FPL;                 // [3][FPL] rhs planes
@@ -663,6 +687,7 @@ __global__ void __launch_bounds__(256) k_residual(const T* __restrict__ phi, con
                                                   TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
                                                   int ixmax, int iymin, int iymax, int izmin, int izmax, T cx, T cy,
                                                   T cz, T mgparam, unsigned long long* maxout) {
+  pdl_entry();
   // MODE 0 covers the padded array, the others the node array; ZPT planes
   // per thread with all loads issued first; 32-bit offsets
   const int g = (MODE == 0) ? 1 : 0;
@@ -713,6 +738,7 @@ template <typename T, int MODE, typename TO>
 __global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, int nx, int ny, int nz, CondArgs<T> C,
                               Bnd B, double dxsqi, double dysqi, double dzsqi, double mgparam_d, int voltfac_on,
                               int mgform2init, int lcndbndy, unsigned long long* maxout) {
+  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double m = 0.;
   auto store = [&](int ix, int iy, int iz, T v) {
@@ -797,6 +823,7 @@ __global__ void __launch_bounds__(256) k_restrict(const T* __restrict__ res, T* 
                                                   int izcmin, int izcmax, const int32_t* __restrict__ tlo,
                                                   const int32_t* __restrict__ tn, const double* __restrict__ tw,
                                                   double ff) {
+  pdl_entry();
   const int ixc = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int iyc = (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int izc = blockIdx.z;
@@ -855,6 +882,7 @@ __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __
                                                 int nxc, int nyc, int ixmin, int ixmax, int iymin, int iymax,
                                                 int izmin, int izmax, const int32_t* __restrict__ ej,
                                                 const double* __restrict__ ew) {
+  pdl_entry();
   const int ix = ixmin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = iymin + (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int iz0 = izmin + (int)blockIdx.z * ZPT;
@@ -907,6 +935,7 @@ __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __
 // mgerror = max|phisave - phi| over nodes 0..n (f3d_mgrid.F:383-391).
 __global__ void k_maxdiff(const double* __restrict__ a, const double* __restrict__ b, int nx, int ny,
                           unsigned long long* maxout) {
+  pdl_entry();
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z;
@@ -922,6 +951,7 @@ __global__ void k_maxdiff(const double* __restrict__ a, const double* __restrict
 // rhs (node layout) into the interior of a padded array: the source of the
 // full multigrid's restriction of rho, whose windows stay inside 0..n.
 __global__ void k_pad_copy(const double* __restrict__ src, double* __restrict__ dst, int nx, int ny) {
+  pdl_entry();
   const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y, iz = blockIdx.z;
   if (ix > nx || iy > ny) return;
   dst[(size_t)(ix + 1) + (size_t)(nx + 3) * ((size_t)(iy + 1) + (size_t)(ny + 3) * (iz + 1))] =
@@ -930,6 +960,7 @@ __global__ void k_pad_copy(const double* __restrict__ src, double* __restrict__ 
 
 __global__ void k_scale_rhs(const double* __restrict__ rho, double* __restrict__ rhs, size_t n, double s,
                             unsigned long long* maxout, unsigned long long* flag) {
+  pdl_entry();
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   double m = 0.;
   if (i < n) {
@@ -946,6 +977,7 @@ __global__ void k_scale_rhs(const double* __restrict__ rho, double* __restrict__
 constexpr int kCorrPlanes = 4;
 __global__ void __launch_bounds__(256) k_add_corr(double* __restrict__ phi, const float* __restrict__ e, int nx,
                                                   int ny, int nz, unsigned long long* maxout) {
+  pdl_entry();
   const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 1;
   const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
   const int iz0 = (int)blockIdx.z * kCorrPlanes - 1;
@@ -1038,6 +1070,41 @@ struct Solver {
   cudaStream_t s;
   bool fused_ok;  // boundary types and options allow the fused sweep
   bool capturing = false;
+  bool pdl = false;  // launch with programmatic dependent launch
+  cudaError_t lerr = cudaSuccess;  // first launch error
+
+  // One kernel launch on the solver's stream; with pdl set, the kernel may
+  // be scheduled while the previous one in the stream still runs (every
+  // kernel launched here starts with pdl_entry()).
+  template <typename... KArgs, typename... Args>
+  void launch(void (*k)(KArgs...), dim3 g, dim3 b, size_t smem, Args&&... args) {
+    ++c->nlaunch;
+    cudaError_t e;
+    if (pdl) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = g;
+      cfg.blockDim = b;
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = s;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      e = cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+    } else {
+      k<<<g, b, smem, s>>>(std::forward<Args>(args)...);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess && lerr == cudaSuccess) lerr = e;
+  }
+
+  // zeroes n elements (a kernel, so that a chain of launches stays PDL)
+  template <typename T>
+  void zero(T* u, size_t n) {
+    const unsigned nb = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
+    launch(k_zero<T>, dim3(nb), dim3(256), 0, u, n);
+  }
 
   int prof_begin(int l, int kind, double units) { return (!capturing && l == 0) ? c->prof_begin(kind, units) : -1; }
 
@@ -1046,10 +1113,10 @@ struct Solver {
     const int* b = B.b;
     bool xy = lwithdirichlet || b[0] >= 1 || b[1] >= 1 || b[2] >= 1 || b[3] >= 1;
     bool z = lwithdirichlet || b[4] >= 1 || b[5] >= 1;
-    if (xy) { ++c->nlaunch; k_bc_xy<T><<<L.d.nz + 1, 256, 0, s>>>(u, L.d.nx, L.d.ny, B, (int)lwithdirichlet); }
+    if (xy) { launch(k_bc_xy<T>, L.d.nz + 1, 256, 0, u, L.d.nx, L.d.ny, B, (int)lwithdirichlet); }
     if (z) {
       size_t nxy = (size_t)(L.d.nx + 3) * (L.d.ny + 3);
-      { ++c->nlaunch; k_bc_z<T><<<cdiv(nxy, 256), 256, 0, s>>>(u, L.d.nx, L.d.ny, L.d.nz, B, (int)lwithdirichlet); }
+      { launch(k_bc_z<T>, cdiv(nxy, 256), 256, 0, u, L.d.nx, L.d.ny, L.d.nz, B, (int)lwithdirichlet); }
     }
   }
 
@@ -1065,8 +1132,7 @@ struct Solver {
     for (int par = 0; par < 2; ++par) {
       DevSubgrid& S = L.sub[par];
       if (S.n) {
-        ++c->nlaunch;
-        k_condbndymgint<T><<<cdiv(S.n, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, S.ijk, S.dels, S.n, B);
+        launch(k_condbndymgint<T>, cdiv(S.n, 128), 128, 0, phi, L.d.nx, L.d.ny, L.d.nz, S.ijk, S.dels, S.n, B);
       }
     }
   }
@@ -1077,8 +1143,7 @@ struct Solver {
     Level& L = c->lv[l];
     int n = L.n_int + L.sub[0].n + L.sub[1].n;
     if (!n) return;
-    ++c->nlaunch;
-    k_box<T><<<cdiv(n, 128), 128, 0, s>>>(Arr<T>::rhs(L), L.d.nx, L.d.ny, cond_args<T>(L), Arr<T>::srhs(L.sub[0]),
+    launch(k_box<T>, cdiv(n, 128), 128, 0, Arr<T>::rhs(L), L.d.nx, L.d.ny, cond_args<T>(L), Arr<T>::srhs(L.sub[0]),
                                           Arr<T>::srhs(L.sub[1]));
   }
 
@@ -1103,9 +1168,8 @@ struct Solver {
       a.lcndbndy = o->lcndbndy;
       dim3 grd(cdiv(L.d.nx + 3, FTX), cdiv(L.d.ny + 3, FTY), cdiv(L.d.nz + 3, FZC));
       const size_t smem = 7 * FPL * sizeof(T);
-      ++c->nlaunch;
       int pe = prof_begin(l, WG_PROF_SOR0, 2. * (double)L.nr);
-      k_sor_fused<T><<<grd, FNT, smem, s>>>(a);
+      launch(k_sor_fused<T>, grd, FNT, smem, a);
       c->prof_end(pe);
       std::swap(Arr<T>::phi(L), Arr<T>::phi2(L));
       return;
@@ -1123,8 +1187,7 @@ struct Solver {
     const bool merged = !L.has_neumann_sub && xy_dir && (zper || zdir) && L.d.nz >= 2;
     const int wtz = (merged && zper) ? 1 : 0;
     if (L.n_int) {
-      ++c->nlaunch;
-      k_interior<T><<<cdiv(L.n_int, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev,
+      launch(k_interior<T>, cdiv(L.n_int, 128), 128, 0, phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev,
                                                         L.d.nz, wtz);
     }
     neumann_int<T>(L, phi);
@@ -1147,16 +1210,14 @@ struct Solver {
       const int nbz = bulk ? (int)cdiv(nzr, zpt) : 0;
       const int nspz = merged ? (int)cdiv((size_t)nsub, 256u * gx * gy) : 0;
       if (nbz + nspz > 0) {
-        ++c->nlaunch;
         int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
-        k_sor_bulk<T, zpt><<<dim3(gx, gy, nbz + nspz), blk, 0, s>>>(
+        launch(k_sor_bulk<T, zpt>, dim3(gx, gy, nbz + nspz), blk, 0, 
             phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, izmax, parity, (T)k.cx, (T)k.cy,
             (T)k.cz, (T)k.spm1, L.d.nz, wtz, nbz, ca, B, k, (int)usev, o->lcndbndy);
         c->prof_end(pe);
       }
       if (!merged && nsub + ca.nint) {
-        ++c->nlaunch;
-        k_special_sor<T><<<cdiv(nsub + ca.nint, 128), 128, 0, s>>>(phi, L.d.nx, L.d.ny, L.d.nz, ca, parity, B, k,
+        launch(k_special_sor<T>, cdiv(nsub + ca.nint, 128), 128, 0, phi, L.d.nx, L.d.ny, L.d.nz, ca, parity, B, k,
                                                                     (int)usev, (int)usev, o->lcndbndy);
       }
       neumann_int<T>(L, phi);
@@ -1177,9 +1238,8 @@ struct Solver {
     constexpr int zpt = ZPlanes<T>::value;
     dim3 blk(32, 8), grd(cdiv(L.d.nx + 1 + 2 * g, 32), cdiv(L.d.ny + 1 + 2 * g, 8), cdiv(L.d.nz + 1 + 2 * g, zpt));
     {
-      ++c->nlaunch;
       int pe = prof_begin(l, WG_PROF_RESID0, (double)L.nr);
-      k_residual<T, MODE, TO, zpt><<<grd, blk, 0, s>>>(phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
+      launch(k_residual<T, MODE, TO, zpt>, grd, blk, 0, phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
                                                   R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
                                                   (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst),
                                                   (T)o->mgparam, maxout);
@@ -1191,8 +1251,7 @@ struct Solver {
     ca.nint = 0;
     int n = L.sub[0].n + L.sub[1].n;
     if (n) {
-      ++c->nlaunch;
-      k_special_res<T, MODE, TO><<<cdiv(n, 128), 128, 0, s>>>(phi, out, L.d.nx, L.d.ny, L.d.nz, ca, B,
+      launch(k_special_res<T, MODE, TO>, cdiv(n, 128), 128, 0, phi, out, L.d.nx, L.d.ny, L.d.nz, ca, B,
                                                               dxsqi, dysqi, dzsqi, o->mgparam, (int)voltfac_on,
                                                               (int)mgform2init, o->lcndbndy, maxout);
     }
@@ -1214,18 +1273,17 @@ struct Solver {
       double ff = (dxsqi + dysqi + dzsqi) / (dxcsqi + dycsqi + dzcsqi);
       Ranges Rc = ranges(dc, B.b, false);
       dim3 blk(32, 8), grd(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), dc.nz + 1);
-      ++c->nlaunch;
       int pr = prof_begin(l, WG_PROF_RESTRICT0, (double)L.nr);
       if (L.rmax <= 3)
-        k_restrict<T, 3><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin,
+        launch(k_restrict<T, 3>, grd, blk, 0, Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin,
                                              Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax, L.rlo, L.rn, L.rw, ff);
       else
-        k_restrict<T, kRestrictTaps><<<grd, blk, 0, s>>>(Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny,
+        launch(k_restrict<T, kRestrictTaps>, grd, blk, 0, Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny,
                                                          Rc.ixmin, Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
                                                          L.rlo, L.rn, L.rw, ff);
       c->prof_end(pr);
       box<T>(l + 1);
-      cudaMemsetAsync(Arr<T>::phi(Lc), 0, Lc.np * sizeof(T), s);
+      zero(Arr<T>::phi(Lc), Lc.np);
       int pc = (l == 0) ? prof_begin(0, WG_PROF_COARSE, (double)Lc.nr) : -1;
       vcycle<T>(l + 1, false);
       c->prof_end(pc);
@@ -1248,13 +1306,12 @@ struct Solver {
     dim3 blk(32, 8);
     dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), cdiv(R.izmax - R.izmin + 1, zpt));
     if (R.ixmax >= R.ixmin && R.iymax >= R.iymin && R.izmax >= R.izmin) {
-      ++c->nlaunch;
       int pe = prof_begin(l, WG_PROF_EXPAND0, (double)L.nr);
       if (dc.nz == d.nz)
-        k_expand<T, zpt, false><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
+        launch(k_expand<T, zpt, false>, grd2, blk, 0, Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
                                                      R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
       else
-        k_expand<T, zpt, true><<<grd2, blk, 0, s>>>(Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
+        launch(k_expand<T, zpt, true>, grd2, blk, 0, Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
                                                     R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
       c->prof_end(pe);
     }
@@ -1283,18 +1340,17 @@ struct Solver {
       const LevelDims& d = L.d;
       const LevelDims& dc = Lc.d;
       dim3 blk(32, 8);
-      { ++c->nlaunch; k_pad_copy<<<dim3(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1), blk, 0, s>>>(L.rhs, L.res, d.nx, d.ny); }
+      { launch(k_pad_copy, dim3(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, 8), d.nz + 1), blk, 0, L.rhs, L.res, d.nx, d.ny); }
       double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
       double dxcsqi = 1. / (dc.dx * dc.dx), dycsqi = 1. / (dc.dy * dc.dy), dzcsqi = 1. / (dc.dz * dc.dz);
       double ff = (dxsqi + dysqi + dzsqi) / (dxcsqi + dycsqi + dzcsqi);
       Ranges Rc = ranges(dc, B.b, false);
       dim3 grd(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), dc.nz + 1);
-      ++c->nlaunch;
       if (L.rmax0 <= 3)
-        k_restrict<double, 3><<<grd, blk, 0, s>>>(L.res, Lc.rhs, d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin, Rc.ixmax,
+        launch(k_restrict<double, 3>, grd, blk, 0, L.res, Lc.rhs, d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin, Rc.ixmax,
                                                   Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax, L.rlo0, L.rn0, L.rw0, ff);
       else
-        k_restrict<double, kRestrictTaps><<<grd, blk, 0, s>>>(L.res, Lc.rhs, d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin,
+        launch(k_restrict<double, kRestrictTaps>, grd, blk, 0, L.res, Lc.rhs, d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin,
                                                               Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
                                                               L.rlo0, L.rn0, L.rw0, ff);
     }
@@ -1309,10 +1365,10 @@ struct Solver {
     for (int l = lmax; l >= 0; --l) {
       Level& L = c->lv[l];
       if (l < lmax) {
-        WG_TRY_CUDA(cudaMemsetAsync(L.phi, 0, L.np * sizeof(double), s));
+        zero(L.phi, L.np);
         expand<double>(l);
       } else if (l > 0) {
-        WG_TRY_CUDA(cudaMemsetAsync(L.phi, 0, L.np * sizeof(double), s));
+        zero(L.phi, L.np);
       }
       bc<double>(L, L.phi, false);
       if (l == 0) break;
@@ -1326,12 +1382,12 @@ struct Solver {
   // reduction slot area of quantity q: 0 max|dphi|, 1 max|res|, 2 max|rhs|
   unsigned long long* slotq(int q) { return c->dslot + (size_t)q * kRedQ; }
   int clear_slots(int q) {
-    WG_TRY_CUDA(cudaMemsetAsync(slotq(q), 0, kRedQ * sizeof(unsigned long long), s));
+    zero(slotq(q), (size_t)kRedQ);
     return WG_OK;
   }
 
   int fetch_red(double* out, int n) {
-    { ++c->nlaunch; k_fold_max<<<1, 96, 0, s>>>(c->dslot, c->dred, 3); }
+    { launch(k_fold_max, 1, 96, 0, c->dslot, c->dred, 3); }
     WG_TRY_CUDA(cudaMemcpyAsync(c->hred, c->dred, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     WG_TRY_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n; ++i) {
@@ -1370,6 +1426,7 @@ int run_vcycle(Solver& S, bool usev) {
   unsigned long long key = mp ^ ((unsigned long long)o->mgmaxlevels << 1) ^ ((unsigned long long)o->downpasses << 9) ^
                            ((unsigned long long)o->uppasses << 17) ^ ((unsigned long long)o->lcndbndy << 25) ^
                            ((unsigned long long)S.fused_ok << 27) ^ ((unsigned long long)usev << 28) ^
+                           ((unsigned long long)S.pdl << 29) ^
                            ((unsigned long long)c->cond_version << 32);
   if (!c->vgraph[gi] || c->vgraph_key[gi] != key) {
     if (c->vgraph[gi]) cudaGraphExecDestroy(c->vgraph[gi]);
@@ -1382,7 +1439,9 @@ int run_vcycle(Solver& S, bool usev) {
     cudaGraph_t g;
     WG_TRY_CUDA(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
     G.vcycle<T>(0, usev);
-    WG_TRY_CUDA(cudaStreamEndCapture(c->cap_stream, &g));
+    cudaError_t ce = cudaStreamEndCapture(c->cap_stream, &g);
+    if (G.lerr != cudaSuccess) ce = G.lerr;
+    WG_TRY_CUDA(ce);
     cudaError_t e = cudaGraphInstantiate(&c->vgraph[gi], g, 0);
     cudaGraphDestroy(g);
     WG_TRY_CUDA(e);
@@ -1422,6 +1481,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   Solver S{c, o, {}, c->stream, false};
   for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
   S.fused_ok = fused_allowed(S.B.b) && (o->flags & WG_SOLVE_FUSED);
+  S.pdl = (o->flags & WG_SOLVE_PDL) && !c->prof_mask;
   cudaStream_t s = c->stream;
   Level& L0 = c->lv[0];
   double* user_phi = L0.phi;
@@ -1430,7 +1490,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   double reps0c = o->mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
   WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
   WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
-  { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
+  { S.launch(k_scale_rhs, cdiv(L0.nr, 256), 256, 0, c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
   const bool fmg = o->mgmaxvcycles > 0;
   const int lmax = fmg ? S.deepest() : 0;
   if (fmg) S.fmg_restrict(lmax);
@@ -1463,7 +1523,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       it += 1;
       if (o->tolkind == 0) {
         WG_TRY(S.clear_slots(0));
-        { ++c->nlaunch; k_maxdiff<<<grdn, blk, 0, s>>>(c->phisave, L0.phi, d.nx, d.ny, S.slotq(0)); }
+        { S.launch(k_maxdiff, grdn, blk, 0, c->phisave, L0.phi, d.nx, d.ny, S.slotq(0)); }
         WG_TRY(S.fetch_red(rv, 1));
         err = rv[0];
         if (!(err > o->mgtol)) { conv = true; break; }
@@ -1473,8 +1533,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
     for (;;) {
       // residual of the FP64 solution with actual voltages (mgform = 2 set-up)
       if (L0.n_int) {
-        ++c->nlaunch;
-        k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(L0.phi, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);
+        S.launch(k_interior<double>, cdiv(L0.n_int, 128), 128, 0, L0.phi, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1, 0, 0);
       }
       S.neumann_int<double>(L0, L0.phi);
       WG_TRY(S.clear_slots(1));
@@ -1486,14 +1545,13 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       }
       if (it >= o->mgmaxiters) break;
       S.box<float>(0);
-      WG_TRY_CUDA(cudaMemsetAsync(L0.phif, 0, L0.np * sizeof(float), s));
+      S.zero(L0.phif, L0.np);
       WG_TRY(run_vcycle<float>(S, false));
       WG_TRY(S.clear_slots(0));
       {
-        ++c->nlaunch;
         dim3 grdc(cdiv(d.nx + 3, 32), cdiv(d.ny + 3, 8), cdiv(d.nz + 3, kCorrPlanes));
         int pe = S.prof_begin(0, WG_PROF_CORR, (double)L0.nr);
-        k_add_corr<<<grdc, blk, 0, s>>>(L0.phi, L0.phif, d.nx, d.ny, d.nz, S.slotq(0));
+        S.launch(k_add_corr, grdc, blk, 0, L0.phi, L0.phif, d.nx, d.ny, d.nz, S.slotq(0));
         c->prof_end(pe);
       }
       S.bc<double>(L0, L0.phi, false);
@@ -1507,6 +1565,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   }
   WG_TRY(S.restore_phi(user_phi));
   S.bc<double>(L0, L0.phi, true);
+  WG_TRY_CUDA(S.lerr);
   WG_TRY_CUDA(cudaGetLastError());
   WG_TRY_CUDA(cudaStreamSynchronize(s));
   st->mgiters = it;
