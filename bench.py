@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--forms", default="plain,mixed")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-vcycles", type=float, default=None)
     ap.add_argument("--ref-sample", type=int, default=1_000_000)
@@ -184,8 +184,9 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
 def e2e_steps(run, steps):
     """The drop-in path with host-owned particles (WARP's pgroup lives in
     host memory): every step moves the 7 particle arrays host->device from
-    pinned memory and back through ESPIC.step_host, which pipelines the
-    copies in chunks against the advance, the deposit and the solve."""
+    pinned memory and back through ESPIC.run_host, which pipelines the
+    copies in chunks against the advance and the deposit, and queues the
+    next step's uploads before the field solve."""
     import torch
     from warp_b200.particles import FIELDS
     pg = run.pgroup
@@ -199,8 +200,7 @@ def e2e_steps(run, steps):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(steps):
-        run.step_host(host)
+    run.run_host(host, steps)
     e1.record(stream)
     torch.cuda.synchronize()
     nbytes = 8 * pg.np * len(FIELDS)

@@ -165,6 +165,18 @@ int wg_field_energy(wg_ctx* ctx, double* out);
  * 64-bit fixed-point grid, so rho is bit-identical from run to run.
  * zero_first clears rho first (loadrho3d zeroes rho before depositing). */
 int wg_deposit(wg_ctx* ctx, const wg_particles* p, int zero_first);
+/* The deposit of wg_deposit in pieces, for a caller that streams particles
+ * in (no counterpart in the reference; it replaces one wg_deposit of a
+ * species whose arrays arrive chunk by chunk). wg_deposit_begin clears the
+ * fixed-point accumulator; wg_deposit_add accumulates one piece (every piece
+ * must carry the same q and w); wg_deposit_end converts into rho, replacing
+ * it when zero_first is set. The result equals one wg_deposit of all pieces
+ * bit for bit. None of the three synchronizes the stream: an accumulator
+ * overflow is reported as WG_EOVERFLOW by the next wg_solve. wg_deposit
+ * returns WG_ESTATE while a chunked deposit is open. */
+int wg_deposit_begin(wg_ctx* ctx);
+int wg_deposit_add(wg_ctx* ctx, const wg_particles* p);
+int wg_deposit_end(wg_ctx* ctx, int zero_first);
 /* The deposit of wg_deposit into a caller-owned rho(0:nx,0:ny,0:nz) array,
  * with no context and no allocation (no counterpart in the reference). For
  * callers that cannot let a library allocate device memory: host codes that

@@ -147,6 +147,53 @@ def test_accumulator_overflow_is_reported():
     assert e.value.code == -4
 
 
+def test_chunked_deposit_matches_loadrho_and_checks_its_use():
+    from warp_b200._lib import WgError
+    s = _solver()
+    p = _beam(30_000, seed=4)
+    pg = _group(p)
+    s.loadrho(pgroups=[pg])
+    ref = s.rho.clone()
+    s.deposit_begin()
+    for a, b in ((0, 7000), (7000, 7000), (7000, 30_000)):
+        s.deposit_add(pg, a, b)
+    s.deposit_end()
+    assert torch.equal(s.rho, ref)
+    # pieces with another weight, a plain deposit while open, add after end
+    s.deposit_begin()
+    s.deposit_add(pg, 0, 100)
+    with pytest.raises(WgError) as e:
+        s.deposit_add(_group(p, w=2e4), 100, 200)
+    assert e.value.code == -1
+    with pytest.raises(WgError) as e:
+        s.loadrho(pgroups=[pg])
+    assert e.value.code == -3
+    s.deposit_end()
+    with pytest.raises(WgError) as e:
+        s.deposit_add(pg, 0, 10)
+    assert e.value.code == -3
+
+
+def test_chunked_deposit_overflow_is_reported_by_the_next_solve():
+    from warp_b200._lib import WgError
+    s = _solver()
+    n = 70000
+    x0, y0, z0 = s.xmmin + 5 * s.dx, s.ymmin + 5 * s.dy, s.zmmin + 5 * s.dz
+    p = {"x": np.full(n, x0), "y": np.full(n, y0), "z": np.full(n, z0), "ux": np.zeros(n), "uy": np.zeros(n),
+         "uz": np.zeros(n), "gaminv": np.ones(n)}
+    pg = _group(p)
+    s.deposit_begin()
+    s.deposit_add(pg, 0, 40000)
+    s.deposit_add(pg, 40000, n)
+    s.deposit_end()
+    with pytest.raises(WgError) as e:
+        s.solve()
+    assert e.value.code == -4
+    # the flag is cleared once reported
+    s.rho = np.zeros((s.nx + 1, s.ny + 1, s.nz + 1))
+    s.solve()
+
+
 def test_bad_and_too_large_grids():
     from warp_b200._lib import WgError
     with pytest.raises(WgError) as e:

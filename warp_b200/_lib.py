@@ -89,6 +89,9 @@ SIGNATURES = {
     "wg_set_lattice": [_vp, _dp, _dp, _dp, _c.c_int, _c.c_double, _c.c_double],
     "wg_advance": [_vp, ctypes.POINTER(Particles), ctypes.POINTER(PushParams)],
     "wg_set_correctede": [_vp, _c.c_int],
+    "wg_deposit_begin": [_vp],
+    "wg_deposit_add": [_vp, ctypes.POINTER(Particles)],
+    "wg_deposit_end": [_vp, _c.c_int],
     "wg_moments": [_vp, ctypes.POINTER(Particles), _dp],
     "wg_prof_enable": [_vp, _c.c_int],
     "wg_prof_read": [_vp, _c.c_int, _dp, _i64p, _dp],

@@ -23,6 +23,9 @@ int field_energy(wg_ctx* c, double* out);
 int deposit(wg_ctx* c, const wg_particles* p, int zero_first);
 int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream);
 int finalize_rho(wg_ctx* c);
+int deposit_begin(wg_ctx* c);
+int deposit_add(wg_ctx* c, const wg_particles* p);
+int deposit_end(wg_ctx* c, int zero_first);
 int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double* ex, double* ey, double* ez,
             int64_t np);
 int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm);
@@ -333,7 +336,7 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
   if (rc == WG_OK) rc = dalloc(&c->phisave, L0.np);
   if (rc == WG_OK) rc = dalloc(&c->rho, L0.nr);
   if (rc == WG_OK) rc = dalloc(&c->racc, L0.nr);
-  if (rc == WG_OK) rc = dalloc(&c->dred, (size_t)4);
+  if (rc == WG_OK) rc = dalloc(&c->dred, (size_t)5);
   if (rc == WG_OK) rc = dalloc(&c->dese, (size_t)(G.nx + 1) * (G.ny + 1) + 1);
   if (rc == WG_OK) rc = dalloc(&c->dslot, (size_t)3 * 32 * 16);
   if (rc == WG_OK) {
@@ -342,7 +345,7 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
     c->mom_blocks = prop.multiProcessorCount * 4;
     rc = dalloc(&c->dmom, (size_t)moments_scratch_doubles(c->mom_blocks));
   }
-  if (rc == WG_OK && cudaMallocHost((void**)&c->hred, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+  if (rc == WG_OK && cudaMallocHost((void**)&c->hred, 5 * sizeof(unsigned long long)) != cudaSuccess) {
     set_error("wg_create: cudaMallocHost failed");
     rc = WG_ENOMEM;
   }
@@ -498,7 +501,23 @@ int wg_relresidual(wg_ctx* c, double mgparam, double* out) {
 
 int wg_deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
   if (!c) { set_error("null context"); return WG_EINVAL; }
+  if (c->dep_open) { set_error("wg_deposit: a chunked deposit is open (wg_deposit_end first)"); return WG_ESTATE; }
   return deposit(c, p, zero_first);
+}
+
+int wg_deposit_begin(wg_ctx* c) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return deposit_begin(c);
+}
+
+int wg_deposit_add(wg_ctx* c, const wg_particles* p) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return deposit_add(c, p);
+}
+
+int wg_deposit_end(wg_ctx* c, int zero_first) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return deposit_end(c, zero_first);
 }
 
 int wg_deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream) {

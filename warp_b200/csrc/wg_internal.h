@@ -124,7 +124,8 @@ struct wg_ctx {
   double* phisave = nullptr;          // copy of phi at the start of a V-cycle
   double* rho = nullptr;              // user-visible rho (Fortran layout)
   unsigned long long* racc = nullptr; // fixed-point deposit accumulator
-  // reductions: [0] max|dphi| bits, [1] max|res| bits, [2] max|rhs| bits, [3] flags
+  // reductions: [0] max|dphi| bits, [1] max|res| bits, [2] max|rhs| bits, [3] flags,
+  // [4] accumulator overflow of the last chunked deposit (reported by wg_solve)
   unsigned long long* dred = nullptr;
   unsigned long long* dslot = nullptr; // per-block max slots of [0..2], folded into dred
   unsigned long long* hred = nullptr;  // pinned host copy
@@ -138,6 +139,11 @@ struct wg_ctx {
   int nzl = -1;
   double zlmin = 0., dzl = 1.;
   bool have_fp32 = false;
+  // chunked deposit (wg_deposit_begin/add/end): open, and the q*w/(dx dy dz)
+  // that every piece shares
+  bool dep_open = false;
+  bool dep_gg_set = false;
+  double dep_gg = 0.;
   // lcorrectede: E next to conductors from the subgrid data
   int correctede = 0;
   int* icgrid = nullptr;                 // level-0 nodes: 0 vacuum, kIcInterior, +/- (subgrid index + 1)

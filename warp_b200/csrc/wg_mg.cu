@@ -1391,7 +1391,7 @@ struct Solver {
 
   int fetch_red(double* out, int n) {
     { launch(k_fold_max, 1, 96, 0, c->dslot, c->dred, 3); }
-    WG_TRY_CUDA(cudaMemcpyAsync(c->hred, c->dred, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    WG_TRY_CUDA(cudaMemcpyAsync(c->hred, c->dred, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     WG_TRY_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n; ++i) {
       unsigned long long v = c->hred[i];
@@ -1508,6 +1508,12 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   if (c->hred[3] & 2ull) {
     set_error("wg_solve: rho contains NaN or Inf");
     return WG_EINVAL;
+  }
+  if (c->hred[4]) {
+    WG_TRY_CUDA(cudaMemsetAsync(c->dred + 4, 0, sizeof(unsigned long long), s));
+    set_error("wg_solve: the last chunked deposit overflowed the fixed-point accumulator (more than 65536 full "
+              "particle weights on one node)");
+    return WG_EOVERFLOW;
   }
   if (fmg) WG_TRY(S.fmg_up(lmax, o->mgmaxvcycles));
   if (o->precision == 0) {

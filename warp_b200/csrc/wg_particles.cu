@@ -747,6 +747,58 @@ int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
   return WG_OK;
 }
 
+// Chunked deposit: the pieces accumulate in the same fixed-point grid and
+// are converted once, so the result is the same as one deposit of all
+// pieces, bit for bit. Nothing here synchronizes the stream; an overflow is
+// flagged in dred[4] and reported by the next solve.
+int deposit_begin(wg_ctx* c) {
+  cudaStream_t s = c->stream;
+  WG_TRY_CUDA(cudaMemsetAsync(c->racc, 0, c->lv[0].nr * sizeof(unsigned long long), s));
+  WG_TRY_CUDA(cudaMemsetAsync(c->dred + 4, 0, sizeof(unsigned long long), s));
+  c->dep_open = true;
+  c->dep_gg_set = false;
+  c->dep_gg = 0.;
+  return WG_OK;
+}
+
+int deposit_add(wg_ctx* c, const wg_particles* p) {
+  if (!p || (p->np > 0 && (!p->x || !p->y || !p->z || !p->gaminv)) || p->np < 0) {
+    set_error("wg_deposit_add: null particle arrays");
+    return WG_EINVAL;
+  }
+  if (!c->dep_open) {
+    set_error("wg_deposit_add: no chunked deposit open (wg_deposit_begin)");
+    return WG_ESTATE;
+  }
+  double gg = p->w * p->q;
+  gg = gg / c->dx;
+  gg = gg / c->dy;
+  gg = gg / c->dz;
+  if (c->dep_gg_set && gg != c->dep_gg) {
+    set_error("wg_deposit_add: the pieces of one deposit must share q and w");
+    return WG_EINVAL;
+  }
+  c->dep_gg = gg;
+  c->dep_gg_set = true;
+  if (p->np == 0) return WG_OK;
+  if (cdiv64(p->np, 256) > 2147483647LL) { set_error("wg_deposit_add: too many particles"); return WG_ETOOLARGE; }
+  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, c->stream>>>(p->x, p->y, p->z, p->gaminv, p->np, gridp(c), c->racc); c->prof_end(pe); }
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
+int deposit_end(wg_ctx* c, int zero_first) {
+  if (!c->dep_open) {
+    set_error("wg_deposit_end: no chunked deposit open (wg_deposit_begin)");
+    return WG_ESTATE;
+  }
+  c->dep_open = false;
+  Level& L0 = c->lv[0];
+  { ++c->nlaunch; k_fix_to_rho<<<cdiv64((int64_t)L0.nr, 256), 256, 0, c->stream>>>(c->racc, c->rho, L0.nr, c->dep_gg * kFixInv, zero_first ? 0 : 1, c->dred + 4); }
+  WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
 int finalize_rho(wg_ctx* c) {
   const wg_grid& G = c->grid;
   cudaStream_t s = c->stream;

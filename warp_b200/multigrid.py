@@ -246,6 +246,28 @@ class MultiGridB200(FieldSolver):
         if lfinalize_rho:
             _lib.check(_lib.lib.wg_finalize_rho(self._h))
 
+    def deposit_begin(self):
+        """Opens a deposit in pieces (wg_deposit_begin): clears the
+        fixed-point accumulator. No host synchronization."""
+        self._bind_stream()
+        _lib.check(_lib.lib.wg_deposit_begin(self._h))
+
+    def deposit_add(self, pgroup, start=0, stop=None):
+        """Accumulates particles start:stop of pgroup (wg_deposit_add)."""
+        self._bind_stream()
+        s = pgroup.cstruct(start, stop)
+        _lib.check(_lib.lib.wg_deposit_add(self._h, ctypes.byref(s)))
+
+    def deposit_end(self, zero_first=True, lfinalize_rho=True):
+        """Converts the accumulated pieces into rho (replacing it when
+        zero_first) and applies the rho boundary conditions. The result is
+        the same as loadrho of all pieces at once, bit for bit; an
+        accumulator overflow is reported by the next solve."""
+        self._bind_stream()
+        _lib.check(_lib.lib.wg_deposit_end(self._h, int(bool(zero_first))))
+        if lfinalize_rho:
+            _lib.check(_lib.lib.wg_finalize_rho(self._h))
+
     def _opts(self):
         flags = (_lib.SOLVE_GRAPH if self.use_graphs else 0) | (_lib.SOLVE_FUSED if self.fused_sweep else 0) | \
             (_lib.SOLVE_PDL if self.use_pdl else 0)

@@ -120,58 +120,82 @@ class ESPIC:
 
     def step_host(self, host, nchunks=8):
         """One step of the drop-in mode in which the host owns the particles
-        (WARP keeps top.pgroup in host memory): `host` maps each of
-        x, y, z, ux, uy, uz, gaminv to a pinned CPU float64 tensor, read at
-        the start of the step and rewritten with the advanced particles.
+        (WARP keeps top.pgroup in host memory); run_host with nsteps = 1."""
+        self.run_host(host, 1, nchunks)
+
+    def run_host(self, host, nsteps=1, nchunks=8):
+        """nsteps steps of the drop-in mode in which the host owns the
+        particles (WARP keeps top.pgroup in host memory, and step(n) runs n
+        steps): `host` maps each of x, y, z, ux, uy, uz, gaminv to a pinned
+        CPU float64 tensor. Every step reads the arrays from the host and
+        writes the advanced particles back.
 
         The arrays cross PCIe in `nchunks` chunks. Uploads run on one copy
-        stream, and each chunk is advanced as soon as it has landed. The
-        advanced chunks go back on a second copy stream, so downloads overlap
-        the remaining uploads (PCIe is full duplex), the deposit and the
-        field solve. The step returns with the host arrays written; the
-        device state is the same as after step()."""
+        stream; each chunk is advanced and deposited as soon as it has
+        landed, then goes back on a second copy stream, so downloads overlap
+        the remaining uploads (PCIe is full duplex). The pieces accumulate in
+        one fixed-point deposit, so rho is the same as after step(). The
+        uploads of the next step are queued before this step's field solve:
+        chunk k goes up as soon as this step has brought chunk k down, so the
+        transfers of step n+1 overlap the solve of step n. The host arrays
+        are complete once the call returns and the current stream has been
+        synchronized; the device state is then the same as after nsteps
+        calls of step()."""
         import torch
         from .particles import FIELDS
-        pg = self.pgroup
+        pg, s = self.pgroup, self.solver
         n = pg.np
         if self.sort_interval:
-            raise ValueError("step_host: the host owns the particle order; use sort_interval=0")
+            raise ValueError("run_host: the host owns the particle order; use sort_interval=0")
         main = torch.cuda.current_stream(pg.device)
         if not hasattr(self, "_h2d"):
             self._h2d = torch.cuda.Stream(pg.device)
             self._d2h = torch.cuda.Stream(pg.device)
         h2d, d2h = self._h2d, self._d2h
         edges = [n * k // nchunks for k in range(nchunks + 1)]
-        center = self._center()
-        landed, advanced = [], []
-        h2d.wait_stream(main)
-        with torch.cuda.stream(h2d):
+        landed = [None] * nchunks
+        brought = [None] * nchunks  # chunk k is back on the host
+
+        def upload():
             for k in range(nchunks):
+                if brought[k] is None:
+                    h2d.wait_stream(main)
+                else:
+                    h2d.wait_event(brought[k])
                 a, b = edges[k], edges[k + 1]
-                for f in FIELDS:
-                    getattr(pg, f)[a:b].copy_(host[f][a:b], non_blocking=True)
+                with torch.cuda.stream(h2d):
+                    for f in FIELDS:
+                        getattr(pg, f)[a:b].copy_(host[f][a:b], non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(h2d)
-                landed.append(ev)
-        for k in range(nchunks):
-            a, b = edges[k], edges[k + 1]
-            main.wait_event(landed[k])
-            if b > a:
-                self.solver.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], start=a, stop=b, center=center)
-            ev = torch.cuda.Event()
-            ev.record(main)
-            advanced.append(ev)
-        with torch.cuda.stream(d2h):
+                landed[k] = ev
+
+        upload()
+        for it in range(nsteps):
+            center = self._center()
+            s.deposit_begin()
             for k in range(nchunks):
                 a, b = edges[k], edges[k + 1]
-                d2h.wait_event(advanced[k])
-                for f in FIELDS:
-                    host[f][a:b].copy_(getattr(pg, f)[a:b], non_blocking=True)
-        self.solver.loadrho()
-        self.solver.solve()
+                main.wait_event(landed[k])
+                if b > a:
+                    s.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], start=a, stop=b, center=center)
+                    s.deposit_add(pg, a, b)
+                ev = torch.cuda.Event()
+                ev.record(main)
+                d2h.wait_event(ev)
+                with torch.cuda.stream(d2h):
+                    for f in FIELDS:
+                        host[f][a:b].copy_(getattr(pg, f)[a:b], non_blocking=True)
+                back = torch.cuda.Event()
+                back.record(d2h)
+                brought[k] = back
+            s.deposit_end(zero_first=True)
+            self.vsync = False
+            if it + 1 < nsteps:
+                upload()
+            s.solve()
+            self.it += 1
         main.wait_stream(d2h)
-        self.vsync = False
-        self.it += 1
 
     def synchv(self):
         """padvnc3d("synchv") at the end of a special step (w3d.F:975): a
