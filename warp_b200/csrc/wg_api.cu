@@ -345,9 +345,16 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
     c->mom_blocks = prop.multiProcessorCount * 4;
     rc = dalloc(&c->dmom, (size_t)moments_scratch_doubles(c->mom_blocks));
   }
-  if (rc == WG_OK && cudaMallocHost((void**)&c->hred, 5 * sizeof(unsigned long long)) != cudaSuccess) {
-    set_error("wg_create: cudaMallocHost failed");
+  // The reduction words reach the host through mapped pinned memory written
+  // by a kernel, not through a copy: a small device-to-host copy would queue
+  // behind the bulk copies of a caller's other streams on the copy engines.
+  if (rc == WG_OK && cudaHostAlloc((void**)&c->hred, 5 * sizeof(unsigned long long), cudaHostAllocMapped) != cudaSuccess) {
+    set_error("wg_create: cudaHostAlloc failed");
     rc = WG_ENOMEM;
+  }
+  if (rc == WG_OK && cudaHostGetDevicePointer((void**)&c->hred_dev, c->hred, 0) != cudaSuccess) {
+    set_error("wg_create: cudaHostGetDevicePointer failed");
+    rc = WG_ECUDA;
   }
   if (rc == WG_OK) rc = configure_kernels();
   if (rc == WG_OK) {

@@ -128,7 +128,8 @@ struct wg_ctx {
   // [4] accumulator overflow of the last chunked deposit (reported by wg_solve)
   unsigned long long* dred = nullptr;
   unsigned long long* dslot = nullptr; // per-block max slots of [0..2], folded into dred
-  unsigned long long* hred = nullptr;  // pinned host copy
+  unsigned long long* hred = nullptr;      // mapped pinned host copy, written by kernels
+  unsigned long long* hred_dev = nullptr;  // device address of hred
   double* dmom = nullptr;              // moment partial sums
   double* dese = nullptr;              // field-energy row sums ((nx+1)(ny+1) + 1)
   int mom_blocks = 0;

@@ -135,6 +135,19 @@ __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Reduction words into the mapped host copy (read after a stream sync).
+__global__ void k_publish(const unsigned long long* __restrict__ src, unsigned long long* dst, int n) {
+  pdl_entry();
+  if ((int)threadIdx.x < n) ((volatile unsigned long long*)dst)[threadIdx.x] = src[threadIdx.x];
+  __threadfence_system();
+}
+
+template <typename T>
+__global__ void k_copy(const T* __restrict__ a, T* __restrict__ b, size_t n) {
+  pdl_entry();
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = a[i];
+}
+
 template <typename T>
 __global__ void k_zero(T* __restrict__ u, size_t n) {
   pdl_entry();
@@ -1102,11 +1115,19 @@ struct Solver {
     if (e != cudaSuccess && lerr == cudaSuccess) lerr = e;
   }
 
-  // zeroes n elements (a kernel, so that a chain of launches stays PDL)
+  // Zeroing and copying are kernels here, not cudaMemsetAsync or a
+  // device-to-device cudaMemcpyAsync, so that a chain of launches stays PDL
+  // and nothing in the solve waits for a copy engine that a caller's bulk
+  // transfers keep busy.
   template <typename T>
   void zero(T* u, size_t n) {
     const unsigned nb = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
     launch(k_zero<T>, dim3(nb), dim3(256), 0, u, n);
+  }
+  template <typename T>
+  void copy(const T* a, T* b, size_t n) {
+    const unsigned nb = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
+    launch(k_copy<T>, dim3(nb), dim3(256), 0, a, b, n);
   }
 
   int prof_begin(int l, int kind, double units) { return (!capturing && l == 0) ? c->prof_begin(kind, units) : -1; }
@@ -1391,8 +1412,9 @@ struct Solver {
 
   int fetch_red(double* out, int n) {
     { launch(k_fold_max, 1, 96, 0, c->dslot, c->dred, 3); }
-    WG_TRY_CUDA(cudaMemcpyAsync(c->hred, c->dred, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    { launch(k_publish, 1, 32, 0, c->dred, c->hred_dev, 5); }
     WG_TRY_CUDA(cudaStreamSynchronize(s));
+    WG_TRY_CUDA(lerr);
     for (int i = 0; i < n; ++i) {
       unsigned long long v = c->hred[i];
       double dv;
@@ -1406,7 +1428,7 @@ struct Solver {
   int restore_phi(double* user) {
     Level& L0 = c->lv[0];
     if (L0.phi != user) {
-      WG_TRY_CUDA(cudaMemcpyAsync(user, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      copy(L0.phi, user, L0.np);
       std::swap(L0.phi, L0.phi2);
     }
     return WG_OK;
@@ -1491,8 +1513,8 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   const LevelDims& d = L0.d;
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = o->mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
+  S.zero(c->dred, (size_t)4);
+  S.zero(c->dslot, (size_t)3 * kRedQ);
   { S.launch(k_scale_rhs, cdiv(L0.nr, 256), 256, 0, c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
   const bool fmg = o->mgmaxvcycles > 0;
   const int lmax = fmg ? S.deepest() : 0;
@@ -1510,7 +1532,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
     return WG_EINVAL;
   }
   if (c->hred[4]) {
-    WG_TRY_CUDA(cudaMemsetAsync(c->dred + 4, 0, sizeof(unsigned long long), s));
+    S.zero(c->dred + 4, (size_t)1);
     set_error("wg_solve: the last chunked deposit overflowed the fixed-point accumulator (more than 65536 full "
               "particle weights on one node)");
     return WG_EOVERFLOW;
@@ -1527,7 +1549,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       }
       if (it >= o->mgmaxiters) break;
       if (o->tolkind == 0)
-        WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        S.copy(L0.phi, c->phisave, L0.np);
       WG_TRY(run_vcycle<double>(S, true));
       it += 1;
       if (o->tolkind == 0) {
@@ -1593,12 +1615,12 @@ int relresidual(wg_ctx* c, double mgparam, double* out) {
   const LevelDims& d = L0.d;
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
+  S.zero(c->dred, (size_t)4);
+  S.zero(c->dslot, (size_t)3 * kRedQ);
   { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
   S.box<double>(0);
   // residual of a copy with the conductor voltages imposed, as the solver sees it
-  WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  S.copy(L0.phi, c->phisave, L0.np);
   if (L0.n_int) {
     ++c->nlaunch;
     k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);
@@ -1624,11 +1646,11 @@ int residual_field(wg_ctx* c, double mgparam, double* out) {
   const LevelDims& d = L0.d;
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dred, 0, 4 * sizeof(unsigned long long), s));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dslot, 0, 3 * kRedQ * sizeof(unsigned long long), s));
+  S.zero(c->dred, (size_t)4);
+  S.zero(c->dslot, (size_t)3 * kRedQ);
   { ++c->nlaunch; k_scale_rhs<<<cdiv(L0.nr, 256), 256, 0, s>>>(c->rho, L0.rhs, L0.nr, reps0c, S.slotq(2), c->dred + 3); }
   S.box<double>(0);
-  WG_TRY_CUDA(cudaMemcpyAsync(c->phisave, L0.phi, L0.np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  S.copy(L0.phi, c->phisave, L0.np);
   if (L0.n_int) {
     ++c->nlaunch;
     k_interior<double><<<cdiv(L0.n_int, 128), 128, 0, s>>>(c->phisave, d.nx, d.ny, L0.int_ijk, L0.int_volt, L0.n_int, 1);

@@ -222,6 +222,17 @@ __global__ void __launch_bounds__(DEP_NT) k_deposit(const double* __restrict__ x
 }
 
 // rho (+)= acc * g * 2^-46; flags accumulator values at or above 2^62.
+// Zeroing as a kernel: a cudaMemsetAsync may wait for a copy engine that a
+// caller's bulk transfers on other streams keep busy.
+__global__ void k_zero_u64(unsigned long long* __restrict__ u, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) u[i] = 0ull;
+}
+
+__global__ void k_publish_word(const unsigned long long* __restrict__ src, unsigned long long* dst) {
+  *(volatile unsigned long long*)dst = *src;
+  __threadfence_system();
+}
+
 __global__ void k_fix_to_rho(const unsigned long long* __restrict__ acc, double* __restrict__ rho, size_t n,
                              double scale, int add, unsigned long long* flag) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -722,8 +733,8 @@ int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
   }
   Level& L0 = c->lv[0];
   cudaStream_t s = c->stream;
-  WG_TRY_CUDA(cudaMemsetAsync(c->racc, 0, L0.nr * sizeof(unsigned long long), s));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dred + 3, 0, sizeof(unsigned long long), s));
+  { ++c->nlaunch; k_zero_u64<<<(unsigned)std::min<size_t>((L0.nr + 255) / 256, 148 * 16), 256, 0, s>>>(c->racc, L0.nr); }
+  { ++c->nlaunch; k_zero_u64<<<1, 32, 0, s>>>(c->dred + 3, 1); }
   GridP g = gridp(c);
   if (p->np > 0) {
     const int64_t maxblocks = 2147483647LL;
@@ -737,7 +748,8 @@ int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
   { ++c->nlaunch; k_fix_to_rho<<<cdiv64((int64_t)L0.nr, 256), 256, 0, s>>>(c->racc, c->rho, L0.nr, gg * kFixInv, zero_first ? 0 : 1,
                                                            c->dred + 3); }
   WG_TRY_CUDA(cudaGetLastError());
-  WG_TRY_CUDA(cudaMemcpyAsync(c->hred + 3, c->dred + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  { ++c->nlaunch; k_publish_word<<<1, 1, 0, s>>>(c->dred + 3, c->hred_dev + 3); }
+  WG_TRY_CUDA(cudaGetLastError());
   WG_TRY_CUDA(cudaStreamSynchronize(s));
   if (c->hred[3]) {
     set_error("wg_deposit: fixed-point charge accumulator above 2^62 at some node (more than 65536 full "
@@ -753,8 +765,10 @@ int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
 // flagged in dred[4] and reported by the next solve.
 int deposit_begin(wg_ctx* c) {
   cudaStream_t s = c->stream;
-  WG_TRY_CUDA(cudaMemsetAsync(c->racc, 0, c->lv[0].nr * sizeof(unsigned long long), s));
-  WG_TRY_CUDA(cudaMemsetAsync(c->dred + 4, 0, sizeof(unsigned long long), s));
+  const size_t nr = c->lv[0].nr;
+  { ++c->nlaunch; k_zero_u64<<<(unsigned)std::min<size_t>((nr + 255) / 256, 148 * 16), 256, 0, s>>>(c->racc, nr); }
+  { ++c->nlaunch; k_zero_u64<<<1, 32, 0, s>>>(c->dred + 4, 1); }
+  WG_TRY_CUDA(cudaGetLastError());
   c->dep_open = true;
   c->dep_gg_set = false;
   c->dep_gg = 0.;
