@@ -223,6 +223,21 @@ int wg_advance(wg_ctx* ctx, const wg_particles* p, const wg_push_params* prm);
  * 2 ybar, 3 xrms, 4 yrms, 5 epsx, 6 epsy (x' = ux/uz), 7 reserved. FP64,
  * deterministic order. */
 int wg_moments(wg_ctx* ctx, const wg_particles* p, double* out);
+/* The moment sums of getzmmnt, itask = 2 (top.F:814-860, 880-1160), for a
+ * non-relativistic species with ifzmmnt = 2: zmmnts0[33] over all live
+ * particles, and zmmnts[(nzmmnt+1)*33] (moment fastest) on the z grid of
+ * nzmmnt cells over [zmmntmin, zmmntmax) relative to zbeam. Each particle is
+ * extrapolated in time to the two planes around it, its velocity change
+ * taken from uxo/uyo/uzo (device arrays of the velocities dt earlier; the
+ * reference calls this in the synchv step with the pre-synchv velocities
+ * and dt = dt/2), and added to both with its linear weights times dtscale;
+ * the extrapolation time is clipped at zmmntdtextmax*dt. The moment index k
+ * is the reference's k+1. Sums are FP64 with atomic accumulation: they match
+ * the serial sums to rounding, not bit for bit. Output arrays are host
+ * memory; synchronizes the stream. */
+int wg_zmoments(wg_ctx* ctx, const wg_particles* p, const double* uxo, const double* uyo, const double* uzo,
+                double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt,
+                double zmmntdtextmax, double* zmmnts0, double* zmmnts);
 
 /* Cell keys for sorting particles by cell, as particlesortxyzwithcopy
  * (top.F:5095-5130): key = ix + (nx+1)*(iy + (ny+1)*iz); lost particles get

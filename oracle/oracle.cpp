@@ -1610,6 +1610,116 @@ void or_sete_cond(or_conductors* hc, int nx, int ny, int nz, double dx, double d
   });
 }
 
+// The moment sums of getzmmnt, itask = 2 (top.F:814-860 and 880-1160), for
+// a non-relativistic species (lrelativ false: the velocities are the u
+// themselves and the factors pp(13), pp(18) are 1) with ifzmmnt = 2. Lost particles (gaminv = 0) are
+// skipped. zmmnts0[33]: the global sums over all particles. zmmnts
+// [(nzmmnt+1)*33], moment fastest: each particle in [zmmntmin, zmmntmax)
+// (relative to zbeam) is extrapolated in time to the two z-grid planes
+// around it, with the velocity change between uo (the velocities dt earlier)
+// and u, and adds to both planes with its linear weights times dtscale.
+// The moment index k (0-based) is the reference's index k+1.
+void or_zmoments(int64_t np, const double* xp, const double* yp, const double* zp, const double* uxp,
+                 const double* uyp, const double* uzp, const double* gaminv, const double* uxpo, const double* uypo,
+                 const double* uzpo, double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax,
+                 int nzmmnt, double zmmntdtextmax, double* zmmnts0, double* zmmnts) {
+  const int NM = 33;
+  const double dzm = (zmmntmax - zmmntmin) / nzmmnt, dzmi = 1. / dzm;
+  const double oneondt = 1. / dt;
+  std::fill(zmmnts0, zmmnts0 + NM, 0.);
+  std::fill(zmmnts, zmmnts + (size_t)(nzmmnt + 1) * NM, 0.);
+  for (int64_t ip = 0; ip < np; ++ip) {
+    if (gaminv[ip] == 0.) continue;
+    const double x = xp[ip], y = yp[ip], z = zp[ip], ux = uxp[ip], uy = uyp[ip], uz = uzp[ip];
+    double vzi = 1. / (uz + SMALLPOS);
+    double* g = zmmnts0;
+    g[0] += 1.;
+    g[1] += x;
+    g[2] += y;
+    g[3] += z;
+    g[6] += ux;
+    g[7] += uy;
+    g[8] += uz;
+    g[9] += x * y;
+    g[11] += x * x;
+    g[12] += y * y;
+    g[13] += z * z;
+    g[16] += ux * ux;
+    g[17] += uy * uy;
+    g[18] += uz * uz;
+    g[21] += z * uz;
+    g[24] += x * uz;
+    g[25] += y * uz;
+    g[26] += ux * uz;
+    g[27] += uy * uz;
+    g[4] += ux * vzi;
+    g[5] += uy * vzi;
+    g[10] += ux * uy * (vzi * vzi);
+    g[14] += (ux * vzi) * (ux * vzi);
+    g[15] += (uy * vzi) * (uy * vzi);
+    g[19] += x * ux * vzi;
+    g[20] += y * uy * vzi;
+    g[22] += x * uy * vzi;
+    g[23] += y * ux * vzi;
+    g[28] += x * ux;
+    g[29] += y * uy;
+    g[30] += x * uy;
+    g[31] += y * ux;
+    g[32] += ux * uy;
+    if ((z - zbeam) < zmmntmin || (z - zbeam) >= zmmntmax) continue;
+    const double vzgi = 1. / (uz * gaminv[ip] + SMALLPOS);
+    int iz = (int)((z - zbeam - zmmntmin) * dzmi);
+    if (iz == nzmmnt) iz = nzmmnt - 1;
+    for (int side = 0; side < 2; ++side) {
+      double dtx = ((iz + side) * dzm - z + zbeam + zmmntmin) * vzgi;
+      dtx = std::max(-zmmntdtextmax * dt, std::min(zmmntdtextmax * dt, dtx));
+      const double px = ux * (1. + dtx * oneondt) - uxpo[ip] * dtx * oneondt;
+      const double py = uy * (1. + dtx * oneondt) - uypo[ip] * dtx * oneondt;
+      const double pz = uz * (1. + dtx * oneondt) - uzpo[ip] * dtx * oneondt;
+      const double qx = x + ux * dtx * gaminv[ip];
+      const double qy = y + uy * dtx * gaminv[ip];
+      const double qz = z + uz * dtx * gaminv[ip];
+      const double w = side == 0 ? (1. - (z - zbeam - zmmntmin) * dzmi + iz) * dtscale
+                                 : ((z - zbeam - zmmntmin) * dzmi - iz) * dtscale;
+      const double v = 1. / (pz + SMALLPOS);
+      double* m = zmmnts + (size_t)(iz + side) * NM;
+      m[0] += w;
+      m[1] += qx * w;
+      m[2] += qy * w;
+      m[3] += qz * w;
+      m[6] += px * w;
+      m[7] += py * w;
+      m[8] += pz * w;
+      m[9] += qx * qy * w;
+      m[11] += qx * qx * w;
+      m[12] += qy * qy * w;
+      m[13] += qz * qz * w;
+      m[16] += px * px * w;
+      m[17] += py * py * w;
+      m[18] += pz * pz * w;
+      m[21] += qz * pz * w;
+      m[24] += qx * pz * w;
+      m[25] += qy * pz * w;
+      m[26] += px * pz * w;
+      m[27] += py * pz * w;
+      m[4] += px * v * w;
+      m[5] += py * v * w;
+      m[10] += px * py * (v * v) * w;
+      m[14] += (px * v) * (px * v) * w;
+      m[15] += (py * v) * (py * v) * w;
+      m[19] += qx * px * v * w;
+      m[20] += qy * py * v * w;
+      m[22] += qx * py * v * w;
+      m[23] += qy * px * v * w;
+      m[28] += qx * px * w;
+      m[29] += qy * py * w;
+      m[30] += qx * py * w;
+      m[31] += qy * px * w;
+      m[32] += px * py * w;
+    }
+  }
+}
+
 // Global moments of the live particles (getzmmnt, top.F:521-1444). out[]:
 // 0 n, 1 xbar, 2 ybar, 3 xrms, 4 yrms, 5 epsx, 6 epsy (x' = ux/uz).
 void or_moments(int64_t np, const double* xp, const double* yp, const double* uxp, const double* uyp,

@@ -59,6 +59,7 @@ def lib():
         L.or_push.argtypes = [ctypes.c_int, ctypes.c_int64] + [_dp] * 10 + [ctypes.c_double] * 3 + [_dp] * 3 + \
             [ctypes.c_int] + [ctypes.c_double] * 7
         L.or_moments.argtypes = [ctypes.c_int64] + [_dp] * 6 + [_dp]
+        L.or_zmoments.argtypes = [ctypes.c_int64] + [_dp] * 10 + [ctypes.c_double] * 5 + [ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.or_sete_cond.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 3 + [ctypes.c_double] * 7 + \
             [_dp, ctypes.c_int64] + [_dp] * 6
         L.or_eps0.restype = ctypes.c_double
@@ -257,6 +258,19 @@ def push(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall, prwa
 def push_fullv(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall, prwallx=0.0, prwally=0.0):
     """The fullv advance of push()."""
     push(p, ex, ey, ez, q, m, dt, tables, zlmin, dzl, zmmin, zmmax, prwall, prwallx, prwally, "fullv")
+
+
+def zmoments(p, po, dt, zmmntmin, zmmntmax, nzmmnt, zbeam=0.0, dtscale=1.0, zmmntdtextmax=1e36):
+    """getzmmnt moment sums (itask = 2, ifzmmnt = 2): p holds the particles
+    (x, y, z, ux, uy, uz, gaminv), po the velocities ux, uy, uz a time dt
+    earlier. Returns (zmmnts0[33], zmmnts[nzmmnt+1, 33])."""
+    n = len(p["x"])
+    z0 = np.zeros(33)
+    zm = np.zeros((nzmmnt + 1, 33))
+    lib().or_zmoments(n, *(_d(p[k]) for k in ("x", "y", "z", "ux", "uy", "uz", "gaminv")),
+                      *(_d(po[k]) for k in ("ux", "uy", "uz")), dt, dtscale, zbeam, zmmntmin, zmmntmax, nzmmnt,
+                      zmmntdtextmax, _d(z0), _d(zm))
+    return z0, zm
 
 
 def moments(p):

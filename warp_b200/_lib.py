@@ -89,6 +89,7 @@ SIGNATURES = {
     "wg_set_lattice": [_vp, _dp, _dp, _dp, _c.c_int, _c.c_double, _c.c_double],
     "wg_advance": [_vp, ctypes.POINTER(Particles), ctypes.POINTER(PushParams)],
     "wg_set_correctede": [_vp, _c.c_int],
+    "wg_zmoments": [_vp, ctypes.POINTER(Particles), _vp, _vp, _vp] + [_c.c_double] * 5 + [_c.c_int, _c.c_double, _dp, _dp],
     "wg_deposit_begin": [_vp],
     "wg_deposit_add": [_vp, ctypes.POINTER(Particles)],
     "wg_deposit_end": [_vp, _c.c_int],

@@ -30,6 +30,9 @@ int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double
             int64_t np);
 int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm);
 int moments(wg_ctx* c, const wg_particles* p, double* out);
+int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* uyo, const double* uzo, double dt,
+             double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt, double zmmntdtextmax,
+             double* zmmnts0, double* zmmnts);
 int moments_scratch_doubles(int nb);
 int configure_kernels();
 
@@ -205,6 +208,7 @@ void free_all(wg_ctx* c) {
   dfree(c->dslot);
   dfree(c->dmom);
   dfree(c->dese);
+  dfree(c->zmom);
   dfree(c->czs);
   dfree(c->cze);
   dfree(c->cdb);
@@ -569,6 +573,13 @@ int wg_set_correctede(wg_ctx* c, int on) {
 int wg_advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
   if (!c) { set_error("null context"); return WG_EINVAL; }
   return advance(c, p, prm);
+}
+
+int wg_zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* uyo, const double* uzo, double dt,
+                double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt, double zmmntdtextmax,
+                double* zmmnts0, double* zmmnts) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return zmoments(c, p, uxo, uyo, uzo, dt, dtscale, zbeam, zmmntmin, zmmntmax, nzmmnt, zmmntdtextmax, zmmnts0, zmmnts);
 }
 
 int wg_moments(wg_ctx* c, const wg_particles* p, double* out) {

@@ -132,6 +132,8 @@ struct wg_ctx {
   unsigned long long* hred_dev = nullptr;  // device address of hred
   double* dmom = nullptr;              // moment partial sums
   double* dese = nullptr;              // field-energy row sums ((nx+1)(ny+1) + 1)
+  double* zmom = nullptr;              // z-moment sums (33 global, then 33 per plane)
+  size_t zmom_n = 0;
   int mom_blocks = 0;
   // lattice tables
   double* czs = nullptr;

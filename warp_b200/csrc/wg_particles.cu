@@ -656,6 +656,145 @@ __global__ void k_permute(const int64_t* __restrict__ perm, int64_t np, wg_parti
   dst.gaminv[i] = src.gaminv[j];
 }
 
+// ---- z moments (getzmmnt, itask = 2, ifzmmnt = 2) --------------------------
+
+constexpr int kZM = 33;              // moments per sum (the reference's NUMZMMNT)
+constexpr int kZMSmemPlanes = 640;   // planes kept in shared memory (168 KB)
+
+struct ZMomP {
+  double dt, oneondt, dtscale, zbeam, zmmntmin, zmmntmax, dzm, dzmi, dtmax;
+  int nzmmnt;
+};
+
+// The 33 moment contributions of one particle state (reference indices
+// k+1), non-relativistic branch. For the global sums pass w = 1 and the
+// unextrapolated state; vz is the value the velocity ratios divide by.
+__device__ __forceinline__ void zm_terms(double qx, double qy, double qz, double px, double py, double pz,
+                                         double w, double* m) {
+  const double v = 1. / (pz + 1.0e-36);
+  m[0] = w;
+  m[1] = qx * w;
+  m[2] = qy * w;
+  m[3] = qz * w;
+  m[6] = px * w;
+  m[7] = py * w;
+  m[8] = pz * w;
+  m[9] = qx * qy * w;
+  m[11] = qx * qx * w;
+  m[12] = qy * qy * w;
+  m[13] = qz * qz * w;
+  m[16] = px * px * w;
+  m[17] = py * py * w;
+  m[18] = pz * pz * w;
+  m[21] = qz * pz * w;
+  m[24] = qx * pz * w;
+  m[25] = qy * pz * w;
+  m[26] = px * pz * w;
+  m[27] = py * pz * w;
+  m[4] = px * v * w;
+  m[5] = py * v * w;
+  m[10] = px * py * (v * v) * w;
+  m[14] = (px * v) * (px * v) * w;
+  m[15] = (py * v) * (py * v) * w;
+  m[19] = qx * px * v * w;
+  m[20] = qy * py * v * w;
+  m[22] = qx * py * v * w;
+  m[23] = qy * px * v * w;
+  m[28] = qx * px * w;
+  m[29] = qy * py * w;
+  m[30] = qx * py * w;
+  m[31] = qy * px * w;
+  m[32] = px * py * w;
+}
+
+__device__ __forceinline__ void zm_add(double* dst, const double* m, bool warp_uniform, bool lead) {
+  if (warp_uniform) {
+#pragma unroll
+    for (int k = 0; k < kZM; ++k) {
+      double v = m[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lead) atomicAdd(dst + k, v);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kZM; ++k) atomicAdd(dst + k, m[k]);
+  }
+}
+
+// Sums over the live particles: the global sums (g, 33) and the two-plane
+// extrapolated sums on the z grid (zm, (nzmmnt+1) x 33), accumulated in
+// shared memory when the grid fits there, then added to the outputs. The
+// floating-point addition order is not fixed, so the sums agree with the
+// serial ones to rounding, not bit for bit.
+__global__ void __launch_bounds__(256) k_zmoments(const double* __restrict__ xp, const double* __restrict__ yp,
+                                                  const double* __restrict__ zp, const double* __restrict__ uxp,
+                                                  const double* __restrict__ uyp, const double* __restrict__ uzp,
+                                                  const double* __restrict__ gaminv, const double* __restrict__ uxo,
+                                                  const double* __restrict__ uyo, const double* __restrict__ uzo,
+                                                  int64_t np, ZMomP P, double* __restrict__ g_out,
+                                                  double* __restrict__ zm_out) {
+  extern __shared__ double sh[];
+  const bool in_smem = P.nzmmnt + 1 <= kZMSmemPlanes;
+  double* gs = sh;
+  double* zs = in_smem ? sh + kZM : zm_out;
+  const int nsh = kZM + (in_smem ? (P.nzmmnt + 1) * kZM : 0);
+  for (int i = threadIdx.x; i < nsh; i += blockDim.x) sh[i] = 0.;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nround = (np + stride - 1) / stride;
+  for (int64_t r = 0; r < nround; ++r) {
+    const int64_t i = r * stride + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < np && gaminv[i] != 0.;
+    double x = 0., y = 0., z = 0., ux = 0., uy = 0., uz = 1., gi = 0.;
+    if (live) {
+      x = xp[i];
+      y = yp[i];
+      z = zp[i];
+      ux = uxp[i];
+      uy = uyp[i];
+      uz = uzp[i];
+      gi = gaminv[i];
+    }
+    double m[kZM];
+    // global sums: the unextrapolated state, weight 1
+    zm_terms(x, y, z, ux, uy, uz, live ? 1. : 0., m);
+    const unsigned all = __ballot_sync(0xffffffffu, true);
+    zm_add(gs, m, all == 0xffffffffu, lane == 0);
+    // z grid
+    const double zr = z - P.zbeam;
+    const bool in = live && !(zr < P.zmmntmin || zr >= P.zmmntmax);
+    int iz = -1;
+    if (in) {
+      iz = (int)((z - P.zbeam - P.zmmntmin) * P.dzmi);
+      if (iz == P.nzmmnt) iz = P.nzmmnt - 1;
+    }
+    const int iz0 = __shfl_sync(0xffffffffu, iz, 0);
+    const bool uniform = __all_sync(0xffffffffu, in && iz == iz0);
+    if (!uniform && !in) continue;
+    const double vzgi = 1. / (uz * gi + 1.0e-36);
+    const double ux_o = in ? uxo[i] : 0., uy_o = in ? uyo[i] : 0., uz_o = in ? uzo[i] : 0.;
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+      double dtx = ((iz + side) * P.dzm - z + P.zbeam + P.zmmntmin) * vzgi;
+      dtx = fmax(-P.dtmax * P.dt, fmin(P.dtmax * P.dt, dtx));
+      const double px = ux * (1. + dtx * P.oneondt) - ux_o * dtx * P.oneondt;
+      const double py = uy * (1. + dtx * P.oneondt) - uy_o * dtx * P.oneondt;
+      const double pz = uz * (1. + dtx * P.oneondt) - uz_o * dtx * P.oneondt;
+      const double qx = x + ux * dtx * gi, qy = y + uy * dtx * gi, qz = z + uz * dtx * gi;
+      const double w = side == 0 ? (1. - (z - P.zbeam - P.zmmntmin) * P.dzmi + iz) * P.dtscale
+                                 : ((z - P.zbeam - P.zmmntmin) * P.dzmi - iz) * P.dtscale;
+      zm_terms(qx, qy, qz, px, py, pz, w, m);
+      zm_add(zs + (size_t)(iz + side) * kZM, m, uniform, lane == 0);
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < kZM; k += blockDim.x) atomicAdd(g_out + k, gs[k]);
+  if (in_smem)
+    for (int k = threadIdx.x; k < (P.nzmmnt + 1) * kZM; k += blockDim.x) atomicAdd(zm_out + k, zs[k]);
+}
+
 constexpr int kMomN = 11;
 
 // Per-block partial sums of the moments of live particles (getzmmnt,
@@ -922,6 +1061,54 @@ int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
   { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, ce, p->x, p->y, p->z, p->ux, p->uy,
                                                   p->uz, p->gaminv, p->np); c->prof_end(pe); }
   WG_TRY_CUDA(cudaGetLastError());
+  return WG_OK;
+}
+
+int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* uyo, const double* uzo, double dt,
+             double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt, double zmmntdtextmax,
+             double* zmmnts0, double* zmmnts) {
+  if (!p || p->np < 0 || !zmmnts0 || !zmmnts ||
+      (p->np > 0 && (!p->x || !p->y || !p->z || !p->ux || !p->uy || !p->uz || !p->gaminv || !uxo || !uyo || !uzo))) {
+    set_error("wg_zmoments: null arguments");
+    return WG_EINVAL;
+  }
+  if (nzmmnt < 1 || !(zmmntmax > zmmntmin) || !(dt > 0.)) {
+    set_error("wg_zmoments: need nzmmnt >= 1, zmmntmax > zmmntmin and dt > 0");
+    return WG_EINVAL;
+  }
+  const size_t n = (size_t)(nzmmnt + 2) * kZM;
+  if (c->zmom_n < n) {
+    if (c->zmom) cudaFree(c->zmom);
+    c->zmom = nullptr;
+    c->zmom_n = 0;
+    WG_TRY_CUDA(cudaMalloc((void**)&c->zmom, n * sizeof(double)));
+    c->zmom_n = n;
+  }
+  cudaStream_t s = c->stream;
+  WG_TRY_CUDA(cudaMemsetAsync(c->zmom, 0, n * sizeof(double), s));
+  ZMomP P;
+  P.dt = dt;
+  P.oneondt = 1. / dt;
+  P.dtscale = dtscale;
+  P.zbeam = zbeam;
+  P.zmmntmin = zmmntmin;
+  P.zmmntmax = zmmntmax;
+  P.dzm = (zmmntmax - zmmntmin) / nzmmnt;
+  P.dzmi = 1. / P.dzm;
+  P.dtmax = zmmntdtextmax;
+  P.nzmmnt = nzmmnt;
+  if (p->np > 0) {
+    const bool in_smem = nzmmnt + 1 <= kZMSmemPlanes;
+    const size_t smem = (size_t)(kZM + (in_smem ? (nzmmnt + 1) * kZM : 0)) * sizeof(double);
+    WG_TRY_CUDA(cudaFuncSetAttribute(k_zmoments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const unsigned blocks = in_smem ? 148u : 592u;
+    { ++c->nlaunch; k_zmoments<<<blocks, 256, smem, s>>>(p->x, p->y, p->z, p->ux, p->uy, p->uz, p->gaminv, uxo, uyo, uzo, p->np, P, c->zmom, c->zmom + kZM); }
+    WG_TRY_CUDA(cudaGetLastError());
+  }
+  WG_TRY_CUDA(cudaMemcpyAsync(zmmnts0, c->zmom, kZM * sizeof(double), cudaMemcpyDeviceToHost, s));
+  WG_TRY_CUDA(cudaMemcpyAsync(zmmnts, c->zmom + kZM, (size_t)(nzmmnt + 1) * kZM * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  WG_TRY_CUDA(cudaStreamSynchronize(s));
   return WG_OK;
 }
 

@@ -389,6 +389,23 @@ class MultiGridB200(FieldSolver):
                             int(self._lattice is not None), _lib.CENTERS[center])
         _lib.check(_lib.lib.wg_advance(self._h, ctypes.byref(s), ctypes.byref(p)))
 
+    def zmoments(self, pgroup, uold, dt, zmmntmin, zmmntmax, nzmmnt, zbeam=0., dtscale=1., zmmntdtextmax=1e36):
+        """The moment sums of getzmmnt (wg_zmoments): returns zmmnts0 (33,)
+        over all live particles and zmmnts (nzmmnt+1, 33) on the z grid.
+        uold is a triple of device arrays with the velocities dt earlier (the
+        reference takes them before the synchv half step, with dt = dt/2).
+        warp_b200.diagnostics.finalize turns the sums into moments."""
+        self._bind_stream()
+        s = pgroup.cstruct()
+        z0 = np.zeros(33)
+        zm = np.zeros((int(nzmmnt) + 1, 33))
+        dp = ctypes.POINTER(ctypes.c_double)
+        uo = [ctypes.c_void_p(u.data_ptr()) for u in uold]
+        _lib.check(_lib.lib.wg_zmoments(self._h, ctypes.byref(s), uo[0], uo[1], uo[2], float(dt), float(dtscale),
+                                        float(zbeam), float(zmmntmin), float(zmmntmax), int(nzmmnt),
+                                        float(zmmntdtextmax), z0.ctypes.data_as(dp), zm.ctypes.data_as(dp)))
+        return z0, zm
+
     def moments(self, pgroup):
         """Global moments of live particles: dict n, xbar, ybar, xrms, yrms,
         epsx, epsy (getzmmnt, top.F:521-1444)."""

@@ -197,14 +197,39 @@ class ESPIC:
             self.it += 1
         main.wait_stream(d2h)
 
-    def synchv(self):
+    def synchv(self, nzmmnt=0, zmmntmin=None, zmmntmax=None):
         """padvnc3d("synchv") at the end of a special step (w3d.F:975): a
         half kick with the field of the last solve takes the velocities from
         t - dt/2 to t, where the positions are. The next step is then halfv.
-        Does nothing when the velocities are already in step."""
-        if not self.vsync:
-            self.solver.advance(self.pgroup, self.dt, prwall=self.cfg["pipe_radius"], center="synchv")
-            self.vsync = True
+        Does nothing when the velocities are already in step.
+
+        With nzmmnt > 0 it also takes the moments of that step, as the
+        synchv call of getzmmnt does (w3d.F:2327-2345): the moments on a z
+        grid of nzmmnt cells over [zmmntmin, zmmntmax) (default the field
+        grid) with each particle extrapolated in time using its velocity
+        change over the half step, and the global moments. The moments
+        (diagnostics.finalize, keys as the reference's pnum, xrms, epsx,
+        pnumz, xrmsz, epsxz, ...) are appended to self.history with the step
+        number and time, and returned."""
+        if self.vsync:
+            return None
+        pg = self.pgroup
+        uold = (pg.ux.clone(), pg.uy.clone(), pg.uz.clone()) if nzmmnt > 0 else None
+        self.solver.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], center="synchv")
+        self.vsync = True
+        if not nzmmnt:
+            return None
+        from .diagnostics import finalize
+        zmin = self.cfg["zmmin"] if zmmntmin is None else zmmntmin
+        zmax = self.cfg["zmmax"] if zmmntmax is None else zmmntmax
+        z0, zm = self.solver.zmoments(pg, uold, 0.5 * self.dt, zmin, zmax, nzmmnt)
+        out = {"it": self.it, "time": self.it * self.dt}
+        out.update(finalize(z0))
+        out.update(finalize(zm, "z"))
+        if not hasattr(self, "history"):
+            self.history = []
+        self.history.append(out)
+        return out
 
     def moments(self):
         """Moments of the particles as they are; call synchv() first for
