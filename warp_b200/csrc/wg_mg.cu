@@ -893,6 +893,87 @@ __global__ void __launch_bounds__(256) k_restrict(const T* __restrict__ res, T* 
 // consecutive fine planes per thread, all loads issued before the sums;
 // 32-bit offsets. The weight products keep the reference's left-to-right
 // order, ((wx' * wy') * wz') * q, with the x-y part formed once per thread.
+// restrict3d for a coarse level whose z is not coarsened (nzc == nz). The
+// z window of a coarse plane is the fine plane itself with weight exactly 1,
+// so each tap weight is (wx * wy) * 1 = wx * wy, and the sums below are the
+// generic kernel's, operation for operation. The x-y weights and their sum
+// are formed once and serve ZPT coarse planes per thread.
+template <typename T, int NT, int ZPT>
+__global__ void __launch_bounds__(256) k_restrict_xy(const T* __restrict__ res, T* __restrict__ rhoc, int nx, int ny,
+                                                     int nxc, int nyc, int nzc, int ixcmin, int ixcmax, int iycmin,
+                                                     int iycmax, int izcmin, int izcmax,
+                                                     const int32_t* __restrict__ tlo, const int32_t* __restrict__ tn,
+                                                     const double* __restrict__ tw, double ff) {
+  pdl_entry();
+  const int ixc = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iyc = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int izc0 = (int)blockIdx.z * ZPT;
+  if (ixc > nxc || iyc > nyc) return;
+  const bool xyin = ixc >= ixcmin && ixc <= ixcmax && iyc >= iycmin && iyc <= iycmax;
+  const int ox = ixc, oy = nxc + 1 + iyc;
+  int lx = 0, ly = 0, cx = 0, cy = 0;
+  T wxy[NT][NT];
+  T w = (T)0.;
+  if (xyin) {
+    lx = tlo[ox];
+    ly = tlo[oy];
+    cx = tn[ox];
+    cy = tn[oy];
+#pragma unroll
+    for (int ky = 0; ky < NT; ++ky)
+#pragma unroll
+      for (int kx = 0; kx < NT; ++kx) wxy[ky][kx] = (T)tw[ox * kRestrictTaps + kx] * (T)tw[oy * kRestrictTaps + ky];
+#pragma unroll
+    for (int ky = 0; ky < NT; ++ky) {
+      if (ky >= cy) break;
+#pragma unroll
+      for (int kx = 0; kx < NT; ++kx) {
+        if (kx >= cx) break;
+        w = w + wxy[ky][kx];
+      }
+    }
+  }
+  const int sy = nx + 3, sz = sy * (ny + 3);
+  const int b0 = (lx + 1) + sy * (ly + 1);
+  T v[ZPT][NT][NT];
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k) {
+    const int izc = izc0 + k;
+    const bool in = xyin && izc >= izcmin && izc <= izcmax;
+    const T* plane = res + (b0 + sz * (izc + 1));
+#pragma unroll
+    for (int ky = 0; ky < NT; ++ky)
+#pragma unroll
+      for (int kx = 0; kx < NT; ++kx) v[k][ky][kx] = (in && ky < cy && kx < cx) ? plane[ky * sy + kx] : (T)0.;
+  }
+#pragma unroll
+  for (int k = 0; k < ZPT; ++k) {
+    const int izc = izc0 + k;
+    if (izc > nzc) break;
+    const int o = ixc + (nxc + 1) * (iyc + (nyc + 1) * izc);
+    if (!xyin || izc < izcmin || izc > izcmax) {
+      rhoc[o] = (T)0.;
+      continue;
+    }
+    T r = (T)0.;
+#pragma unroll
+    for (int ky = 0; ky < NT; ++ky) {
+      if (ky >= cy) break;
+#pragma unroll
+      for (int kx = 0; kx < NT; ++kx) {
+        if (kx >= cx) break;
+        r = r + wxy[ky][kx] * v[k][ky][kx];
+      }
+    }
+    if (w > (T)0.) {
+      r = r / w;
+      rhoc[o] = r * (T)ff;
+    } else {
+      rhoc[o] = (T)0.;
+    }
+  }
+}
+
 template <typename T, int ZPT, bool ZC>
 __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __restrict__ pc, int nx, int ny,
                                                 int nxc, int nyc, int ixmin, int ixmax, int iymin, int iymax,
@@ -919,8 +1000,10 @@ __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __
     const int iz = iz0 + k;
     ok[k] = iz <= izmax;
     if (ok[k]) {
-      const int jz = ej[oz + iz + 1];
-      wz[k] = (T)ew[oz + iz + 1];
+      // z not coarsened: the coarse plane is the fine plane and its weight
+      // is exactly 0, so the tables need not be read
+      const int jz = ZC ? ej[oz + iz + 1] : iz;
+      wz[k] = ZC ? (T)ew[oz + iz + 1] : (T)0.;
       const T* b = pc + (cxy + szc * (jz + 1));
       q[k][0] = b[0];
       q[k][1] = b[1];
@@ -942,8 +1025,8 @@ __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __
     if (ZC)
       phi[f0 + k * sz] = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3] +
                          a00 * z * q[k][4] + a10 * z * q[k][5] + a01 * z * q[k][6] + a11 * z * q[k][7];
-    else  // z not coarsened: wz = 0 exactly, the z+1 terms add zeros
-      phi[f0 + k * sz] = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3];
+    else  // z not coarsened: wz = 0 and z1 = 1 exactly, the z+1 terms add zeros
+      phi[f0 + k * sz] = f[k] + a00 * q[k][0] + a10 * q[k][1] + a01 * q[k][2] + a11 * q[k][3];
   }
 }
 
@@ -1298,13 +1381,20 @@ struct Solver {
       Ranges Rc = ranges(dc, B.b, false);
       dim3 blk(32, 8), grd(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), dc.nz + 1);
       int pr = prof_begin(l, WG_PROF_RESTRICT0, (double)L.nr);
-      if (L.rmax <= 3)
+      if (dc.nz == d.nz && L.rmax <= 3) {
+        // z not coarsened: x-y windows only, several coarse planes per thread
+        constexpr int zpt = ZPlanes<T>::value;
+        dim3 grdxy(cdiv(dc.nx + 1, 32), cdiv(dc.ny + 1, 8), cdiv(dc.nz + 1, zpt));
+        launch(k_restrict_xy<T, 3, zpt>, grdxy, blk, 0, Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny,
+               dc.nz, Rc.ixmin, Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax, L.rlo, L.rn, L.rw, ff);
+      } else if (L.rmax <= 3) {
         launch(k_restrict<T, 3>, grd, blk, 0, Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny, Rc.ixmin,
                                              Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax, L.rlo, L.rn, L.rw, ff);
-      else
+      } else {
         launch(k_restrict<T, kRestrictTaps>, grd, blk, 0, Arr<T>::res(L), Arr<T>::rhs(Lc), d.nx, d.ny, dc.nx, dc.ny,
                                                          Rc.ixmin, Rc.ixmax, Rc.iymin, Rc.iymax, Rc.izmin, Rc.izmax,
                                                          L.rlo, L.rn, L.rw, ff);
+      }
       c->prof_end(pr);
       box<T>(l + 1);
       zero(Arr<T>::phi(Lc), Lc.np);
