@@ -698,18 +698,20 @@ __global__ void __launch_bounds__(FNT, 3) k_sor_fused(FusedArgs<T> a) {
 // Six blocks per SM (40 registers): the kernel is bound by memory latency, and
 // the extra resident warps took the FP32 residual of the finest 256x256x512
 // level from 187 to 167 us on the B200.
+// The bulk residual for the thread's node column of block (bx, by, bz).
+// keep_sub: leave subgrid-point nodes unwritten (a merged kernel's
+// subgrid blocks write them).
 template <typename T, int MODE, typename TO, int ZPT>
-__global__ void __launch_bounds__(256, 6) k_residual(const T* __restrict__ phi, const T* __restrict__ rhs,
-                                                  TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
-                                                  int ixmax, int iymin, int iymax, int izmin, int izmax, T cx, T cy,
-                                                  T cz, T mgparam, unsigned long long* maxout) {
-  pdl_entry();
+__device__ __forceinline__ void residual_bulk(const T* __restrict__ phi, const T* __restrict__ rhs,
+                                              TO* __restrict__ out, int nx, int ny, int nz, int ixmin, int ixmax,
+                                              int iymin, int iymax, int izmin, int izmax, T cx, T cy, T cz, T mgparam,
+                                              int bx, int by, int bz, bool keep_sub, T& m) {
   // MODE 0 covers the padded array, the others the node array; ZPT planes
   // per thread with all loads issued first; 32-bit offsets
   const int g = (MODE == 0) ? 1 : 0;
-  const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x) - g;
-  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y) - g;
-  const int iz0 = (int)blockIdx.z * ZPT - g;
+  const int ix = (int)(bx * blockDim.x + threadIdx.x) - g;
+  const int iy = (int)(by * blockDim.y + threadIdx.y) - g;
+  const int iz0 = bz * ZPT - g;
   const bool live = ix <= nx + g && iy <= ny + g;
   const bool xyin = ix >= ixmin && ix <= ixmax && iy >= iymin && iy <= iymax;
   const int sy = nx + 3, sz = sy * (ny + 3), ry = nx + 1, rz = ry * (ny + 1);
@@ -733,29 +735,42 @@ __global__ void __launch_bounds__(256, 6) k_residual(const T* __restrict__ phi, 
       zp[k] = phi[p + sz];
     }
   }
-  T m = (T)0.;
 #pragma unroll
   for (int k = 0; k < ZPT; ++k) {
     if (!live || iz0 + k > nz + g) continue;
     T r = (T)0.;
-    if (in[k] && !isbox(b[k])) {
-      r = b[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz - c[k] * mgparam;
-      m = fmax(m, fabs(r));
+    if (in[k]) {
+      if (!isbox(b[k])) {
+        r = b[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz - c[k] * mgparam;
+        m = fmax(m, fabs(r));
+      } else if (keep_sub && !Box<T>::interior(b[k])) {
+        continue;
+      }
     }
     if (MODE == 0) out[p0 + k * sz] = (TO)r;
     if (MODE == 2) out[q0 + k * rz] = (TO)r;
   }
+}
+
+template <typename T, int MODE, typename TO, int ZPT>
+__global__ void __launch_bounds__(256, 6) k_residual(const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                  TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
+                                                  int ixmax, int iymin, int iymax, int izmin, int izmax, T cx, T cy,
+                                                  T cz, T mgparam, unsigned long long* maxout) {
+  pdl_entry();
+  T m = (T)0.;
+  residual_bulk<T, MODE, TO, ZPT>(phi, rhs, out, nx, ny, nz, ixmin, ixmax, iymin, iymax, izmin, izmax, cx, cy, cz,
+                                  mgparam, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, false, m);
   if (maxout) block_max_to(maxout, (double)m);
 }
 
 // cond_potmgres (interior -> 0, f3d_mgrid.F:2472-2500) and condbndyres
 // (icndbndy = 2, f3d_mgrid.F:3240-3362) for both colours.
 template <typename T, int MODE, typename TO>
-__global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, int nx, int ny, int nz, CondArgs<T> C,
-                              Bnd B, double dxsqi, double dysqi, double dzsqi, double mgparam_d, int voltfac_on,
-                              int mgform2init, int lcndbndy, unsigned long long* maxout) {
-  pdl_entry();
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double special_res_point(const T* __restrict__ phi, TO* __restrict__ out, int nx, int ny,
+                                                    int nz, const CondArgs<T>& C, const Bnd& B, double dxsqi,
+                                                    double dysqi, double dzsqi, double mgparam_d, int voltfac_on,
+                                                    int mgform2init, int lcndbndy, int i) {
   double m = 0.;
   auto store = [&](int ix, int iy, int iz, T v) {
     if (MODE == 0) out[pix(nx, ny, ix, iy, iz)] = (TO)v;
@@ -824,7 +839,47 @@ __global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, i
       }
     }
   }
+  return m;
+}
+
+template <typename T, int MODE, typename TO>
+__global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, int nx, int ny, int nz, CondArgs<T> C,
+                              Bnd B, double dxsqi, double dysqi, double dzsqi, double mgparam_d, int voltfac_on,
+                              int mgform2init, int lcndbndy, unsigned long long* maxout) {
+  pdl_entry();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double m = special_res_point<T, MODE, TO>(phi, out, nx, ny, nz, C, B, dxsqi, dysqi, dzsqi, mgparam_d,
+                                                  voltfac_on, mgform2init, lcndbndy, i);
   if (maxout) block_max_to(maxout, m);
+}
+
+// The residual of a level without Neumann-type subgrid points in one launch:
+// the first nspz z-slices of blocks compute the subgrid points
+// (k_special_res), the others the bulk, which leaves those nodes unwritten.
+template <typename T, int MODE, typename TO, int ZPT>
+__global__ void __launch_bounds__(256) k_residual_sp(const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                     TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
+                                                     int ixmax, int iymin, int iymax, int izmin, int izmax, T cx,
+                                                     T cy, T cz, T mgparam, int nbz, CondArgs<T> C, Bnd B,
+                                                     double dxsqi, double dysqi, double dzsqi, double mgparam_d,
+                                                     int voltfac_on, int mgform2init, int lcndbndy,
+                                                     unsigned long long* maxout) {
+  pdl_entry();
+  const int nspz = (int)gridDim.z - nbz;
+  double md;
+  if ((int)blockIdx.z < nspz) {
+    const int i = (((int)blockIdx.z * (int)gridDim.y + (int)blockIdx.y) * (int)gridDim.x + (int)blockIdx.x) *
+                      (int)(blockDim.x * blockDim.y) +
+                  (int)(threadIdx.y * blockDim.x + threadIdx.x);
+    md = special_res_point<T, MODE, TO>(phi, out, nx, ny, nz, C, B, dxsqi, dysqi, dzsqi, mgparam_d, voltfac_on,
+                                        mgform2init, lcndbndy, i);
+  } else {
+    T m = (T)0.;
+    residual_bulk<T, MODE, TO, ZPT>(phi, rhs, out, nx, ny, nz, ixmin, ixmax, iymin, iymax, izmin, izmax, cx, cy,
+                                    cz, mgparam, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z - nspz, true, m);
+    md = (double)m;
+  }
+  if (maxout) block_max_to(maxout, md);
 }
 
 // restrict3d (f3d_mgrid.F:1593-1775): one thread per coarse node, summing
@@ -1256,7 +1311,7 @@ struct Solver {
 
   // sorpass3d (f3d_mgrid.F:1949-2093)
   template <typename T>
-  void sorpass(int l, bool usev) {
+  void sorpass(int l, bool usev, bool phi_zero = false) {
     Level& L = c->lv[l];
     const SorCoef k = coef(L.d);
     if (fused_ok && !L.has_neumann_sub) {
@@ -1293,7 +1348,9 @@ struct Solver {
     const bool zper = b[4] == 2 && b[5] == 2, zdir = b[4] == 0 && b[5] == 0;
     const bool merged = !L.has_neumann_sub && xy_dir && (zper || zdir) && L.d.nz >= 2;
     const int wtz = (merged && zper) ? 1 : 0;
-    if (L.n_int) {
+    // cond_potmg sets the interior nodes to their voltage or, below the
+    // finest level, to 0: a no-op on a phi that was just zeroed
+    if (L.n_int && !(phi_zero && !usev)) {
       launch(k_interior<T>, cdiv(L.n_int, 128), 128, 0, phi, L.d.nx, L.d.ny, L.int_ijk, L.int_volt, L.n_int, usev,
                                                         L.d.nz, wtz);
     }
@@ -1344,6 +1401,23 @@ struct Solver {
     const int g = (MODE == 0) ? 1 : 0;
     constexpr int zpt = ZPlanes<T>::value;
     dim3 blk(32, 8), grd(cdiv(L.d.nx + 1 + 2 * g, 32), cdiv(L.d.ny + 1 + 2 * g, 8), cdiv(L.d.nz + 1 + 2 * g, zpt));
+    // interior conductor nodes are boxed, so the bulk kernel already stored
+    // their zero residual
+    CondArgs<T> ca = cond_args<T>(L);
+    ca.nint = 0;
+    int n = L.sub[0].n + L.sub[1].n;
+    if (sizeof(T) == 4 && l > 0 && MODE == 0 && n && !L.has_neumann_sub) {
+      // FP32, below the finest level: bulk and subgrid points in one launch
+      // (the FP64 form of the merged kernel needs 76 registers and is slower)
+      const int nbz = (int)grd.z;
+      const int nspz = (int)cdiv((size_t)n, 256u * grd.x * grd.y);
+      launch(k_residual_sp<T, MODE, TO, zpt>, dim3(grd.x, grd.y, nbz + nspz), blk, 0, phi, rhs, out, L.d.nx, L.d.ny,
+             L.d.nz, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
+             (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst), (T)o->mgparam, nbz, ca, B, dxsqi, dysqi,
+             dzsqi, o->mgparam, (int)voltfac_on, (int)mgform2init, o->lcndbndy, maxout);
+      bc<TO>(L, (TO*)out, false);
+      return;
+    }
     {
       int pe = prof_begin(l, WG_PROF_RESID0, (double)L.nr);
       launch(k_residual<T, MODE, TO, zpt>, grd, blk, 0, phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
@@ -1352,11 +1426,6 @@ struct Solver {
                                                   (T)o->mgparam, maxout);
       c->prof_end(pe);
     }
-    // interior conductor nodes are boxed, so the bulk kernel already stored
-    // their zero residual
-    CondArgs<T> ca = cond_args<T>(L);
-    ca.nint = 0;
-    int n = L.sub[0].n + L.sub[1].n;
     if (n) {
       launch(k_special_res<T, MODE, TO>, cdiv(n, 128), 128, 0, phi, out, L.d.nx, L.d.ny, L.d.nz, ca, B,
                                                               dxsqi, dysqi, dzsqi, o->mgparam, (int)voltfac_on,
@@ -1367,9 +1436,10 @@ struct Solver {
 
   // vcycle (f3d_mgrid.F:1101-1591)
   template <typename T>
-  void vcycle(int l, bool usev) {
+  // phi_zero: phi of level l is all zeros on entry
+  void vcycle(int l, bool usev, bool phi_zero = false) {
     Level& L = c->lv[l];
-    for (int i = 0; i < o->downpasses; ++i) sorpass<T>(l, usev);
+    for (int i = 0; i < o->downpasses; ++i) sorpass<T>(l, usev, phi_zero && i == 0);
     const LevelDims& d = L.d;
     if (d.nx >= 4 && d.ny >= 4 && d.nz >= 4 && l < o->mgmaxlevels && l + 1 < (int)c->lv.size()) {
       residual<T, 0, T>(l, Arr<T>::phi(L), Arr<T>::res(L), false, usev, nullptr);
@@ -1399,7 +1469,7 @@ struct Solver {
       box<T>(l + 1);
       zero(Arr<T>::phi(Lc), Lc.np);
       int pc = (l == 0) ? prof_begin(0, WG_PROF_COARSE, (double)Lc.nr) : -1;
-      vcycle<T>(l + 1, false);
+      vcycle<T>(l + 1, false, true);
       c->prof_end(pc);
       expand<T>(l);
       bc<T>(L, Arr<T>::phi(L), false);
@@ -1532,7 +1602,7 @@ int run_vcycle(Solver& S, bool usev) {
   wg_ctx* c = S.c;
   const wg_solve_opts* o = S.o;
   if (!(o->flags & WG_SOLVE_GRAPH) || c->prof_mask) {
-    S.vcycle<T>(0, usev);
+    S.vcycle<T>(0, usev, !usev);
     return WG_OK;
   }
   const int gi = sizeof(T) == 8 ? 0 : 1;
@@ -1553,7 +1623,7 @@ int run_vcycle(Solver& S, bool usev) {
     const long long n0 = c->nlaunch;
     cudaGraph_t g;
     WG_TRY_CUDA(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
-    G.vcycle<T>(0, usev);
+    G.vcycle<T>(0, usev, !usev);
     cudaError_t ce = cudaStreamEndCapture(c->cap_stream, &g);
     if (G.lerr != cudaSuccess) ce = G.lerr;
     WG_TRY_CUDA(ce);
