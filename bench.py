@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--forms", default="plain,mixed")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-vcycles", type=float, default=None)
     ap.add_argument("--ref-sample", type=int, default=1_000_000)
