@@ -6,7 +6,7 @@ The network is trained on snapshots of the plain solver on the
 - On held-out snapshots, the network's correction is closer to the true
   phi^n - phi^(n-1) than the zero correction of the plain warm start.
 - Multigrid still converges to the 1e-6 relative residual from the
-  learned guess; the plain solver remains the judge of every step.
+  learned guess; the plain solver still decides when each step has converged.
 
 The V-cycle counts of both starts are measured and printed. On this problem
 the learned start saves no V-cycles, and the test records that rather than

@@ -162,7 +162,7 @@ class WarmStart:
     out_scale is fixed from the training snapshots."""
 
     # Low-pass filters applied to the prediction before it is added: the
-    # multigrid judges a guess by its residual, and the bf16 output carries
+    # multigrid measures a guess by its residual, and the bf16 output carries
     # rounding and fitting noise whose Laplacian is as large as the residual
     # it removes. "box2": two passes of a 3x3x3 mean; "coarse4": mean over
     # 4x4x4 blocks, then trilinear interpolation back.

@@ -110,7 +110,7 @@ def laplacian(u):
 
 def guess_loss(pred, y, lap_weight):
     """MSE of the correction plus lap_weight times the MSE of its Laplacian:
-    the multigrid judges a guess by its residual, which the Laplacian of the
+    the multigrid measures a guess by its residual, which the Laplacian of the
     error dominates, so high-frequency error costs more than its size."""
     e = pred - y.float()
     return torch.mean(e * e) + lap_weight * torch.mean(laplacian(e) ** 2)
