@@ -63,7 +63,6 @@ typedef struct {
 } wg_solve_opts;
 
 #define WG_SOLVE_GRAPH 1  /* replay each V-cycle from a captured CUDA graph */
-#define WG_SOLVE_FUSED 2  /* fused out-of-place red+black sweep where allowed */
 #define WG_SOLVE_PDL 4    /* launch the solver's kernels with programmatic
                              dependent launch (each launch overlaps the end of
                              the previous kernel; same results) */

@@ -36,7 +36,7 @@ class SolveOpts(ctypes.Structure):
                 ("flags", ctypes.c_int), ("mgmaxvcycles", ctypes.c_int)]
 
 
-SOLVE_GRAPH, SOLVE_FUSED, SOLVE_PDL = 1, 2, 4
+SOLVE_GRAPH, SOLVE_PDL = 1, 4
 
 
 class SolveStats(ctypes.Structure):

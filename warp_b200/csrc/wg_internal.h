@@ -68,11 +68,9 @@ struct Level {
   size_t np = 0;  // (nx+3)(ny+3)(nz+3)
   size_t nr = 0;  // (nx+1)(ny+1)(nz+1)
   double* phi = nullptr;
-  double* phi2 = nullptr;  // second buffer of the out-of-place fused sweep
   double* rhs = nullptr;
   double* res = nullptr;
   float* phif = nullptr;
-  float* phif2 = nullptr;
   float* rhsf = nullptr;
   float* resf = nullptr;
   int n_int = 0;

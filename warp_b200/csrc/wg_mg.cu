@@ -18,15 +18,11 @@
 // list record. A sweep therefore reads exactly phi and rhs per node and
 // finds the conductor nodes without a separate tag array.
 //
-// Two SOR paths implement sorpass3d:
-//  * the fused sweep (k_sor_fused): both colours of one pass in a single
-//    out-of-place kernel that streams z-planes through shared memory,
-//    updating red on the tile plus a one-cell halo and then black on the
-//    tile, 24 B/node of DRAM traffic in FP64. Used when x and y are
-//    Dirichlet, z is Dirichlet or periodic, and no conductor surface point
-//    is of Neumann type.
-//  * the generic in-place path: one kernel per colour plus the conductor
-//    and boundary kernels, for every other case.
+// sorpass3d is one kernel per colour (k_sor_bulk). With Dirichlet x and y,
+// Dirichlet or periodic z and no Neumann-type conductor surface point, that
+// kernel also updates the colour's subgrid points and writes the periodic
+// images, so a half sweep is one launch; otherwise the subgrid and boundary
+// kernels follow it.
 
 #include <cmath>
 #include <cstdio>
@@ -519,177 +515,6 @@ __global__ void k_condbndymgint(T* __restrict__ phi, int nx, int ny, int nz, con
 }
 
 // ---------------------------------------------------------------------------
-// Fused sweep: one sorpass3d (both colours, conductors, guard planes) from
-// phi_in to phi_out. A CTA owns a FTX x FTY column of nodes (guards
-// included) over FZC output planes and marches in z with four planes of phi
-// (halo 2) and three planes of rhs in shared memory: red is updated on
-// plane k over the tile plus a one-cell halo, then black on plane k-1 over
-// the tile, then plane k-1 is stored. Halo values are recomputed by the
-// neighbouring CTAs identically, so tiles need no synchronisation. With
-// periodic z, planes -1 and nz+1 (and nz) are computed from wrapped loads,
-// which gives exactly the guard copies of applyboundaryconditions3d.
-constexpr int FTX = 32, FTY = 16, FHX = FTX + 4, FHY = FTY + 4, FPL = FHX * FHY, FZC = 32, FNT = 256;
-
-template <typename T>
-struct FusedArgs {
-  const T* in;
-  T* out;
-  const T* rhs;
-  int nx, ny, nz, zper;
-  SorCoef c;
-  CondArgs<T> C;
-  int usev, voltfac_on, lcndbndy;
-};
-
-// Per-thread load slots of one halo-2 plane tile (FPL elements over FNT
-// threads): the tile-relative offsets are the same for every plane.
-constexpr int FLD = (FPL + FNT - 1) / FNT;
-
-template <typename T, int HALO>
-__device__ inline void fused_relax(T* __restrict__ pc, const T* __restrict__ pm, const T* __restrict__ pp,
-                                   const T* __restrict__ rr, int par, int zr, int x0, int y0, const FusedArgs<T>& a,
-                                   T cx, T cy, T cz, T spm1) {
-  constexpr int W = FTX + 2 * HALO, H = FTY + 2 * HALO, HALF = W / 2;
-  const int nx = a.nx, ny = a.ny;
-#pragma unroll 2
-  for (int i = threadIdx.x; i < HALF * H; i += FNT) {
-    const int ly = 2 - HALO + i / HALF;
-    const int iy = y0 - 2 + ly;
-    const int ixs = x0 - HALO;
-    const int lx = 2 - HALO + ((ixs + iy + zr + par) & 1) + 2 * (i % HALF);
-    const int ix = x0 - 2 + lx;
-    if (ix < 1 || ix > nx - 1 || iy < 1 || iy > ny - 1) continue;
-    const int q = lx + FHX * ly;
-    const T r = rr[q];
-    const T self = pc[q];
-    T nv;
-    if (isbox(r)) {
-      if (Box<T>::interior(r)) continue;  // imposed at load time
-      const uint32_t k2 = Box<T>::idx(r);
-      if (k2 >= (uint32_t)a.C.nsub[par]) {
-        nv = r;  // not a valid record: propagate the NaN
-      } else {
-        nv = subgrid_value<T>(a.C, par, (int)k2, pc[q - 1], pc[q + 1], pc[q - FHX], pc[q + FHX], pm[q], pp[q], self,
-                              a.c, a.voltfac_on, a.lcndbndy);
-      }
-    } else {
-      nv = r + (pc[q - 1] + pc[q + 1]) * cx + (pc[q - FHX] + pc[q + FHX]) * cy + (pm[q] + pp[q]) * cz + spm1 * self;
-    }
-    pc[q] = nv;
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(FNT, 3) k_sor_fused(FusedArgs<T> a) {
-  pdl_entry();
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* sp = reinterpret_cast<T*>(smraw);  // [4][FPL] phi planes
-  T* sr = sp + 4 * FPL;                 // [3][FPL] rhs planes
-  const int tid = threadIdx.x;
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int x0 = -1 + (int)blockIdx.x * FTX, y0 = -1 + (int)blockIdx.y * FTY;
-  const int zs = -1 + (int)blockIdx.z * FZC;
-  const int ze = min(zs + FZC, nz + 2);
-  const T cx = (T)a.c.cx, cy = (T)a.c.cy, cz = (T)a.c.cz, spm1 = (T)a.c.spm1;
-  const size_t pplane = (size_t)(nx + 3) * (ny + 3), rplane = (size_t)(nx + 1) * (ny + 1);
-
-  // periodic z: plane nz is the same node set as plane 0 (applyboundaryconditions3d
-  // copies 0 -> nz after every half pass), so virtual planes wrap modulo nz
-  auto wrapz = [&](int p) { return !a.zper ? p : ((p % nz) + nz) % nz; };
-  auto zexists = [&](int p) { return a.zper || (p >= -1 && p <= nz + 1); };
-  auto zupdated = [&](int p) { return a.zper || (p >= 1 && p <= nz - 1); };
-  auto mod3 = [](int p) { return ((p % 3) + 3) % 3; };
-
-  // this thread's load slots: phi offset within a plane (-1 if outside the
-  // padded array) and rhs offset (-1 if not a node)
-  int poff[FLD], roff[FLD];
-#pragma unroll
-  for (int j = 0; j < FLD; ++j) {
-    const int i = tid + j * FNT;
-    poff[j] = -1;
-    roff[j] = -1;
-    if (i < FPL) {
-      const int ix = x0 - 2 + i % FHX, iy = y0 - 2 + i / FHX;
-      if (ix >= -1 && ix <= nx + 1 && iy >= -1 && iy <= ny + 1) {
-        poff[j] = (ix + 1) + (nx + 3) * (iy + 1);
-        if (ix >= 0 && ix <= nx && iy >= 0 && iy <= ny) roff[j] = ix + (nx + 1) * iy;
-      }
-    }
-  }
-  T vreg[FLD], rreg[FLD];
-  // global loads of virtual plane p into registers
-  auto fetch = [&](int p) {
-    const bool ok = zexists(p);
-    const int zr = wrapz(p);
-    const bool zreal = zr >= 0 && zr <= nz;
-#pragma unroll
-    for (int j = 0; j < FLD; ++j) {
-      vreg[j] = (T)0.;
-      rreg[j] = (T)0.;
-      if (ok && poff[j] >= 0) vreg[j] = a.in[(size_t)poff[j] + pplane * (size_t)(zr + 1)];
-      if (ok && zreal && roff[j] >= 0) rreg[j] = a.rhs[(size_t)roff[j] + rplane * (size_t)zr];
-    }
-  };
-  // registers -> shared slots of plane p; interior conductor nodes take their
-  // imposed value (cond_potmg at the start of sorpass3d)
-  auto deposit = [&](int p) {
-    T* dp = sp + (p & 3) * FPL;
-    T* dr = sr + mod3(p) * FPL;
-#pragma unroll
-    for (int j = 0; j < FLD; ++j) {
-      const int i = tid + j * FNT;
-      if (i < FPL) {
-        T v = vreg[j];
-        const T r = rreg[j];
-        if (isbox(r) && Box<T>::interior(r)) {
-          const uint32_t k = Box<T>::idx(r);
-          if (k < (uint32_t)a.C.nint) v = a.usev ? (T)a.C.ivolt[k] : (T)0.;
-        }
-        dp[i] = v;
-        dr[i] = r;
-      }
-    }
-  };
-  auto red = [&](int k) {
-    if (zupdated(k))
-      fused_relax<T, 1>(sp + (k & 3) * FPL, sp + ((k - 1) & 3) * FPL, sp + ((k + 1) & 3) * FPL, sr + mod3(k) * FPL,
-                        0, wrapz(k), x0, y0, a, cx, cy, cz, spm1);
-  };
-  auto black = [&](int k) {
-    if (zupdated(k))
-      fused_relax<T, 0>(sp + (k & 3) * FPL, sp + ((k - 1) & 3) * FPL, sp + ((k + 1) & 3) * FPL, sr + mod3(k) * FPL,
-                        1, wrapz(k), x0, y0, a, cx, cy, cz, spm1);
-  };
-  auto store = [&](int k) {
-    const T* pc = sp + (k & 3) * FPL;
-    for (int i = tid; i < FTX * FTY; i += FNT) {
-      const int lx = 2 + i % FTX, ly = 2 + i / FTX;
-      const int ix = x0 + i % FTX, iy = y0 + i / FTX;
-      if (ix <= nx + 1 && iy <= ny + 1) a.out[pix(nx, ny, ix, iy, k)] = pc[lx + FHX * ly];
-    }
-  };
-
-  // prologue: planes zs-2 .. zs+1, red on zs-1
-  for (int p = zs - 2; p <= zs + 1; ++p) {
-    fetch(p);
-    deposit(p);
-  }
-  __syncthreads();
-  red(zs - 1);
-  for (int k = zs; k <= ze; ++k) {
-    // the next plane's loads are in flight while this plane is relaxed
-    fetch(k + 2);
-    red(k);
-    __syncthreads();
-    if (k - 1 >= zs) black(k - 1);
-    __syncthreads();
-    if (k - 1 >= zs) store(k - 1);
-    deposit(k + 2);
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------
 // residual3d bulk part (f3d_mgrid.F:3519-3586).
 //   MODE 0: writes the padded res array (0 outside the updated range)
 //   MODE 1: no store, only the max over non-conductor nodes (norm)
@@ -1170,7 +995,6 @@ struct Arr;
 template <>
 struct Arr<double> {
   static double*& phi(Level& L) { return L.phi; }
-  static double*& phi2(Level& L) { return L.phi2; }
   static double* rhs(Level& L) { return L.rhs; }
   static double* res(Level& L) { return L.res; }
   static double* srhs(DevSubgrid& S) { return S.rhs; }
@@ -1178,7 +1002,6 @@ struct Arr<double> {
 template <>
 struct Arr<float> {
   static float*& phi(Level& L) { return L.phif; }
-  static float*& phi2(Level& L) { return L.phif2; }
   static float* rhs(Level& L) { return L.rhsf; }
   static float* res(Level& L) { return L.resf; }
   static float* srhs(DevSubgrid& S) { return S.rhsf; }
@@ -1222,7 +1045,6 @@ struct Solver {
   const wg_solve_opts* o;
   Bnd B;
   cudaStream_t s;
-  bool fused_ok;  // boundary types and options allow the fused sweep
   bool capturing = false;
   bool pdl = false;  // launch with programmatic dependent launch
   cudaError_t lerr = cudaSuccess;  // first launch error
@@ -1314,28 +1136,6 @@ struct Solver {
   void sorpass(int l, bool usev, bool phi_zero = false) {
     Level& L = c->lv[l];
     const SorCoef k = coef(L.d);
-    if (fused_ok && !L.has_neumann_sub) {
-      FusedArgs<T> a;
-      a.in = Arr<T>::phi(L);
-      a.out = Arr<T>::phi2(L);
-      a.rhs = Arr<T>::rhs(L);
-      a.nx = L.d.nx;
-      a.ny = L.d.ny;
-      a.nz = L.d.nz;
-      a.zper = B.b[4] == 2;
-      a.c = k;
-      a.C = cond_args<T>(L);
-      a.usev = usev;
-      a.voltfac_on = usev;
-      a.lcndbndy = o->lcndbndy;
-      dim3 grd(cdiv(L.d.nx + 3, FTX), cdiv(L.d.ny + 3, FTY), cdiv(L.d.nz + 3, FZC));
-      const size_t smem = 7 * FPL * sizeof(T);
-      int pe = prof_begin(l, WG_PROF_SOR0, 2. * (double)L.nr);
-      launch(k_sor_fused<T>, grd, FNT, smem, a);
-      c->prof_end(pe);
-      std::swap(Arr<T>::phi(L), Arr<T>::phi2(L));
-      return;
-    }
     T* phi = Arr<T>::phi(L);
     const T* rhs = Arr<T>::rhs(L);
     // One launch per half pass (bulk nodes and subgrid points together)
@@ -1584,15 +1384,6 @@ struct Solver {
     return WG_OK;
   }
 
-  // Leaves level 0's phi in the user-visible buffer.
-  int restore_phi(double* user) {
-    Level& L0 = c->lv[0];
-    if (L0.phi != user) {
-      copy(L0.phi, user, L0.np);
-      std::swap(L0.phi, L0.phi2);
-    }
-    return WG_OK;
-  }
 };
 
 // The V-cycle of precision T from a captured CUDA graph (recaptured when the
@@ -1610,7 +1401,7 @@ int run_vcycle(Solver& S, bool usev) {
   memcpy(&mp, &o->mgparam, sizeof(mp));
   unsigned long long key = mp ^ ((unsigned long long)o->mgmaxlevels << 1) ^ ((unsigned long long)o->downpasses << 9) ^
                            ((unsigned long long)o->uppasses << 17) ^ ((unsigned long long)o->lcndbndy << 25) ^
-                           ((unsigned long long)S.fused_ok << 27) ^ ((unsigned long long)usev << 28) ^
+                           ((unsigned long long)usev << 28) ^
                            ((unsigned long long)S.pdl << 29) ^
                            ((unsigned long long)c->cond_version << 32);
   if (!c->vgraph[gi] || c->vgraph_key[gi] != key) {
@@ -1639,9 +1430,6 @@ int run_vcycle(Solver& S, bool usev) {
   return WG_OK;
 }
 
-bool fused_allowed(const int* b) {
-  return b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0 && ((b[4] == 0 && b[5] == 0) || (b[4] == 2 && b[5] == 2));
-}
 
 }  // namespace
 
@@ -1665,11 +1453,9 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   }
   Solver S{c, o, {}, c->stream, false};
   for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
-  S.fused_ok = fused_allowed(S.B.b) && (o->flags & WG_SOLVE_FUSED);
   S.pdl = (o->flags & WG_SOLVE_PDL) && !c->prof_mask;
   cudaStream_t s = c->stream;
   Level& L0 = c->lv[0];
-  double* user_phi = L0.phi;
   const LevelDims& d = L0.d;
   double dxsqi = 1. / (d.dx * d.dx), dysqi = 1. / (d.dy * d.dy), dzsqi = 1. / (d.dz * d.dz);
   double reps0c = o->mgparam / (kEps0 * 2. * (dxsqi + dysqi + dzsqi));
@@ -1754,7 +1540,6 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       }
     }
   }
-  WG_TRY(S.restore_phi(user_phi));
   S.bc<double>(L0, L0.phi, true);
   WG_TRY_CUDA(S.lerr);
   WG_TRY_CUDA(cudaGetLastError());
@@ -1863,13 +1648,7 @@ int field_energy(wg_ctx* c, double* out) {
   return WG_OK;
 }
 
-// Shared memory of the fused sweep exceeds the 48 KB default for FP64.
-int configure_kernels() {
-  WG_TRY_CUDA(cudaFuncSetAttribute(k_sor_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(7 * FPL * sizeof(double))));
-  WG_TRY_CUDA(cudaFuncSetAttribute(k_sor_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(7 * FPL * sizeof(float))));
-  return WG_OK;
-}
+// Per-kernel attributes set once per context (none needed at present).
+int configure_kernels() { return WG_OK; }
 
 }  // namespace wg

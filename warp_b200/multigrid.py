@@ -48,7 +48,7 @@ class MultiGridB200(FieldSolver):
     def __init__(self, nx, ny, nz, xmmin, xmmax, ymmin, ymmax, zmmin, zmmax, bounds=(0, 0, 0, 0, 0, 0),
                  mgparam=1.2, mgtol=1.e-6, mgmaxiters=100, mgmaxlevels=101, downpasses=1, uppasses=1,
                  lcndbndy=True, icndbndy=2, mgform=1, mgverbose=0, precision="fp64", tolkind="mgerror",
-                 device=None, use_graphs=True, fused_sweep=False, use_pdl=True):
+                 device=None, use_graphs=True, use_pdl=True):
         if icndbndy != 2:
             raise ValueError("MultiGridB200 supports icndbndy = 2 (quadratic subgrid stencil) only")
         if mgform != 1:
@@ -71,9 +71,9 @@ class MultiGridB200(FieldSolver):
         self.mgmaxlevels, self.downpasses, self.uppasses = int(mgmaxlevels), int(downpasses), int(uppasses)
         self.lcndbndy, self.icndbndy, self.mgform, self.mgverbose = bool(lcndbndy), icndbndy, mgform, mgverbose
         self.precision, self.tolkind = precision, tolkind
-        # replay V-cycles from captured CUDA graphs; fused out-of-place sweep;
-        # programmatic dependent launch of the solver's kernels
-        self.use_graphs, self.fused_sweep, self.use_pdl = bool(use_graphs), bool(fused_sweep), bool(use_pdl)
+        # replay V-cycles from captured CUDA graphs; programmatic dependent
+        # launch of the solver's kernels
+        self.use_graphs, self.use_pdl = bool(use_graphs), bool(use_pdl)
         self.mgiters, self.mgerror, self.relres, self.converged = 0, 0., -1., True
         self.conductordatalist = []
         self._conductors_installed = False
@@ -269,8 +269,7 @@ class MultiGridB200(FieldSolver):
             _lib.check(_lib.lib.wg_finalize_rho(self._h))
 
     def _opts(self):
-        flags = (_lib.SOLVE_GRAPH if self.use_graphs else 0) | (_lib.SOLVE_FUSED if self.fused_sweep else 0) | \
-            (_lib.SOLVE_PDL if self.use_pdl else 0)
+        flags = (_lib.SOLVE_GRAPH if self.use_graphs else 0) | (_lib.SOLVE_PDL if self.use_pdl else 0)
         return _lib.SolveOpts(self.mgparam, self.mgtol, self.mgmaxiters, self.mgmaxlevels, self.downpasses,
                               self.uppasses, int(self.lcndbndy), _PRECISION[self.precision],
                               _TOLKIND[self.tolkind], flags, int(getattr(self, "mgmaxvcycles", 0)))
