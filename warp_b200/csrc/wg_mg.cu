@@ -375,8 +375,8 @@ __device__ inline void store_wt(T* phi, int p, int iz, int nz, int sz, int wtz, 
 
 // condbndymg update of subgrid point i of colour par (no-op on Dirichlet
 // boundary planes). With wtz the plane nz is left to the write-through of
-// plane 0.
-template <typename T>
+// plane 0. ZERO: phi is taken as all zeros (nothing of it is read).
+template <typename T, bool ZERO = false>
 __device__ __forceinline__ void special_point(T* phi, int nx, int ny, int nz, const CondArgs<T>& C, int par, const Bnd& B,
                                      const SorCoef& c, int voltfac_on, int lcndbndy, int i, int wtz) {
   // pointers chosen without indexing the parameter arrays by a runtime value
@@ -394,8 +394,10 @@ __device__ __forceinline__ void special_point(T* phi, int nx, int ny, int nz, co
   if (wtz && iz == nz) return;
   const int sy = nx + 3, sz = sy * (ny + 3);
   const int p = (ix + 1) + sy * (iy + 1) + sz * (iz + 1);
-  const T v = subgrid_core<T>(r, dl, vl, phi[p - 1], phi[p + 1], phi[p - sy], phi[p + sy], phi[p - sz], phi[p + sz],
-                              phi[p], c, voltfac_on, lcndbndy);
+  const T z = (T)0.;
+  const T v = ZERO ? subgrid_core<T>(r, dl, vl, z, z, z, z, z, z, z, c, voltfac_on, lcndbndy)
+                   : subgrid_core<T>(r, dl, vl, phi[p - 1], phi[p + 1], phi[p - sy], phi[p + sy], phi[p - sz],
+                                     phi[p + sz], phi[p], c, voltfac_on, lcndbndy);
   store_wt(phi, p, iz, nz, sz, wtz, v);
 }
 
@@ -454,6 +456,84 @@ __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* 
     if (ok[k] && !isbox(r[k]))
       store_wt(phi, p0 + k * sz + ((odd0 + k) & 1), iz0 + k, nz, sz, wtz,
                r[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz + spm1 * c[k]);
+}
+
+// The first (red) half sweep of a pass whose phi is all zeros, for a level
+// where k_sor_bulk does the whole half sweep (no Neumann-type subgrid
+// points, Dirichlet x and y, periodic z with an even nz or Dirichlet z). It
+// writes every node of the padded array once, reading rhs only, and so
+// replaces the zeroing: a red node of the update range gets the bulk or
+// subgrid formula evaluated with zero neighbours (the same expressions, so
+// the same bits as zeroing the array and running k_sor_bulk), every other
+// node 0, and with wtz the periodic images take their source plane's value.
+// As in k_sor_bulk, the first nspz z-slices of blocks take the red subgrid
+// points, one a thread; the bulk blocks skip those nodes. A bulk thread
+// takes the x pair (2t-1, 2t) of one row in FZ consecutive planes: one node
+// of a pair is red, and its rhs loads for all FZ planes are issued before
+// the first store.
+template <typename T, int FZ>
+__global__ void __launch_bounds__(256) k_sor_from_zero(T* __restrict__ phi, const T* __restrict__ rhs, int nx, int ny,
+                                                       int nz, int ixmin, int ixmax, int iymin, int iymax, int izmin,
+                                                       int izmax, T cx, T cy, T cz, T spm1, int wtz, int nbz,
+                                                       CondArgs<T> C, Bnd B, SorCoef sc, int lcndbndy) {
+  pdl_entry();
+  const int nspz = (int)gridDim.z - nbz;
+  if ((int)blockIdx.z < nspz) {
+    const int i = (((int)blockIdx.z * (int)gridDim.y + (int)blockIdx.y) * (int)gridDim.x + (int)blockIdx.x) *
+                      (int)(blockDim.x * blockDim.y) +
+                  (int)(threadIdx.y * blockDim.x + threadIdx.x);
+    if (i < C.nsub[0]) special_point<T, true>(phi, nx, ny, nz, C, 0, B, sc, 0, lcndbndy, i, wtz);
+    return;
+  }
+  const int x0 = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x) - 1;
+  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
+  const int z0 = ((int)blockIdx.z - nspz) * FZ - 1;
+  if (x0 > nx + 1 || iy > ny + 1) return;
+  const bool yin = iy >= iymin && iy <= iymax;
+  T r[FZ];
+  int xr[FZ];
+  bool upd[FZ];
+#pragma unroll
+  for (int k = 0; k < FZ; ++k) {
+    const int iz = z0 + k;
+    int src = iz;
+    if (wtz) {
+      if (iz == nz) src = 0;
+      else if (iz == nz + 1) src = 1;
+      else if (iz == -1) src = nz - 1;
+    }
+    xr[k] = x0 + ((x0 + iy + src) & 1);
+    upd[k] = iz <= nz + 1 && yin && src >= izmin && src <= izmax && xr[k] >= ixmin && xr[k] <= ixmax;
+    if (upd[k]) r[k] = rhs[(size_t)xr[k] + (size_t)(nx + 1) * ((size_t)iy + (size_t)(ny + 1) * src)];
+  }
+  const size_t sz = (size_t)(nx + 3) * (ny + 3);
+  const size_t pr = (size_t)(x0 + 1) + (size_t)(nx + 3) * (iy + 1);
+#pragma unroll
+  for (int k = 0; k < FZ; ++k) {
+    const int iz = z0 + k;
+    if (iz > nz + 1) break;
+    // a red subgrid point of the range is written by the subgrid blocks
+    bool mine = true;
+    T v = (T)0.;
+    if (upd[k]) {
+      if (!isbox(r[k])) {
+        const T z = (T)0.;
+        v = r[k] + (z + z) * cx + (z + z) * cy + (z + z) * cz + spm1 * z;
+      } else {
+        mine = Box<T>::interior(r[k]);
+      }
+    }
+    // the pair's second node exists up to x = nx + 1 (an odd row length
+    // leaves the last pair single)
+    T* row = phi + pr + sz * (size_t)(iz + 1);
+    const bool second = xr[k] != x0;
+    if (second) row[0] = (T)0.;
+    else if (mine) row[0] = v;
+    if (x0 + 1 <= nx + 1) {
+      if (!second) row[1] = (T)0.;
+      else if (mine) row[1] = v;
+    }
+  }
 }
 
 // condbndymg for one colour then cond_potmg (f3d_mgrid.F:2874-2978,
@@ -1131,6 +1211,25 @@ struct Solver {
                                           Arr<T>::srhs(L.sub[1]));
   }
 
+  // Whether one launch per half pass does all of sorpass3d's half pass on
+  // level L (k_sor_bulk with its subgrid slices): no Neumann subgrid
+  // points, and the boundary copy after each half pass is either empty
+  // (all Dirichlet) or the periodic-z copy, which the kernel then does
+  // itself by writing every updated node of planes 0, 1 and nz-1 to its
+  // images. That write-through needs an even nz: with an odd nz the nodes
+  // (i, j, 0) and (i, j, nz-1) have the same colour, and the first reads the
+  // image of the second within the half pass.
+  bool merged_ok(const Level& L) const {
+    const int* b = B.b;
+    const bool xy_dir = b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0;
+    const bool zper = b[4] == 2 && b[5] == 2, zdir = b[4] == 0 && b[5] == 0;
+    return !L.has_neumann_sub && xy_dir && (zdir || (zper && L.d.nz % 2 == 0)) && L.d.nz >= 2;
+  }
+
+  // Whether the first red half sweep of level l can start from an
+  // unzeroed phi and write all of it (k_sor_from_zero).
+  bool from_zero_ok(int l) const { return o->downpasses >= 1 && merged_ok(c->lv[l]); }
+
   // sorpass3d (f3d_mgrid.F:1949-2093)
   template <typename T>
   void sorpass(int l, bool usev, bool phi_zero = false) {
@@ -1138,16 +1237,9 @@ struct Solver {
     const SorCoef k = coef(L.d);
     T* phi = Arr<T>::phi(L);
     const T* rhs = Arr<T>::rhs(L);
-    // One launch per half pass (bulk nodes and subgrid points together)
-    // when no Neumann subgrid points exist and the boundary copy after each
-    // half pass is either empty (all Dirichlet) or the periodic-z copy,
-    // which the kernel then does itself by writing every updated node of
-    // planes 0, 1 and nz-1 to its images.
-    const int* b = B.b;
-    const bool xy_dir = b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0;
-    const bool zper = b[4] == 2 && b[5] == 2, zdir = b[4] == 0 && b[5] == 0;
-    const bool merged = !L.has_neumann_sub && xy_dir && (zper || zdir) && L.d.nz >= 2;
-    const int wtz = (merged && zper) ? 1 : 0;
+    // one launch per half pass (bulk nodes and subgrid points together)
+    const bool merged = merged_ok(L);
+    const int wtz = (merged && B.b[4] == 2) ? 1 : 0;
     // cond_potmg sets the interior nodes to their voltage or, below the
     // finest level, to 0: a no-op on a phi that was just zeroed
     if (L.n_int && !(phi_zero && !usev)) {
@@ -1173,7 +1265,18 @@ struct Solver {
       const unsigned gx = bulk ? cdiv(nhalf, 32) : 1, gy = bulk ? cdiv(nyr, 8) : 1;
       const int nbz = bulk ? (int)cdiv(nzr, zpt) : 0;
       const int nspz = merged ? (int)cdiv((size_t)nsub, 256u * gx * gy) : 0;
-      if (nbz + nspz > 0) {
+      if (parity == 0 && phi_zero && !usev && merged) {
+        // phi was not zeroed: this launch writes all of it (from_zero_ok)
+        int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
+        constexpr int fz = 4;
+        const unsigned fgx = cdiv(cdiv(L.d.nx + 3, 2), 32), fgy = cdiv(L.d.ny + 3, 8);
+        const int fbz = (int)cdiv(L.d.nz + 3, fz);
+        const int fspz = (int)cdiv((size_t)nsub, 256u * fgx * fgy);
+        launch(k_sor_from_zero<T, fz>, dim3(fgx, fgy, fbz + fspz), blk, 0, phi, rhs, L.d.nx, L.d.ny, L.d.nz, R.ixmin,
+               R.ixmax, R.iymin, R.iymax, R.izmin, izmax, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1, wtz, fbz, ca, B, k,
+               o->lcndbndy);
+        c->prof_end(pe);
+      } else if (nbz + nspz > 0) {
         int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
         launch(k_sor_bulk<T, zpt>, dim3(gx, gy, nbz + nspz), blk, 0, 
             phi, rhs, L.d.nx, L.d.ny, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, izmax, parity, (T)k.cx, (T)k.cy,
@@ -1267,7 +1370,7 @@ struct Solver {
       }
       c->prof_end(pr);
       box<T>(l + 1);
-      zero(Arr<T>::phi(Lc), Lc.np);
+      if (!from_zero_ok(l + 1)) zero(Arr<T>::phi(Lc), Lc.np);
       int pc = (l == 0) ? prof_begin(0, WG_PROF_COARSE, (double)Lc.nr) : -1;
       vcycle<T>(l + 1, false, true);
       c->prof_end(pc);
@@ -1522,7 +1625,7 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
       }
       if (it >= o->mgmaxiters) break;
       S.box<float>(0);
-      S.zero(L0.phif, L0.np);
+      if (!S.from_zero_ok(0)) S.zero(L0.phif, L0.np);
       WG_TRY(run_vcycle<float>(S, false));
       WG_TRY(S.clear_slots(0));
       {
