@@ -52,7 +52,7 @@ template <typename T>
 struct Box;
 template <>
 struct Box<double> {
-  static constexpr uint32_t kMax = 0xFFFFFFFFu;
+  // the index takes the low 32 bits of the payload: any int count fits
   __device__ static double make(bool interior, uint32_t idx) {
     return __longlong_as_double((long long)(0x7FF8000000000000ull | (interior ? 0x8000000000000000ull : 0ull) |
                                             (unsigned long long)idx));

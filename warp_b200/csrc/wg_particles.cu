@@ -36,10 +36,6 @@ __device__ inline void cellfrac(double s, int n, int& i, double& f) {
   f = s - i;
 }
 
-__device__ inline size_t pix(int nx, int ny, int ix, int iy, int iz) {
-  return (size_t)(ix + 1) + (size_t)(nx + 3) * ((size_t)(iy + 1) + (size_t)(ny + 3) * (size_t)(iz + 1));
-}
-
 // setrho3ddirect1 (w3d.F:7757-7960) with 64-bit fixed-point weights. A CTA
 // takes a chunk of DEP_NT*DEP_PPT consecutive particles; warp w of the CTA
 // takes the DEP_PPT*32 consecutive particles starting at w*32*DEP_PPT, 32 at
