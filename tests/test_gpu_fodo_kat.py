@@ -14,30 +14,15 @@ These are the test's own tolerances. Differences from the reference test:
 Everything else runs through the GPU PIC step: deposit, multigrid, gather,
 quads and Boris push.
 """
-import math
-
 import numpy as np
 import pytest
 import torch
 
+from tests.fodo_setup import A0, B0, EMIT, HLP, IBEAM, PIPERAD
+from tests.fodo_setup import lattice as _lattice
+from tests.fodo_setup import species as _species
+
 pytestmark = pytest.mark.gpu
-
-HLP, QUADLEN, DBDX, PIPERAD = 0.36, 0.11, 8.4817662372660610, 0.02
-A0, B0, EMIT, IBEAM, EKIN = 15.60152892731585e-3, 8.75924684128793e-3, 62.46985327098694e-06, 2e-3, 80e3
-
-
-def _lattice():
-    from warp_b200.lattice import Lattice, Quad
-    return Lattice([Quad(-QUADLEN / 2, QUADLEN / 2, -DBDX), Quad(HLP - QUADLEN / 2, HLP + QUADLEN / 2, +DBDX)],
-                   zlatperi=2 * HLP)
-
-
-def _species():
-    from warp_b200.constants import amu, clight, echarge
-    m = 39.0983 * amu
-    gamma = 1. + EKIN * echarge / (m * clight * clight)
-    v = math.sqrt(1. - 1. / (gamma * gamma)) * clight
-    return echarge, m, v, gamma
 
 
 def test_basic_fodo_rms_envelope_follows_kv_envelope():

@@ -1,0 +1,84 @@
+"""A long run against the oracle: the FODO beam of the reference's
+integration test (tests/fodo_setup.py; 20000 particles, 32 x 32 x 64 cells,
+multigrid to max |dphi| <= 1e-6 V) over 1000 steps, 20 lattice periods,
+compared period by period with the oracle's run stored in
+tests/golden/fodo_long_run.npz (made by tests/golden/make_fodo_long_run.py).
+
+- Plain FP64 form: the emittances within 1e-9 relative of the oracle's at
+  every period, the same live-particle counts, and the same V-cycle count
+  in all but at most two of the 1001 solves. Over 1000 steps the only
+  difference is the 2^-46 fixed-point rounding of the deposit.
+- Mixed form (FP32 V-cycles inside FP64 defect correction): the emittances
+  within 1e-4 relative of the FP64 oracle after 1000 steps, the stated
+  accuracy target of the mixed form, and at most two particles lost
+  differently.
+
+On the oracle the run responds linearly to small changes of the field: a
+1e-8 relative change of rho moves the emittance by about 1e-8 after 1000
+steps, so differences do not grow exponentially here."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from tests import fodo_setup as F
+
+pytestmark = pytest.mark.gpu
+
+FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fodo_long_run.npz")
+
+
+def _run(precision, g):
+    from warp_b200.multigrid import MultiGridB200
+    from warp_b200.particles import ParticleGroup
+    q, m, v, _ = F.species()
+    npart = int(g["npart"])
+    p = F.host_beam(npart, int(g["seed"]))
+    assert np.array_equal(p["x"][:8], g["x0"]), "the CPU generator no longer draws the fixture's particles"
+    dx, dy, dz, xmin, ymin, zmin = F.mesh()
+    s = MultiGridB200(F.NX, F.NY, F.NZ, xmin, -xmin, ymin, -ymin, zmin, -zmin, bounds=F.BOUNDS,
+                      precision=precision, tolkind="mgerror", mgtol=float(g["mgtol"]), mgverbose=-1)
+    s.setlattice(F.lattice())
+    pg = ParticleGroup(p, q=q, m=m, w=F.weight(npart))
+    s.addpgroup(pg)
+    s.loadrho()
+    s.solve()
+    vcycles = [s.mgiters]
+    dt = F.timestep()
+    every = int(g["step"][0])
+    rec = []
+    for n in range(int(g["nsteps"])):
+        s.advance(pg, dt, prwall=F.PIPERAD, center="halfv" if n == 0 else "fullv")
+        s.loadrho()
+        s.solve()
+        assert s.converged, "step %d" % n
+        vcycles.append(s.mgiters)
+        if (n + 1) % every == 0:
+            mo = s.moments(pg)
+            rec.append((mo["epsx"], mo["epsy"], mo["n"]))
+    r = np.array(rec)
+    return r[:, 0], r[:, 1], r[:, 2].astype(np.int64), np.array(vcycles)
+
+
+def _rel(a, b):
+    return np.max(np.abs(a / b - 1.0))
+
+
+def test_fodo_1000_steps_plain_and_mixed_against_oracle():
+    torch.cuda.set_device(0)
+    g = np.load(FIXTURE)
+    ex, ey, live, vc = _run("fp64", g)
+    dev = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
+    nvc = int(np.sum(vc != g["vcycles"]))
+    print("plain: max rel emittance deviation %.2e over %d periods; V-cycles %d (oracle %d), %d solves differ" % (
+        dev, len(ex), vc.sum(), g["vcycles"].sum(), nvc))
+    assert np.array_equal(live, g["live"])
+    assert dev <= 1e-9
+    assert nvc <= 2
+    ex, ey, live, vc = _run("mixed", g)
+    dev = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
+    print("mixed: max rel emittance deviation %.2e; after 1000 steps x %.2e y %.2e; V-cycles %d; live %d vs %d" % (
+        dev, abs(ex[-1] / g["epsx"][-1] - 1), abs(ey[-1] / g["epsy"][-1] - 1), vc.sum(), live[-1], g["live"][-1]))
+    assert np.max(np.abs(live - g["live"])) <= 2
+    assert dev <= 1e-4
