@@ -11,7 +11,8 @@ tests/golden/fodo_long_run.npz (made by tests/golden/make_fodo_long_run.py).
 - Mixed form (FP32 V-cycles inside FP64 defect correction): the emittances
   within 1e-4 relative of the FP64 oracle after 1000 steps, the stated
   accuracy target of the mixed form, and at most two particles lost
-  differently.
+  differently. Its final phi and grid E (centred differences) are within
+  1e-9 of max|.| of the plain run's.
 
 On the oracle the run responds linearly to small changes of the field: a
 1e-8 relative change of rho moves the emittance by about 1e-8 after 1000
@@ -58,7 +59,15 @@ def _run(precision, g):
             mo = s.moments(pg)
             rec.append((mo["epsx"], mo["epsy"], mo["n"]))
     r = np.array(rec)
-    return r[:, 0], r[:, 1], r[:, 2].astype(np.int64), np.array(vcycles)
+    return r[:, 0], r[:, 1], r[:, 2].astype(np.int64), np.array(vcycles), s.phi.cpu().numpy()
+
+
+def _efield(phi):
+    """E = -grad phi by centred differences on the nodes 0..n."""
+    dx, dy, dz, *_ = F.mesh()
+    return (-(phi[2:, 1:-1, 1:-1] - phi[:-2, 1:-1, 1:-1]) / (2 * dx),
+            -(phi[1:-1, 2:, 1:-1] - phi[1:-1, :-2, 1:-1]) / (2 * dy),
+            -(phi[1:-1, 1:-1, 2:] - phi[1:-1, 1:-1, :-2]) / (2 * dz))
 
 
 def _rel(a, b):
@@ -68,7 +77,7 @@ def _rel(a, b):
 def test_fodo_1000_steps_plain_and_mixed_against_oracle():
     torch.cuda.set_device(0)
     g = np.load(FIXTURE)
-    ex, ey, live, vc = _run("fp64", g)
+    ex, ey, live, vc, phi_p = _run("fp64", g)
     dev = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
     nvc = int(np.sum(vc != g["vcycles"]))
     print("plain: max rel emittance deviation %.2e over %d periods; V-cycles %d (oracle %d), %d solves differ" % (
@@ -76,9 +85,13 @@ def test_fodo_1000_steps_plain_and_mixed_against_oracle():
     assert np.array_equal(live, g["live"])
     assert dev <= 1e-9
     assert nvc <= 2
-    ex, ey, live, vc = _run("mixed", g)
+    ex, ey, live, vc, phi_m = _run("mixed", g)
     dev = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
+    dphi = np.max(np.abs(phi_m - phi_p)) / np.max(np.abs(phi_p))
+    dE = max(np.max(np.abs(a - b)) / np.max(np.abs(b)) for a, b in zip(_efield(phi_m), _efield(phi_p)))
+    print("mixed after 1000 steps: phi within %.2e and E within %.2e of max|.| of the FP64 run" % (dphi, dE))
     print("mixed: max rel emittance deviation %.2e; after 1000 steps x %.2e y %.2e; V-cycles %d; live %d vs %d" % (
         dev, abs(ex[-1] / g["epsx"][-1] - 1), abs(ey[-1] / g["epsy"][-1] - 1), vc.sum(), live[-1], g["live"][-1]))
     assert np.max(np.abs(live - g["live"])) <= 2
     assert dev <= 1e-4
+    assert dphi <= 1e-9 and dE <= 1e-9
