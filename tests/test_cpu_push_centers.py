@@ -5,6 +5,8 @@ matches bit for bit in tests/test_gpu_particles.py:
   and synchv by half of that, and halfv followed by fullv steps keeps the
   velocity half a step ahead of the positions;
 - inside a quad, the Boris rotation conserves |u| in every center;
+- across a quad edge the kick scales with the residence fraction of the
+  center's time window;
 - synchv moves no particle and applies no boundary."""
 import numpy as np
 import pytest
@@ -77,3 +79,33 @@ def test_synchv_applies_no_boundary():
     assert np.all(p["gaminv"] == 1.0)
     oracle.push(p, z, z, z, echarge, proton_mass, 1e-10, None, 0.0, 1.0, 0.0, 1.0, 0.01, center="fullv")
     assert np.all(p["gaminv"][:10] == 0.0)
+
+
+@pytest.mark.parametrize("center,window", [("fullv", (-0.5, 0.5)), ("halfv", (0.0, 0.5)), ("synchv", (-0.5, 0.0))])
+@pytest.mark.parametrize("side", ["entry", "exit"])
+def test_quad_kick_scales_with_residence_fraction(center, window, side):
+    """applyquad (top_lattice.F:2985-3120): a particle whose time window
+    [z + vz dtl, z + vz dtr] straddles a quad edge feels the quad's field
+    times the fraction of the window inside the quad. With a weak gradient
+    the Boris kick is linear in the field, so the kick of a straddling
+    particle is that fraction of the kick of one inside the quad."""
+    from warp_b200.lattice import Lattice, Quad
+    zs, ze, db = 0.40, 0.55, 1e-3
+    lat = Lattice([Quad(zs, ze, db)], zlatperi=1.0)
+    nzl, zlmin, dzl = 200, 0.0, 1.0 / 200
+    tables = lat.tables(zlmin, dzl, nzl)[:3]
+    dt, vz = 2e-9, 1.4e7
+    a = vz * dt * (window[1] - window[0])
+    f = np.array([0.1, 0.25, 0.5, 0.8, 0.97])
+    n = len(f) + 1
+    if side == "entry":  # window from zs - (1 - f) a to zs + f a
+        zl = zs - (1.0 - f) * a
+    else:  # window from ze - f a to ze + (1 - f) a
+        zl = ze - f * a
+    z = np.concatenate([zl - vz * dt * window[0], [0.5 * (zs + ze)]])
+    p = {"x": np.full(n, 1e-3), "y": np.zeros(n), "z": z, "ux": np.zeros(n), "uy": np.zeros(n),
+         "uz": np.full(n, vz), "gaminv": np.ones(n)}
+    _push(p, (0.0, 0.0, 0.0), dt, center, tables=tables, zlmin=zlmin, dzl=dzl)
+    kick = p["ux"][:-1] / p["ux"][-1]
+    assert p["ux"][-1] != 0.0
+    assert np.allclose(kick, f, rtol=1e-9, atol=0), kick
