@@ -68,3 +68,55 @@ def test_ctypes_mirror_matches_the_header(tmp_path):
         assert getattr(_lib, pname) == c[cname], cname
     for name in ERRORS:
         assert _lib.ERRORS[c[name]] == name
+
+
+def _c_kind(param):
+    """Coarse class of one C parameter declaration."""
+    p = " ".join(param.replace("const", " ").split())
+    if "*" in p:
+        base = p.split("*")[0].strip()
+        depth = p.count("*")
+        return ("ptr", base if depth == 1 else "void")
+    typ = p.rsplit(" ", 1)[0] if " " in p else p
+    return {"double": ("double",), "int64_t": ("i64",), "int": ("i32",), "int32_t": ("i32",)}[typ]
+
+
+def _py_kind(t):
+    from warp_b200 import _lib
+    if t is ctypes.c_void_p:
+        return ("ptr", None)
+    if isinstance(t, type) and issubclass(t, ctypes._Pointer):
+        target = t._type_
+        names = {ctypes.c_double: "double", ctypes.c_int32: "int32_t", ctypes.c_int64: "int64_t",
+                 ctypes.c_void_p: "void"}
+        for cname, pname in STRUCTS.items():
+            if target is getattr(_lib, pname):
+                return ("ptr", cname)
+        return ("ptr", names.get(target, "?"))
+    if t is ctypes.c_double:
+        return ("double",)
+    if t is ctypes.c_int64:
+        return ("i64",)
+    if t is ctypes.c_int:
+        return ("i32",)
+    raise AssertionError(t)
+
+
+def test_ctypes_argtypes_match_the_prototypes():
+    import re
+    from warp_b200 import _lib
+    text = open(os.path.join(ROOT, "include", "warp_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    protos = {m.group(1): m.group(2) for m in re.finditer(r"\bint\s+(wg_\w+)\s*\(([^;]*)\)\s*;", text, re.S)}
+    assert set(protos) == set(_lib.SIGNATURES), set(protos) ^ set(_lib.SIGNATURES)
+    for name, args in _lib.SIGNATURES.items():
+        params = [s for s in (x.strip() for x in protos[name].split(",")) if s and s != "void"]
+        assert len(params) == len(args), name
+        for c, t in zip(params, args):
+            ck, pk = _c_kind(c), _py_kind(t)
+            assert ck[0] == pk[0], (name, c)
+            # typed ctypes pointers must point at the declared type; c_void_p takes any pointer
+            if ck[0] == "ptr" and pk[1] is not None:
+                same = pk[1] == ck[1] or (pk[1] == "int32_t" and ck[1] == "int") or \
+                    (pk[1] == "void" and ck[1] in ("wg_ctx", "void"))
+                assert same, (name, c, pk)
