@@ -82,6 +82,30 @@ def test_fetch_e_bitexact():
     assert np.array_equal(eh[0], ex) and np.array_equal(eh[1], ey) and np.array_equal(eh[2], ez)
 
 
+def test_fetche_slice_as_warp_hands_it_over():
+    """fetche(pgroup, ipmin, np) gathers particles ipmin .. ipmin+np-1
+    (1-based, w3d.ipminfsapi / npfsapi) into that slice of ex/ey/ez and
+    leaves the rest of the arrays alone."""
+    cfg, s, p, pg = _setup(20_000)
+    rng = np.random.default_rng(21)
+    s.phi = np.asfortranarray(rng.standard_normal((s.nx + 3, s.ny + 3, s.nz + 3)))
+    s.fetche(pg)
+    whole = [pg.ex.clone(), pg.ey.clone(), pg.ez.clone()]
+    for e in (pg.ex, pg.ey, pg.ez):
+        e.fill_(7.0)
+    s.fetche(pg, ipmin=1001, np=5000)
+    for e, w in zip((pg.ex, pg.ey, pg.ez), whole):
+        assert torch.equal(e[1000:6000], w[1000:6000])
+        assert bool((e[:1000] == 7.0).all()) and bool((e[6000:] == 7.0).all())
+    s.fetche(pg, ipmin=pg.np + 1, np=0)  # an empty slice is allowed
+    with pytest.raises(ValueError):
+        s.fetche(pg, ipmin=0, np=10)
+    with pytest.raises(ValueError):
+        s.fetche(pg, ipmin=pg.np - 5, np=10)
+    with pytest.raises(ValueError):
+        s.fetche(ipmin=1, np=10)
+
+
 def test_advance_bitexact_with_quads_and_pipe():
     from warp_b200 import pic
     cfg, s, p, pg = _setup(100_000)

@@ -322,19 +322,34 @@ class MultiGridB200(FieldSolver):
         _lib.check(_lib.lib.wg_residual_field(self._h, self.mgparam, ctypes.c_void_p(out.data_ptr())))
         return out.view(self.nz + 1, self.ny + 1, self.nx + 1).permute(2, 1, 0)
 
-    def fetche(self, pgroup=None):
+    def fetche(self, pgroup=None, ipmin=None, np=None):
         """fetche -> fetchfieldfrompositions -> sete3d (multigrid.py:521-558,
-        w3d.F:3963): E at the particles, written to pgroup.ex/ey/ez."""
+        w3d.F:3963): E at the particles, written to pgroup.ex/ey/ez.
+
+        ipmin (1-based) and np select the particles ipmin .. ipmin+np-1 of
+        one group, the slice that WARP's fetche3d zeroes and hands to the
+        registered solver (w3d.ipminfsapi, w3d.npfsapi; fieldsolver.py:
+        1434-1511, w3d.F:10978-11060); E outside the slice is left as it is."""
         self._bind_stream()
         if self._lcorrectede:
             self.getconductorobject()
-        groups = self.pgroups if pgroup is None else [pgroup]
-        for pg in groups:
-            pg.ex.zero_()
-            pg.ey.zero_()
-            pg.ez.zero_()
-            _lib.check(_lib.lib.wg_fetch_e(self._h, pg.x.data_ptr(), pg.y.data_ptr(), pg.z.data_ptr(),
-                                           pg.ex.data_ptr(), pg.ey.data_ptr(), pg.ez.data_ptr(), pg.np))
+        if ipmin is not None or np is not None:
+            if pgroup is None or ipmin is None or np is None:
+                raise ValueError("fetche: a particle slice needs pgroup, ipmin and np")
+            i0, n = int(ipmin) - 1, int(np)
+            if i0 < 0 or n < 0 or i0 + n > pgroup.np:
+                raise ValueError("fetche: slice %d..%d outside the %d particles" % (i0 + 1, i0 + n, pgroup.np))
+            views = [getattr(pgroup, k)[i0:i0 + n] for k in ("x", "y", "z", "ex", "ey", "ez")]
+        else:
+            groups = self.pgroups if pgroup is None else [pgroup]
+            views = None
+        for v in ([views] if views is not None else
+                  [[getattr(pg, k) for k in ("x", "y", "z", "ex", "ey", "ez")] for pg in groups]):
+            n = int(v[0].shape[0])
+            for e in v[3:]:
+                e.zero_()
+            if n:
+                _lib.check(_lib.lib.wg_fetch_e(self._h, *(t.data_ptr() for t in v), n))
 
     fetchfieldfrompositions = fetche
 
