@@ -250,7 +250,7 @@ int wg_particle_permute(wg_ctx* ctx, const int64_t* perm, const wg_particles* sr
 /* ---- instrumentation (no reference counterpart: replaces the wall-clock
  * sub-timers lf3dtimesubs / lw3dtimesubs, f3d.v:1308, w3d.v:1396) -------- */
 
-#define WG_PROF_SOR0 0     /* SOR half pass on the finest level (units: nodes) */
+#define WG_PROF_SOR0 0     /* SOR half pass on the finest level, k_sor_bulk launches (units: nodes) */
 #define WG_PROF_DEPOSIT 1  /* charge deposition (units: particles) */
 #define WG_PROF_ADVANCE 2  /* fused gather + push (units: particles) */
 #define WG_PROF_RESID0 3   /* residual on the finest level (units: nodes) */

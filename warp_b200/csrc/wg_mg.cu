@@ -1266,8 +1266,8 @@ struct Solver {
       const int nbz = bulk ? (int)cdiv(nzr, zpt) : 0;
       const int nspz = merged ? (int)cdiv((size_t)nsub, 256u * gx * gy) : 0;
       if (parity == 0 && phi_zero && !usev && merged) {
-        // phi was not zeroed: this launch writes all of it (from_zero_ok)
-        int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
+        // phi was not zeroed: this launch writes all of it (from_zero_ok).
+        // It is not timed as WG_PROF_SOR0, which times k_sor_bulk only.
         constexpr int fz = 4;
         const unsigned fgx = cdiv(cdiv(L.d.nx + 3, 2), 32), fgy = cdiv(L.d.ny + 3, 8);
         const int fbz = (int)cdiv(L.d.nz + 3, fz);
@@ -1275,7 +1275,6 @@ struct Solver {
         launch(k_sor_from_zero<T, fz>, dim3(fgx, fgy, fbz + fspz), blk, 0, phi, rhs, L.d.nx, L.d.ny, L.d.nz, R.ixmin,
                R.ixmax, R.iymin, R.iymax, R.izmin, izmax, (T)k.cx, (T)k.cy, (T)k.cz, (T)k.spm1, wtz, fbz, ca, B, k,
                o->lcndbndy);
-        c->prof_end(pe);
       } else if (nbz + nspz > 0) {
         int pe = prof_begin(l, WG_PROF_SOR0, (double)L.nr);
         launch(k_sor_bulk<T, zpt>, dim3(gx, gy, nbz + nspz), blk, 0, 
