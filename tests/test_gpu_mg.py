@@ -84,6 +84,31 @@ def test_gpu_mg_conductors_bitexact(bounds, nz):
     assert np.array_equal(gphi[idx[:, 0], idx[:, 1], idx[:, 2]], iv[sel])
 
 
+# MultiGrid3D's solver options away from their defaults: over-relaxation,
+# several or no down passes, extra up passes, fewer levels
+OPTIONS = [dict(mgparam=1.5), dict(downpasses=2, uppasses=3), dict(downpasses=0, uppasses=2),
+           dict(mgmaxlevels=3), dict(mgparam=1.0, downpasses=1, uppasses=2, mgmaxlevels=4)]
+
+
+@pytest.mark.parametrize("opts", OPTIONS, ids=["-".join("%s%s" % kv for kv in o.items()) for o in OPTIONS])
+@pytest.mark.parametrize("bounds", [(0, 0, 0, 0, 2, 2), (0, 0, 0, 0, 0, 0)])
+def test_gpu_mg_solver_options_bitexact(opts, bounds):
+    s, shapes, rho = _conductor_case()
+    sv = H.make_solver(s.nx, s.ny, s.nz, (s.xmmin, s.ymmin, s.zmmin), (s.xmmax, s.ymmax, s.zmmax), bounds,
+                       mgtol=1e-9, **opts)
+    for sh in shapes:
+        sv.installconductor(sh)
+    sv.rho = rho
+    sv.phi = np.zeros((sv.nx + 3, sv.ny + 3, sv.nz + 3), order="F")
+    sv.solve()
+    gphi = sv.phi.cpu().numpy()
+    oc = H.oracle_conductors(sv, shapes)
+    ophi = np.zeros_like(gphi, order="F")
+    it, err = oracle.mgsolve(ophi, rho, sv.dx, sv.dy, sv.dz, bounds, conductors=oc, mgtol=1e-9, **opts)
+    assert sv.mgiters == it < 100
+    assert np.array_equal(gphi, ophi), "max |gpu - oracle| = %g" % np.max(np.abs(gphi - ophi))
+
+
 def test_gpu_mixed_precision_reaches_fp64_tolerance():
     s, shapes, rho = _conductor_case(64, 64, 96)
     ref = H.make_solver(s.nx, s.ny, s.nz, (s.xmmin, s.ymmin, s.zmmin), (s.xmmax, s.ymmax, s.zmmax),
