@@ -85,17 +85,21 @@ def test_gpu_mg_conductors_bitexact(bounds, nz):
 
 
 # MultiGrid3D's solver options away from their defaults: over-relaxation,
-# several or no down passes, extra up passes, fewer levels
+# several or no down passes, extra up passes, fewer levels, and the
+# conductor stencil without the subgrid distances (lcndbndy False)
 OPTIONS = [dict(mgparam=1.5), dict(downpasses=2, uppasses=3), dict(downpasses=0, uppasses=2),
-           dict(mgmaxlevels=3), dict(mgparam=1.0, downpasses=1, uppasses=2, mgmaxlevels=4)]
+           dict(mgmaxlevels=3), dict(mgparam=1.0, downpasses=1, uppasses=2, mgmaxlevels=4),
+           dict(lcndbndy=False, mgtol=1e-6)]
 
 
 @pytest.mark.parametrize("opts", OPTIONS, ids=["-".join("%s%s" % kv for kv in o.items()) for o in OPTIONS])
 @pytest.mark.parametrize("bounds", [(0, 0, 0, 0, 2, 2), (0, 0, 0, 0, 0, 0)])
 def test_gpu_mg_solver_options_bitexact(opts, bounds):
     s, shapes, rho = _conductor_case()
+    opts = dict(opts)
+    mgtol = opts.pop("mgtol", 1e-9)
     sv = H.make_solver(s.nx, s.ny, s.nz, (s.xmmin, s.ymmin, s.zmmin), (s.xmmax, s.ymmax, s.zmmax), bounds,
-                       mgtol=1e-9, **opts)
+                       mgtol=mgtol, **opts)
     for sh in shapes:
         sv.installconductor(sh)
     sv.rho = rho
@@ -104,7 +108,7 @@ def test_gpu_mg_solver_options_bitexact(opts, bounds):
     gphi = sv.phi.cpu().numpy()
     oc = H.oracle_conductors(sv, shapes)
     ophi = np.zeros_like(gphi, order="F")
-    it, err = oracle.mgsolve(ophi, rho, sv.dx, sv.dy, sv.dz, bounds, conductors=oc, mgtol=1e-9, **opts)
+    it, err = oracle.mgsolve(ophi, rho, sv.dx, sv.dy, sv.dz, bounds, conductors=oc, mgtol=mgtol, **opts)
     assert sv.mgiters == it < 100
     assert np.array_equal(gphi, ophi), "max |gpu - oracle| = %g" % np.max(np.abs(gphi - ophi))
 
