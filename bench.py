@@ -255,6 +255,13 @@ def cpu_reference_step(cfg, sample, vcycles):
     return step, desc, {"t_particles_sample": t_part, "t_vcycle": t_v, "t_residual": t_r}
 
 
+def job_config(form, world):
+    """The config object of the JSON line (both arms)."""
+    return {"workload": "256x256x512 cells, 5e7 protons, pipe + FODO, 1e-6 relres", "form": form,
+            "parallelism": "replicas" if world > 1 else "single",
+            "flush": "inputs larger than L2 (phi 271 MB, particles 2.8 GB)"}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -277,8 +284,7 @@ def main():
         line = {"metric": METRIC, "value": v, "unit": "steps/s", "impl": "reference", "n_gpus": 0,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-                "config": {"workload": "256x256x512 cells, 5e7 protons, pipe + FODO, 1e-6 relres",
-                           "flush": "inputs larger than L2"},
+                "config": job_config("reference arithmetic (FP64 oracle on the host cores)", 1),
                 "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc},
                 "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -341,9 +347,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if headline == "plain" else "f32+f64",
             "data": "synthetic (seeded semi-Gaussian beam)",
-            "config": {"workload": "256x256x512 cells, 5e7 protons, pipe + FODO, 1e-6 relres",
-                       "form": headline, "parallelism": "replicas" if world > 1 else "single",
-                       "flush": "inputs larger than L2 (phi 271 MB, particles 2.8 GB)"},
+            "config": job_config(headline, world),
             "forms": results, "gpu_launches": results[headline]["launches"],
             "e2e": {"value": 1000.0 / e2e_ms * world, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
