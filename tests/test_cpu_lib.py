@@ -29,8 +29,16 @@ def test_library_exports_header_symbols():
 
 
 def test_library_is_sm100a_build():
-    from warp_b200 import _lib
-    assert os.path.exists(_lib.LIBPATH)
+    """The in-tree library exists and the build compiles every source under
+    warp_b200/csrc for sm_100a only, with FMA contraction off."""
+    from warp_b200 import _lib, build
+    assert os.path.exists(_lib.LIBPATH) and _lib.LIBPATH == build.LIB
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    srcs = sorted(f for f in os.listdir(build.CSRC) if f.endswith((".cu", ".cpp")))
+    assert sorted(build.SOURCES) == srcs
+    import inspect
+    body = inspect.getsource(build.build)
+    assert "--fmad=false" in body and "-lineinfo" in body
 
 
 def test_lattice_tables_match_oracle():
