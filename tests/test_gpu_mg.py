@@ -175,3 +175,22 @@ def test_gpu_field_energy_bitexact():
     ref = oracle.ese(rho, s.phi.cpu().numpy(), s.dx, s.dy, s.dz)
     assert e == ref
     assert e != 0.0
+
+
+def test_gpu_find_mgparam_tunes_a_converging_solver():
+    """MultiGrid3D.find_mgparam on the conductor problem: the parameters it
+    settles on are in range and solve the problem within mgmaxiters."""
+    s, shapes, rho = _conductor_case()
+    for sh in shapes:
+        s.installconductor(sh)
+    s.rho = rho
+    s.phi = np.zeros((s.nx + 3, s.ny + 3, s.nz + 3), order="F")
+    s.solve()
+    default_iters = s.mgiters
+    s.find_mgparam(log=lambda *a: None)
+    assert 0.01 < s.mgparam <= 2.0 and s.downpasses >= 1 and s.uppasses >= 1
+    s.phi = np.zeros((s.nx + 3, s.ny + 3, s.nz + 3), order="F")
+    s.solve()
+    assert s.converged and s.mgiters < s.mgmaxiters
+    print("find_mgparam: mgparam %.3f, passes %d/%d, V-cycles %d (default %d)" % (
+        s.mgparam, s.downpasses, s.uppasses, s.mgiters, default_iters))

@@ -293,6 +293,13 @@ class MultiGridB200(FieldSolver):
 
     dosolve = solve
 
+    def find_mgparam(self, lsavephi=False, resetpasses=1, log=print):
+        """MultiGrid3D.find_mgparam (multigrid.py:827-831,
+        find_mgparam.py:28-237): tunes mgparam, downpasses and uppasses for
+        the fastest solve of the problem the solver holds."""
+        from .find_mgparam import find_mgparam
+        return find_mgparam(self, lsavephi=lsavephi, resetpasses=resetpasses, log=log)
+
     def relresidual(self):
         self._bind_stream()
         self.getconductorobject()
