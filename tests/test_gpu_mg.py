@@ -194,3 +194,27 @@ def test_gpu_find_mgparam_tunes_a_converging_solver():
     assert s.converged and s.mgiters < s.mgmaxiters
     print("find_mgparam: mgparam %.3f, passes %d/%d, V-cycles %d (default %d)" % (
         s.mgparam, s.downpasses, s.uppasses, s.mgiters, default_iters))
+
+
+def test_gpu_setconductorvoltage_matches_oracle():
+    """setconductorvoltage changes one conductor's voltage (by id or by the
+    conductor object); the next solve equals the oracle's with the new
+    voltage bit for bit."""
+    s, shapes, rho = _conductor_case()
+    for sh in shapes:
+        s.installconductor(sh)
+    s.rho = rho
+    s.solve()
+    s.setconductorvoltage(1.3, condid=shapes[1].condid)
+    s.setconductorvoltage(-0.9, condid=shapes[3])
+    assert shapes[1].voltage == 1.3 and shapes[3].voltage == -0.9
+    s.phi = np.zeros((s.nx + 3, s.ny + 3, s.nz + 3), order="F")
+    s.solve()
+    gphi = s.phi.cpu().numpy()
+    oc = H.oracle_conductors(s, shapes)
+    ophi = np.zeros_like(gphi, order="F")
+    it, err = oracle.mgsolve(ophi, rho, s.dx, s.dy, s.dz, (0,) * 6, conductors=oc, mgtol=1e-10)
+    assert s.mgiters == it
+    assert np.array_equal(gphi, ophi)
+    with pytest.raises(NotImplementedError):
+        s.setconductorvoltage([0.0] * (s.nz + 1), condid=shapes[1].condid)

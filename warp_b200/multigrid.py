@@ -160,6 +160,26 @@ class MultiGridB200(FieldSolver):
             raise Exception("conductor was not found")
         self._conductors_installed = False
 
+    def setconductorvoltage(self, voltage, condid=0, discrete=False, setvinject=False):
+        """setconductorvoltage (multigrid.py:252-260, generateconductors.py:
+        2910-3000) for a scalar voltage: every installed conductor with the
+        id condid (or the conductor object itself) takes the voltage, and its
+        data is regenerated at the next solve. Voltages given per z cell or
+        as a function of position, and setvinject (particle injection), are
+        not supported here and raise."""
+        if setvinject:
+            raise NotImplementedError("setconductorvoltage: setvinject (particle injection) is not supported")
+        if callable(voltage) or np.ndim(voltage) != 0:
+            raise NotImplementedError("setconductorvoltage: only a scalar voltage is supported")
+        cid = getattr(condid, "condid", condid)
+        hit = False
+        for cond, _ in self.conductordatalist:
+            if cond.condid == cid:
+                cond.voltage = float(voltage)
+                hit = True
+        if hit:
+            self._conductors_installed = False
+
     def clearconductors(self):
         self.conductordatalist = []
         self._conductors_installed = False
