@@ -88,3 +88,22 @@ def test_oracle_field_energy_matches_direct_sum():
     e = oracle.ese(rho, phi, 0.1, 0.2, 0.05)
     ref = 0.1 * 0.2 * 0.05 * 0.5 * np.sum(rho * phi[1:-1, 1:-1, 1:-1])
     assert abs(e - ref) <= 1e-12 * np.sum(np.abs(rho * phi[1:-1, 1:-1, 1:-1]))
+
+
+def test_product_never_imports_the_oracle():
+    """The oracle is test infrastructure: no module of the warp_b200 package
+    imports it, so no product path can route through it."""
+    import ast
+    pkg = os.path.join(ROOT, "warp_b200")
+    for name in sorted(os.listdir(pkg)):
+        if not name.endswith(".py"):
+            continue
+        tree = ast.parse(open(os.path.join(pkg, name)).read())
+        for node in ast.walk(tree):
+            if isinstance(node, ast.Import):
+                mods = [a.name for a in node.names]
+            elif isinstance(node, ast.ImportFrom):
+                mods = [node.module or ""]
+            else:
+                continue
+            assert not any(m == "oracle" or m.startswith("oracle.") for m in mods), (name, mods)
