@@ -27,10 +27,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "PIC steps/s, 256²×512 grid/5e7 ptcl: plain vs learned+mixed @1e-6 residual"
 WORKLOAD = "B"
-# V-cycles per warm-started solve of the FP64 form at 1e-6 relative
-# residual on this workload (the oracle runs the identical algorithm); used
-# to extrapolate the CPU reference's per-V-cycle sample to one step.
-DEFAULT_REF_VCYCLES = 6
 # particles are re-sorted by cell every SORT_INTERVAL steps (inside the timed steps)
 SORT_INTERVAL = 10
 # DRAM bytes (read + write) per finest-level node of one k_sor_bulk<float>
@@ -50,8 +46,8 @@ def parse():
     ap.add_argument("--forms", default="plain,mixed")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-vcycles", type=float, default=None)
-    ap.add_argument("--ref-sample", type=int, default=1_000_000)
+    ap.add_argument("--cpu-steps", type=int, default=2,
+                    help="oracle steps timed for cpu_baseline (continuing the GPU run's state)")
     ap.add_argument("--npart", type=int, default=None, help="override the particle count (profiling runs)")
     return ap.parse_args()
 
@@ -207,87 +203,67 @@ def e2e_steps(run, steps):
     return e0.elapsed_time(e1) / steps, nbytes, nbytes
 
 
-def cpu_reference_step(cfg, sample, vcycles):
-    """Oracle timing of one step on a bounded sample: deposit + gather + push
-    of `sample` particles (scaled to the full count) and one V-cycle plus one
-    residual evaluation on the full grid (scaled by `vcycles`)."""
-    import numpy as np
-
-    from oracle import oracle
-    from warp_b200 import pic
-    from warp_b200.lattice import fodo
-    from warp_b200.particles import beam_weight, semigaussian
-    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
-    dx = (cfg["xmmax"] - cfg["xmmin"]) / nx
-    dy = (cfg["ymmax"] - cfg["ymmin"]) / ny
-    dz = (cfg["zmmax"] - cfg["zmmin"]) / nz
-    mins = (cfg["xmmin"], cfg["ymmin"], cfg["zmmin"])
-    p = semigaussian(sample, seed=cfg["seed"], radius=cfg["radius"], mismatch=cfg["mismatch"],
-                     angle_rms=cfg["angle_rms"], zmin=cfg["zmmin"], zmax=cfg["zmmax"], ekin_ev=cfg["ekin_ev"])
-    w = beam_weight(cfg["current"], cfg["zmmax"] - cfg["zmmin"], cfg["npart"])
-    lat = fodo(cfg["quad_gradient"], cfg["quad_length"], cfg["period"])
-    tables = lat.tables(cfg["zmmin"], dz, nz + 1)
-    oc = oracle.Conductors(nx, ny, nz, dx, dy, dz, *mins)
-    oc.add_shape("ZCylinderOut", cfg["pipe_radius"], 100.0, 0.0, 0., 0., 0.5 * (cfg["zmmin"] + cfg["zmmax"]), 1)
-    oc.finalize()
-    phi = np.zeros((nx + 3, ny + 3, nz + 3), order="F")
-    rho = np.zeros((nx + 1, ny + 1, nz + 1), order="F")
-    from warp_b200.constants import echarge, proton_mass
-    dt = pic.timestep(cfg)
-    t0 = time.perf_counter()
-    ex, ey, ez = oracle.sete(phi, p["x"], p["y"], p["z"], dx, dy, dz, *mins)
-    oracle.push_fullv(p, ex, ey, ez, echarge, proton_mass, dt, tables, cfg["zmmin"], dz, cfg["zmmin"],
-                      cfg["zmmax"], cfg["pipe_radius"])
-    oracle.setrho(rho, p["x"], p["y"], p["z"], echarge, w * cfg["npart"] / sample, dx, dy, dz, *mins,
-                  gaminv=p["gaminv"])
-    oracle.rhobc(rho, (0, 0, 0, 0, 2, 2))
-    t_part = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    oracle.mgsolve(phi, rho, dx, dy, dz, (0, 0, 0, 0, 2, 2), conductors=oc, mgmaxiters=1, mgtol=0.0)
-    t_v = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    oracle.relresidual(phi, rho, dx, dy, dz, (0, 0, 0, 0, 2, 2), oc)
-    t_r = time.perf_counter() - t0
-    step = t_part * cfg["npart"] / sample + t_v * vcycles + t_r * (vcycles + 1)
-    desc = ("oracle (C++ FP64 restatement, %d host threads): gather+push+deposit of %d of %d particles scaled "
-            "x%g, one V-cycle and one residual on the full %dx%dx%d grid scaled to %g V-cycles per solve"
-            % (oracle.threads(), sample, cfg["npart"], cfg["npart"] / sample, nx, ny, nz, vcycles))
-    return step, desc, {"t_particles_sample": t_part, "t_vcycle": t_v, "t_residual": t_r}
+def oracle_steps(orun, warmup, steps):
+    """Times `steps` full PIC steps of the oracle run after `warmup` untimed
+    ones; returns (seconds per step, V-cycles per solve)."""
+    for _ in range(warmup):
+        orun.step()
+    vc, t = 0, 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        vc += orun.step()
+        t += time.perf_counter() - t0
+    return t / max(steps, 1), vc / max(steps, 1)
 
 
-def job_config(form, world):
-    """The config object of the JSON line (both arms)."""
-    return {"workload": "256x256x512 cells, 5e7 protons, pipe + FODO, 1e-6 relres", "form": form,
+def oracle_desc(cfg, threads, steps, npart, start):
+    return ("oracle (C++ FP64 restatement of the reference's Fortran, %d host threads): %d full PIC steps "
+            "(gather+push, deposit and multigrid to 1e-6 relative residual) of %d particles on the %dx%dx%d "
+            "grid, %s" % (threads, steps, npart, cfg["nx"], cfg["ny"], cfg["nz"], start))
+
+
+def job_config(cfg, world):
+    """The config object of the JSON line, identical in both arms."""
+    n = cfg["npart"]
+    e = len(str(n)) - len(str(n).rstrip("0"))
+    npart = "%de%d" % (n // 10 ** e, e) if e >= 3 else str(n)
+    return {"workload": "%dx%dx%d cells, %s protons, pipe%s + FODO, 1e-6 relres"
+                        % (cfg["nx"], cfg["ny"], cfg["nz"], npart, " + 4 rods" if cfg.get("rods") else ""),
             "parallelism": "replicas" if world > 1 else "single",
-            "flush": "inputs larger than L2 (phi 271 MB, particles 2.8 GB)"}
+            "flush": "inputs larger than L2 (phi %d MB, particles %.1f GB)"
+                     % (8 * (cfg["nx"] + 3) * (cfg["ny"] + 3) * (cfg["nz"] + 3) // 10 ** 6, 56e-9 * n)}
+
+
+def reference_arm(args, cfg, world):
+    """The reference's arithmetic on the host cores: the oracle's PIC steps
+    on the same workload, nothing of the CUDA library loaded."""
+    from oracle import oracle
+    from oracle.espic import OracleESPIC
+    orun = OracleESPIC(cfg, tolkind="relres", mgtol=1e-6)
+    orun.generate()
+    sec, vc = oracle_steps(orun, args.warmup, args.steps)
+    threads = oracle.threads()
+    v = 1.0 / sec
+    desc = oracle_desc(cfg, threads, args.steps, len(orun.p["x"]),
+                       "after %d untimed steps from the loaded beam" % args.warmup)
+    return {"metric": METRIC, "value": v, "unit": "steps/s", "impl": "reference", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded semi-Gaussian beam)",
+            "config": job_config(cfg, world), "form": "reference arithmetic (FP64 oracle on the host cores)",
+            "vcycles_per_solve": vc,
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     args = parse()
     rank, world, local = dist_env()
-    from warp_b200 import pic
-    cfg = pic.workload(args.workload) if args.npart is None else pic.workload(args.workload, npart=args.npart)
+    from warp_b200.workloads import workload
+    cfg = workload(args.workload) if args.npart is None else workload(args.workload, npart=args.npart)
     if args.impl == "reference":
         if rank != 0:
             return 0
-        vcyc = args.ref_vcycles if args.ref_vcycles is not None else DEFAULT_REF_VCYCLES
-        times = []
-        desc = ""
-        for i in range(args.warmup + args.steps):
-            st, desc, _ = cpu_reference_step(cfg, args.ref_sample, vcyc)
-            if i >= args.warmup:
-                times.append(st)
-        sec = sum(times) / len(times)
-        from oracle import oracle
-        threads = oracle.threads()
-        v = 1.0 / sec
-        line = {"metric": METRIC, "value": v, "unit": "steps/s", "impl": "reference", "n_gpus": 0,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-                "config": job_config("reference arithmetic (FP64 oracle on the host cores)", 1),
-                "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc},
-                "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        print(json.dumps(reference_arm(args, cfg, world)))
         return 0
 
     import torch
@@ -347,18 +323,25 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if headline == "plain" else "f32+f64",
             "data": "synthetic (seeded semi-Gaussian beam)",
-            "config": job_config(headline, world),
+            "config": job_config(cfg, world), "form": headline,
             "forms": results, "gpu_launches": results[headline]["launches"],
             "e2e": {"value": 1000.0 / e2e_ms * world, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": roofline, "clocks": clk}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        vc = results.get("plain", results[headline])["vcycles_per_solve"]
-        st, desc, parts = cpu_reference_step(cfg, args.ref_sample, vc)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.cpu_steps > 0:
+        # the oracle continues the GPU run from its current particles and
+        # phi for a few full steps (a bounded sample of the same workload)
         from oracle import oracle
-        line["cpu_baseline"] = {"value": 1.0 / st, "unit": "steps/s", "cores": oracle.threads(), "kind": "port",
-                                "sample": desc,
-                                "parts_s": parts}
+        from oracle.espic import OracleESPIC
+        pg = head_run.pgroup
+        orun = OracleESPIC(cfg, particles=pg.to_numpy(), w=pg.w, phi=head_run.solver.phi.cpu().numpy(),
+                           vsync=head_run.vsync)
+        sec, vc = oracle_steps(orun, 0, args.cpu_steps)
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "steps/s", "cores": oracle.threads(), "kind": "port",
+                                "sample": oracle_desc(cfg, oracle.threads(), args.cpu_steps, len(orun.p["x"]),
+                                                      "continuing the GPU run's particles and phi"),
+                                "vcycles_per_solve": vc}
+        del orun
     if world > 1:
         tdist.barrier()
         tdist.destroy_process_group()

@@ -1,12 +1,23 @@
-"""wg_deposit_noalloc (deposit into caller memory, accumulator in a fixed
-library array, no allocation) against the context deposit wg_deposit on the
-same particles: two calls in a row (clear, then accumulate), and the size
-limit. Collected last so that it also runs after every other test."""
+"""wg_deposit_noalloc: the deposit for callers that cannot let a library
+allocate device memory (a host code that manages every device buffer
+itself, or one that keeps cudaMalloc/cudaFree, which synchronize the device,
+out of its step). Its fixed-point accumulator is a fixed array inside the
+library, so it takes no context and allocates nothing.
+
+Checked through the C ABI against the context deposit wg_deposit on the same
+particles, two calls in a row (clear, then accumulate): both run the same
+fixed-point kernels with the same cell sizes, so the results must agree bit
+for bit. The first call is also checked against the oracle's FP64 running
+sum, device memory must not change across the calls, and grids above the
+limit are rejected. Collected last (file name) so that it also runs after
+every other test."""
 import ctypes
 
 import numpy as np
 import pytest
 import torch
+
+from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -55,18 +66,29 @@ def test_noalloc_deposit_matches_context_deposit_twice():
     s.loadrho(pgroups=[g1], lfinalize_rho=False)
     torch.cuda.synchronize()
     r1 = s.rho.cpu().numpy().ravel(order="F")
-    scale = np.max(np.abs(r1))
+    assert np.array_equal(a1, r1)
+    # and against the oracle's FP64 running sum (the fixed-point rounding of
+    # each weight to 2^-46 is the only difference)
+    ref = np.zeros((cfg["nx"] + 1, cfg["ny"] + 1, cfg["nz"] + 1), order="F")
+    oracle.setrho(ref, p1["x"], p1["y"], p1["z"], g1.q, g1.w, s.dx, s.dy, s.dz, s.xmmin, s.ymmin, s.zmmin,
+                  gaminv=p1["gaminv"])
+    ref = ref.ravel(order="F")
+    scale = np.max(np.abs(ref))
     assert scale > 0
-    assert np.max(np.abs(a1 - r1)) <= 1e-13 * scale
+    assert np.max(np.abs(a1 - ref)) <= 1e-13 * scale
 
-    # second call right after: rho += deposit(p2); the accumulator must have been cleared
+    # second call right after: rho += deposit(p2); the accumulator must have
+    # been cleared, and nothing is allocated on the device
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     _lib.check(_noalloc(grid, g2, rho, 0))
     torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
     a2 = rho.cpu().numpy()
     _lib.check(_lib.lib.wg_deposit(s._h, ctypes.byref(g2.cstruct()), 0))
     torch.cuda.synchronize()
     r2 = s.rho.cpu().numpy().ravel(order="F")
-    assert np.max(np.abs(a2 - r2)) <= 1e-13 * np.max(np.abs(r2))
+    assert np.array_equal(a2, r2)
     assert not np.array_equal(a2, a1)
 
 

@@ -1206,8 +1206,10 @@ int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int
   }
   unsigned long long* flag = acc + kNoAllocMaxNodes;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  WG_TRY_CUDA(cudaMemsetAsync(acc, 0, (size_t)nr * sizeof(unsigned long long), s));
-  WG_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned long long), s));
+  // zeroed by kernels, as in wg_deposit: a cudaMemsetAsync may wait behind a
+  // caller's bulk copies on a copy engine
+  k_zero_u64<<<(unsigned)std::min<int64_t>((nr + 255) / 256, 148 * 16), 256, 0, s>>>(acc, (size_t)nr);
+  k_zero_u64<<<1, 32, 0, s>>>(flag, 1);
   const double dx = (G.xmmax - G.xmmin) / G.nx, dy = (G.ymmax - G.ymmin) / G.ny, dz = (G.zmmax - G.zmmin) / G.nz;
   GridP g{G.nx, G.ny, G.nz, dx, dy, dz, G.xmmin, G.ymmin, G.zmmin, 0.};
   if (p->np > 0) k_deposit<<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, acc);

@@ -13,6 +13,7 @@ import torch
 
 from . import _lib
 from .constants import clight, echarge, proton_mass
+from .workloads import beam_weight, semigaussian  # noqa: F401
 
 FIELDS = ("x", "y", "z", "ux", "uy", "uz", "gaminv")
 
@@ -93,29 +94,6 @@ class ParticleGroup:
         return int((self.gaminv != 0).sum().item())
 
 
-def semigaussian(n, seed=0, radius=2e-3, mismatch=0.0, angle_rms=5e-3, zmin=0.0, zmax=1.0, ekin_ev=1e6,
-                 mass=proton_mass, xcent=0.0, ycent=0.0):
-    """Seeded semi-Gaussian beam: uniform in an ellipse with semi-axes
-    radius*(1+mismatch) (x) and radius*(1-mismatch) (y), Gaussian transverse
-    angles of rms `angle_rms` (x' = ux/uz), uniform in z. Non-relativistic
-    push (lrelativ = false): gaminv = 1, uz = beta*c. Returns numpy arrays.
-    Philox counter-based generator, so the stream is reproducible."""
-    rng = np.random.Generator(np.random.Philox(seed))
-    gamma = 1. + ekin_ev * echarge / (mass * clight * clight)
-    beta = math.sqrt(1. - 1. / (gamma * gamma))
-    vz = beta * clight
-    r = np.sqrt(rng.random(n))
-    th = 2. * np.pi * rng.random(n)
-    ax, ay = radius * (1. + mismatch), radius * (1. - mismatch)
-    x = xcent + ax * r * np.cos(th)
-    y = ycent + ay * r * np.sin(th)
-    z = zmin + (zmax - zmin) * rng.random(n)
-    xp = angle_rms * rng.standard_normal(n)
-    yp = angle_rms * rng.standard_normal(n)
-    uz = np.full(n, vz)
-    return {"x": x, "y": y, "z": z, "ux": xp * vz, "uy": yp * vz, "uz": uz, "gaminv": np.ones(n)}
-
-
 def semigaussian_device(n, generator, radius=2e-3, mismatch=0.0, angle_rms=5e-3, zmin=0.0, zmax=1.0,
                         ekin_ev=1e6, mass=proton_mass, device="cuda"):
     """semigaussian() drawn on the device from a seeded torch.Generator (used
@@ -132,14 +110,6 @@ def semigaussian_device(n, generator, radius=2e-3, mismatch=0.0, angle_rms=5e-3,
     uy = angle_rms * torch.randn(n, **kw) * vz
     return {"x": x, "y": y, "z": z, "ux": ux, "uy": uy, "uz": torch.full((n,), vz, **{k: kw[k] for k in ("device", "dtype")}),
             "gaminv": torch.ones(n, device=device, dtype=torch.float64)}
-
-
-def beam_weight(current, length, n, ekin_ev=1e6, mass=proton_mass, charge=echarge):
-    """Real particles per macroparticle for a beam of `current` (A) filling
-    `length` (m): w = I L / (q v N)."""
-    gamma = 1. + ekin_ev * echarge / (mass * clight * clight)
-    v = math.sqrt(1. - 1. / (gamma * gamma)) * clight
-    return current * length / (charge * v * n)
 
 
 def semigaussian_matched(n, generator, z, a, b, ap, bp, emitx, emity, zmin, zmax, v, device="cuda"):

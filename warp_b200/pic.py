@@ -10,56 +10,18 @@ halfv (w3d.F:780 with lspecial at it == 0) and the steps after it fullv;
 ESPIC.synchv() brings the velocities back to the positions' time for
 diagnostics, after which the next step is halfv again.
 
-Workloads (synthetic, seeded):
-  WORKLOADS["A"]: 32x32x64 cells over 8 cm x 8 cm x 1 m, 2e5 protons at
-      1 MeV, semi-Gaussian (2 mm radius, 5 mrad rms angle, 10 mA), FODO of
-      hard-edge quads 10 cm long at +-15 T/m with 50 cm period, grounded pipe
-      of radius 3.5 cm, periodic z, 50 steps.
-  WORKLOADS["B"]: the same physics on 256x256x512 cells with 5e7 particles,
-      4 mm radius with 20% envelope mismatch, 1000 steps.
-  WORKLOADS["E"]: 256x256x1024 cells, 2e8 particles, plus four
-      electrostatic quadrupole rods (radius 1 cm, +-20 kV) inside the pipe.
+The synthetic workloads (A, B, D, E) are defined in warp_b200.workloads.
 """
-import math
-
 import numpy as np
 
 from . import conductors as cond
-from .constants import clight, echarge, proton_mass
+from .constants import echarge, proton_mass
 from .fieldsolver import registersolver
 from .lattice import fodo
 from .multigrid import MultiGridB200
-from .particles import ParticleGroup, beam_weight, semigaussian
-
-WORKLOADS = {
-    "A": dict(nx=32, ny=32, nz=64, npart=200_000, radius=2e-3, mismatch=0.0, nsteps=50, rods=False),
-    "B": dict(nx=256, ny=256, nz=512, npart=50_000_000, radius=4e-3, mismatch=0.2, nsteps=1000, rods=False),
-    "E": dict(nx=256, ny=256, nz=1024, npart=200_000_000, radius=4e-3, mismatch=0.2, nsteps=1000, rods=True),
-    # the box of B at half resolution: training grid of the learned warm start
-    "D": dict(nx=128, ny=128, nz=256, npart=4_000_000, radius=4e-3, mismatch=0.2, nsteps=8, rods=False),
-}
-
-COMMON = dict(xmmin=-0.04, xmmax=0.04, ymmin=-0.04, ymmax=0.04, zmmin=0.0, zmmax=1.0, ekin_ev=1.0e6,
-              angle_rms=5e-3, current=10e-3, quad_gradient=15.0, quad_length=0.10, period=0.50,
-              pipe_radius=0.035, rod_radius=0.01, rod_voltage=20e3, rod_center=0.0225, seed=0,
-              steps_per_period=50)
-
-
-def workload(name, **over):
-    cfg = dict(COMMON)
-    cfg.update(WORKLOADS[name])
-    cfg.update(over)
-    cfg["name"] = name
-    return cfg
-
-
-def beam_velocity(cfg):
-    gamma = 1. + cfg["ekin_ev"] * echarge / (proton_mass * clight * clight)
-    return math.sqrt(1. - 1. / (gamma * gamma)) * clight
-
-
-def timestep(cfg):
-    return (cfg["period"] / cfg["steps_per_period"]) / beam_velocity(cfg)
+from .particles import ParticleGroup
+from .workloads import (COMMON, WORKLOADS, beam_velocity, beam_weight,  # noqa: F401
+                        semigaussian, timestep, workload)
 
 
 class ESPIC:
