@@ -188,7 +188,7 @@ def e2e_steps(run, steps):
     pg = run.pgroup
     # the host owns the particle order in this mode: no device-side re-sort
     run.sort_interval = 0
-    host = {k: torch.empty(pg.np, dtype=torch.float64, pin_memory=True) for k in FIELDS}
+    host = {k: torch.empty(pg.np, dtype=pg.dtype, pin_memory=True) for k in FIELDS}
     for k in FIELDS:
         host[k].copy_(getattr(pg, k))
     run.step_host(host)  # warm-up (creates the copy streams)
@@ -199,7 +199,7 @@ def e2e_steps(run, steps):
     run.run_host(host, steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    nbytes = 8 * pg.np * len(FIELDS)
+    nbytes = sum(host[k].numel() * host[k].element_size() for k in FIELDS)
     return e0.elapsed_time(e1) / steps, nbytes, nbytes
 
 

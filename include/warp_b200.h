@@ -82,6 +82,16 @@ typedef struct {
   double q, m, w; /* charge, mass, macroparticle weight (sq, sm, sw) */
 } wg_particles;
 
+/* The same species stored in FP32 (28 bytes a particle instead of 56): the
+ * particle arrays of the mixed-precision form, whose push runs in FP32. The
+ * reference stores particles in FP64 only (top.pgroup); the _f32 entry
+ * points below are its routines on this storage. q, m and w stay FP64. */
+typedef struct {
+  float *x, *y, *z, *ux, *uy, *uz, *gaminv;
+  int64_t np;
+  double q, m, w;
+} wg_particles_f32;
+
 /* Parameters of one particle advance (padvnc3d, w3d.F:1575). */
 typedef struct {
   double dt;
@@ -218,6 +228,15 @@ int wg_set_correctede(wg_ctx* ctx, int on);
  * (stckxy3d, w3d.F:11473). A SYNCHV step pushes no position and applies no
  * boundary. An unknown center is WG_EINVAL. */
 int wg_advance(wg_ctx* ctx, const wg_particles* p, const wg_push_params* prm);
+/* The FP32-storage forms of wg_deposit, wg_deposit_add and wg_advance
+ * (setrho3d, padvnc3d; same citations). The deposit converts each position
+ * to FP64 and accumulates the same 64-bit fixed-point weights, so rho differs
+ * from the FP64 form only through the positions' FP32 rounding. The advance
+ * gathers E in FP64 from the FP64 phi at the FP32 positions, then kicks,
+ * rotates and drifts in FP32 (quads, periz and the pipe as wg_advance). */
+int wg_deposit_f32(wg_ctx* ctx, const wg_particles_f32* p, int zero_first);
+int wg_deposit_add_f32(wg_ctx* ctx, const wg_particles_f32* p);
+int wg_advance_f32(wg_ctx* ctx, const wg_particles_f32* p, const wg_push_params* prm);
 /* getzmmnt global moments (top.F:521-1444): out[0] live count, 1 xbar,
  * 2 ybar, 3 xrms, 4 yrms, 5 epsx, 6 epsy (x' = ux/uz), 7 reserved. FP64,
  * deterministic order. */
@@ -238,6 +257,13 @@ int wg_zmoments(wg_ctx* ctx, const wg_particles* p, const double* uxo, const dou
                 double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt,
                 double zmmntdtextmax, double* zmmnts0, double* zmmnts);
 
+/* wg_moments and wg_zmoments for FP32 storage (uxo/uyo/uzo are FP32 device
+ * arrays); the sums are FP64. */
+int wg_moments_f32(wg_ctx* ctx, const wg_particles_f32* p, double* out);
+int wg_zmoments_f32(wg_ctx* ctx, const wg_particles_f32* p, const float* uxo, const float* uyo, const float* uzo,
+                    double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt,
+                    double zmmntdtextmax, double* zmmnts0, double* zmmnts);
+
 /* Cell keys for sorting particles by cell, as particlesortxyzwithcopy
  * (top.F:5095-5130): key = ix + (nx+1)*(iy + (ny+1)*iz); lost particles get
  * (nx+1)(ny+1)(nz+1). keys: device int64 array of length np. */
@@ -246,6 +272,10 @@ int wg_particle_keys(wg_ctx* ctx, const wg_particles* p, int64_t* keys);
  * length np; src and dst must not overlap). With perm from a stable sort of
  * the keys this is particlesortbyindex (top.F:5132). */
 int wg_particle_permute(wg_ctx* ctx, const int64_t* perm, const wg_particles* src, const wg_particles* dst);
+/* The same two for FP32 storage (particlesortxyzwithcopy, top.F:5095-5132). */
+int wg_particle_keys_f32(wg_ctx* ctx, const wg_particles_f32* p, int64_t* keys);
+int wg_particle_permute_f32(wg_ctx* ctx, const int64_t* perm, const wg_particles_f32* src,
+                            const wg_particles_f32* dst);
 
 /* ---- instrumentation (no reference counterpart: replaces the wall-clock
  * sub-timers lf3dtimesubs / lw3dtimesubs, f3d.v:1308, w3d.v:1396) -------- */

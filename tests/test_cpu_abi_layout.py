@@ -18,6 +18,7 @@ STRUCTS = {
     "wg_solve_opts": "SolveOpts",
     "wg_solve_stats": "SolveStats",
     "wg_particles": "Particles",
+    "wg_particles_f32": "ParticlesF32",
     "wg_push_params": "PushParams",
 }
 CONSTANTS = {

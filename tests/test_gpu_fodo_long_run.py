@@ -8,11 +8,15 @@ tests/golden/fodo_long_run.npz (made by tests/golden/make_fodo_long_run.py).
   every period, the same live-particle counts, and the same V-cycle count
   in all but at most two of the 1001 solves. Over 1000 steps the only
   difference is the 2^-46 fixed-point rounding of the deposit.
-- Mixed form (FP32 V-cycles inside FP64 defect correction): the emittances
-  within 1e-4 relative of the FP64 oracle after 1000 steps, the stated
-  accuracy target of the mixed form, and at most two particles lost
-  differently. Its final phi and grid E (centred differences) are within
-  1e-9 of max|.| of the plain run's.
+- Mixed form (FP32 V-cycles inside FP64 defect correction, FP32 particles
+  with an FP32 push): the emittances within 1e-4 relative of the FP64
+  oracle after 1000 steps, the stated accuracy target of the mixed form,
+  and at most two particles lost differently. Its final phi and grid E
+  (centred differences) are within 1e-4 of max|.| of the plain run's, and
+  the particles' final positions and transverse velocities within 1e-4 of
+  the plain run's rms values (rms of the differences). The plain run
+  stands in for the oracle here: it matches the fixture's emittances
+  within 1e-9 with the same V-cycle counts.
 
 On the oracle the run responds linearly to small changes of the field: a
 1e-8 relative change of rho moves the emittance by about 1e-8 after 1000
@@ -33,6 +37,7 @@ FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fo
 def _run(precision, g):
     from warp_b200.multigrid import MultiGridB200
     from warp_b200.particles import ParticleGroup
+    dtype = torch.float32 if precision == "mixed" else torch.float64
     q, m, v, _ = F.species()
     npart = int(g["npart"])
     p = F.host_beam(npart, int(g["seed"]))
@@ -41,7 +46,7 @@ def _run(precision, g):
     s = MultiGridB200(F.NX, F.NY, F.NZ, xmin, -xmin, ymin, -ymin, zmin, -zmin, bounds=F.BOUNDS,
                       precision=precision, tolkind="mgerror", mgtol=float(g["mgtol"]), mgverbose=-1)
     s.setlattice(F.lattice())
-    pg = ParticleGroup(p, q=q, m=m, w=F.weight(npart))
+    pg = ParticleGroup(p, q=q, m=m, w=F.weight(npart), dtype=dtype)
     s.addpgroup(pg)
     s.loadrho()
     s.solve()
@@ -59,7 +64,8 @@ def _run(precision, g):
             mo = s.moments(pg)
             rec.append((mo["epsx"], mo["epsy"], mo["n"]))
     r = np.array(rec)
-    return r[:, 0], r[:, 1], r[:, 2].astype(np.int64), np.array(vcycles), s.phi.cpu().numpy()
+    parts = {k: v.astype(np.float64) for k, v in pg.to_numpy().items()}
+    return r[:, 0], r[:, 1], r[:, 2].astype(np.int64), np.array(vcycles), s.phi.cpu().numpy(), parts
 
 
 def _efield(phi):
@@ -77,7 +83,7 @@ def _rel(a, b):
 def test_fodo_1000_steps_plain_and_mixed_against_oracle():
     torch.cuda.set_device(0)
     g = np.load(FIXTURE)
-    ex, ey, live, vc, phi_p = _run("fp64", g)
+    ex, ey, live, vc, phi_p, parts_p = _run("fp64", g)
     dev = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
     nvc = int(np.sum(vc != g["vcycles"]))
     print("plain: max rel emittance deviation %.2e over %d periods; V-cycles %d (oracle %d), %d solves differ" % (
@@ -85,13 +91,19 @@ def test_fodo_1000_steps_plain_and_mixed_against_oracle():
     assert np.array_equal(live, g["live"])
     assert dev <= 1e-9
     assert nvc <= 2
-    ex, ey, live, vc, phi_m = _run("mixed", g)
+    ex, ey, live, vc, phi_m, parts_m = _run("mixed", g)
     dev = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
     dphi = np.max(np.abs(phi_m - phi_p)) / np.max(np.abs(phi_p))
     dE = max(np.max(np.abs(a - b)) / np.max(np.abs(b)) for a, b in zip(_efield(phi_m), _efield(phi_p)))
+    both = (parts_p["gaminv"] != 0) & (parts_m["gaminv"] != 0)
+    dps = {k: np.sqrt(np.mean((parts_m[k][both] - parts_p[k][both]) ** 2)) / np.std(parts_p[k][both])
+           for k in ("x", "y", "ux", "uy")}
     print("mixed after 1000 steps: phi within %.2e and E within %.2e of max|.| of the FP64 run" % (dphi, dE))
+    print("mixed after 1000 steps: rms phase-space difference / rms value: %s" %
+          " ".join("%s %.2e" % kv for kv in dps.items()))
     print("mixed: max rel emittance deviation %.2e; after 1000 steps x %.2e y %.2e; V-cycles %d; live %d vs %d" % (
         dev, abs(ex[-1] / g["epsx"][-1] - 1), abs(ey[-1] / g["epsy"][-1] - 1), vc.sum(), live[-1], g["live"][-1]))
     assert np.max(np.abs(live - g["live"])) <= 2
     assert dev <= 1e-4
-    assert dphi <= 1e-9 and dE <= 1e-9
+    assert dphi <= 1e-4 and dE <= 1e-4
+    assert max(dps.values()) <= 1e-4

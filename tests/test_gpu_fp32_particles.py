@@ -1,0 +1,122 @@
+"""FP32 particle storage, the particle arrays of the mixed-precision form
+(wg_particles_f32 and the _f32 entry points), against the FP64 path and the
+oracle.
+
+- Deposit: the FP32 positions are widened to FP64 before the fixed-point
+  weights are formed, so rho equals the FP64 deposit of the rounded
+  positions bit for bit, and the oracle's FP64 running sum within 1e-13.
+- Advance: E is gathered in FP64 at the FP32 positions, the kicks, rotation
+  and drift run in FP32. After a halfv, two fullv and a synchv step with
+  quads and the pipe, positions and velocities agree with the oracle's FP64
+  push of the same starting values within 1e-6 of each component's largest
+  magnitude.
+- Sort keys, the permutation and the moments see the same numbers as the
+  FP64 path on the widened arrays."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle
+from tests import gpu_helpers as H
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("x", "y", "z", "ux", "uy", "uz", "gaminv")
+
+
+def _setup(npart=200_000, seed=3):
+    from warp_b200 import pic
+    from warp_b200.particles import semigaussian
+    cfg = pic.workload("A")
+    p = semigaussian(npart, seed=seed, radius=4e-3, mismatch=0.2, angle_rms=5e-3)
+    s = H.make_solver(cfg["nx"], cfg["ny"], cfg["nz"], (cfg["xmmin"], cfg["ymmin"], cfg["zmmin"]),
+                      (cfg["xmmax"], cfg["ymmax"], cfg["zmmax"]), (0, 0, 0, 0, 2, 2))
+    return cfg, s, p
+
+
+def _rounded(p):
+    """The FP32 values of p, as FP64 arrays."""
+    return {k: v.astype(np.float32).astype(np.float64) for k, v in p.items()}
+
+
+def _groups(p, w=1e4):
+    from warp_b200.particles import ParticleGroup
+    return (ParticleGroup(p, w=w, dtype=torch.float32), ParticleGroup(_rounded(p), w=w))
+
+
+def test_deposit_f32_is_the_fp64_deposit_of_the_rounded_positions():
+    cfg, s, p = _setup()
+    p["gaminv"][::97] = 0.0
+    g32, g64 = _groups(p)
+    assert g32.x.dtype == torch.float32 and g32.x.element_size() == 4
+    s.loadrho(pgroups=[g32])
+    a = s.rho.cpu().numpy()
+    s.loadrho(pgroups=[g64])
+    b = s.rho.cpu().numpy()
+    assert np.array_equal(a, b)
+    pr = _rounded(p)
+    ref = np.zeros((s.nx + 1, s.ny + 1, s.nz + 1), order="F")
+    oracle.setrho(ref, pr["x"], pr["y"], pr["z"], g32.q, g32.w, s.dx, s.dy, s.dz, s.xmmin, s.ymmin, s.zmmin,
+                  gaminv=pr["gaminv"])
+    oracle.rhobc(ref, s.bounds)
+    assert np.max(np.abs(a - ref)) <= 1e-13 * np.max(np.abs(ref))
+    # chunked form
+    s.deposit_begin()
+    s.deposit_add(g32, 0, 70_000)
+    s.deposit_add(g32, 70_000, None)
+    s.deposit_end(zero_first=True)
+    assert np.array_equal(s.rho.cpu().numpy(), a)
+
+
+def test_advance_f32_against_the_fp64_oracle():
+    from warp_b200 import pic
+    from warp_b200.lattice import fodo
+    from warp_b200.particles import ParticleGroup
+    cfg, s, p = _setup(100_000)
+    rng = np.random.default_rng(11)
+    phi = np.asfortranarray(1e3 * rng.standard_normal((s.nx + 3, s.ny + 3, s.nz + 3)))
+    s.phi = phi
+    s.setlattice(fodo(cfg["quad_gradient"], cfg["quad_length"], cfg["period"]))
+    czs, cze, cdb, nzl, zlmin, dzl = s._lattice
+    dt = pic.timestep(cfg)
+    p["x"][:1000] *= 8.6  # some cross the pipe
+    ref = _rounded(p)
+    pg = ParticleGroup(p, w=1.0, dtype=torch.float32)
+    for center in ("halfv", "fullv", "fullv", "synchv"):
+        ex, ey, ez = oracle.sete(phi, ref["x"], ref["y"], ref["z"], s.dx, s.dy, s.dz, s.xmmin, s.ymmin, s.zmmin)
+        oracle.push(ref, ex, ey, ez, pg.q, pg.m, dt, (czs, cze, cdb), zlmin, dzl, s.zmmin, s.zmmax,
+                    cfg["pipe_radius"], center=center)
+        s.advance(pg, dt, prwall=cfg["pipe_radius"], center=center)
+    got = {k: v.astype(np.float64) for k, v in pg.to_numpy().items()}
+    lost_ref, lost = ref["gaminv"] == 0, got["gaminv"] == 0
+    assert lost_ref.sum() > 0
+    assert np.sum(lost_ref != lost) <= 2
+    both = ~lost_ref & ~lost
+    errs = {}
+    for k in ("x", "y", "z", "ux", "uy", "uz"):
+        errs[k] = np.max(np.abs(got[k][both] - ref[k][both])) / np.max(np.abs(ref[k][both]))
+    print("FP32 push vs FP64 oracle after 4 steps (max abs error / max abs value):",
+          " ".join("%s %.2e" % kv for kv in errs.items()))
+    for k, e in errs.items():
+        assert e <= 1e-6, (k, e)
+
+
+def test_sort_and_moments_f32_see_the_fp64_numbers():
+    cfg, s, p = _setup(150_000)
+    p["gaminv"][::31] = 0.0
+    g32, g64 = _groups(p, w=1.0)
+    m32, m64 = s.moments(g32), s.moments(g64)
+    assert m32 == m64
+    g32.sort(s)
+    g64.sort(s)
+    assert g32.np == g64.np == int((p["gaminv"] != 0).sum())
+    a, b = g32.to_numpy(), g64.to_numpy()
+    for k in KEYS:
+        assert a[k].dtype == np.float32
+        assert np.array_equal(a[k].astype(np.float64), b[k]), k
+    uold = (g32.ux.clone(), g32.uy.clone(), g32.uz.clone())
+    z32 = s.zmoments(g32, uold, 1e-9, 0.0, 1.0, 64)
+    uold64 = (g64.ux.clone(), g64.uy.clone(), g64.uz.clone())
+    z64 = s.zmoments(g64, uold64, 1e-9, 0.0, 1.0, 64)
+    for u, v in zip(z32, z64):
+        assert np.allclose(u, v, rtol=1e-12, atol=1e-12 * np.max(np.abs(v)))

@@ -50,6 +50,10 @@ class Particles(ctypes.Structure):
                 ("np", ctypes.c_int64), ("q", ctypes.c_double), ("m", ctypes.c_double), ("w", ctypes.c_double)]
 
 
+class ParticlesF32(ctypes.Structure):
+    _fields_ = Particles._fields_
+
+
 class PushParams(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("prwall", ctypes.c_double), ("prwallx", ctypes.c_double),
                 ("prwally", ctypes.c_double), ("use_lattice", ctypes.c_int), ("center", ctypes.c_int)]
@@ -99,6 +103,14 @@ SIGNATURES = {
     "wg_launch_count": [_vp, _i64p],
     "wg_particle_keys": [_vp, ctypes.POINTER(Particles), _vp],
     "wg_particle_permute": [_vp, _vp, ctypes.POINTER(Particles), ctypes.POINTER(Particles)],
+    "wg_deposit_f32": [_vp, ctypes.POINTER(ParticlesF32), _c.c_int],
+    "wg_deposit_add_f32": [_vp, ctypes.POINTER(ParticlesF32)],
+    "wg_advance_f32": [_vp, ctypes.POINTER(ParticlesF32), ctypes.POINTER(PushParams)],
+    "wg_moments_f32": [_vp, ctypes.POINTER(ParticlesF32), _dp],
+    "wg_zmoments_f32": [_vp, ctypes.POINTER(ParticlesF32), _vp, _vp, _vp] + [_c.c_double] * 5 +
+                       [_c.c_int, _c.c_double, _dp, _dp],
+    "wg_particle_keys_f32": [_vp, ctypes.POINTER(ParticlesF32), _vp],
+    "wg_particle_permute_f32": [_vp, _vp, ctypes.POINTER(ParticlesF32), ctypes.POINTER(ParticlesF32)],
     "wg_conv3_fwd": [_vp] + [_c.c_int] * 4 + [_vp, _vp, _c.c_int, _vp, _c.c_int, _c.c_int, _vp, _c.c_int, _c.c_int,
                      _vp, _vp],
     "wg_conv3_wgrad": [_vp, _vp] + [_c.c_int] * 5 + [_vp, _vp, _vp],

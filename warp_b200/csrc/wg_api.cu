@@ -35,6 +35,15 @@ int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* 
              double* zmmnts0, double* zmmnts);
 int moments_scratch_doubles(int nb);
 int configure_kernels();
+int deposit_f32(wg_ctx* c, const wg_particles_f32* p, int zero_first);
+int deposit_add_f32(wg_ctx* c, const wg_particles_f32* p);
+int advance_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm);
+int moments_f32(wg_ctx* c, const wg_particles_f32* p, double* out);
+int zmoments_f32(wg_ctx* c, const wg_particles_f32* p, const float* uxo, const float* uyo, const float* uzo,
+                 double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt,
+                 double zmmntdtextmax, double* zmmnts0, double* zmmnts);
+int cell_keys_f32(wg_ctx* c, const wg_particles_f32* p, int64_t* keys);
+int permute_f32(wg_ctx* c, const int64_t* perm, const wg_particles_f32* src, const wg_particles_f32* dst);
 
 // getnextcoarselevel3d / getmglevels (f3d_mgrid.F:3601-3845), serial,
 // mgcoarsening = 2.
@@ -583,6 +592,35 @@ int wg_moments(wg_ctx* c, const wg_particles* p, double* out) {
   return moments(c, p, out);
 }
 
+int wg_deposit_f32(wg_ctx* c, const wg_particles_f32* p, int zero_first) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  if (c->dep_open) { set_error("wg_deposit_f32: a chunked deposit is open (wg_deposit_end first)"); return WG_ESTATE; }
+  return deposit_f32(c, p, zero_first);
+}
+
+int wg_deposit_add_f32(wg_ctx* c, const wg_particles_f32* p) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return deposit_add_f32(c, p);
+}
+
+int wg_advance_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return advance_f32(c, p, prm);
+}
+
+int wg_moments_f32(wg_ctx* c, const wg_particles_f32* p, double* out) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return moments_f32(c, p, out);
+}
+
+int wg_zmoments_f32(wg_ctx* c, const wg_particles_f32* p, const float* uxo, const float* uyo, const float* uzo,
+                    double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt,
+                    double zmmntdtextmax, double* zmmnts0, double* zmmnts) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return zmoments_f32(c, p, uxo, uyo, uzo, dt, dtscale, zbeam, zmmntmin, zmmntmax, nzmmnt, zmmntdtextmax, zmmnts0,
+                      zmmnts);
+}
+
 }  // extern "C"
 
 extern "C" {
@@ -644,6 +682,17 @@ int wg_particle_keys(wg_ctx* c, const wg_particles* p, int64_t* keys) {
 int wg_particle_permute(wg_ctx* c, const int64_t* perm, const wg_particles* src, const wg_particles* dst) {
   if (!c) { set_error("null context"); return WG_EINVAL; }
   return permute(c, perm, src, dst);
+}
+
+int wg_particle_keys_f32(wg_ctx* c, const wg_particles_f32* p, int64_t* keys) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return cell_keys_f32(c, p, keys);
+}
+
+int wg_particle_permute_f32(wg_ctx* c, const int64_t* perm, const wg_particles_f32* src,
+                            const wg_particles_f32* dst) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return permute_f32(c, perm, src, dst);
 }
 
 }  // extern "C"

@@ -69,13 +69,15 @@ __device__ inline void box_add(DepBox& b, int n, unsigned long long v) {
   if (h) atomicAdd(&b.hi[n], h);
 }
 
-__device__ inline bool dep_cell(const double* xp, const double* yp, const double* zp, const double* gaminv,
-                                int64_t i, int64_t np, const GridP& g, int& ii, int& jj, int& kk, double& u1,
-                                double& v1, double& w1) {
-  if (i >= np || gaminv[i] == 0.) return false;
-  cellfrac((xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, u1);
-  cellfrac((yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, v1);
-  cellfrac((zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, w1);
+// Cell and fractions of particle i; FP32 positions are converted to FP64
+// first (exactly), so both storages share the FP64 arithmetic below.
+template <typename T>
+__device__ inline bool dep_cell(const T* xp, const T* yp, const T* zp, const T* gaminv, int64_t i, int64_t np,
+                                const GridP& g, int& ii, int& jj, int& kk, double& u1, double& v1, double& w1) {
+  if (i >= np || gaminv[i] == (T)0) return false;
+  cellfrac(((double)xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, u1);
+  cellfrac(((double)yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, v1);
+  cellfrac(((double)zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, w1);
   return true;
 }
 
@@ -89,10 +91,10 @@ __device__ inline void dep_add(DepBox& box, bool use_box, int ox, int oy, int oz
 }
 
 // Four blocks per SM (64 registers): 1.37 -> 1.21 ms for 5e7 particles.
-__global__ void __launch_bounds__(DEP_NT, 4) k_deposit(const double* __restrict__ xp, const double* __restrict__ yp,
-                                                    const double* __restrict__ zp,
-                                                    const double* __restrict__ gaminv, int64_t np, GridP g,
-                                                    unsigned long long* __restrict__ acc) {
+template <typename T>
+__global__ void __launch_bounds__(DEP_NT, 4) k_deposit(const T* __restrict__ xp, const T* __restrict__ yp,
+                                                    const T* __restrict__ zp, const T* __restrict__ gaminv,
+                                                    int64_t np, GridP g, unsigned long long* __restrict__ acc) {
   __shared__ DepBox box;
   __shared__ int bmin[3], bmax[3];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -531,65 +533,76 @@ struct PushP {
 // at 0 for a particle outside the grid. Four blocks per SM (64 registers and
 // a few spills to L1): the kernel waits on memory, and the extra warps took
 // it from 1.97 to 1.83 ms for 5e7 particles on the B200.
-template <int CENTER, bool COND>
+// T is the particle storage and push arithmetic: double is the reference's
+// arithmetic (bit-identical to the oracle); float is the push of the mixed
+// form, whose E is gathered in FP64 at the FP32 positions and then rounded.
+// The push constants (q dt / 2m, the lattice tables, the pipe radius) are
+// formed in FP64 and rounded once.
+template <typename T, int CENTER, bool COND>
 __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ phi, GridP g, PushP P, CondE ce,
-                                                 double* __restrict__ xp, double* __restrict__ yp,
-                                                 double* __restrict__ zp, double* __restrict__ uxp,
-                                                 double* __restrict__ uyp, double* __restrict__ uzp,
-                                                 double* __restrict__ gaminv, int64_t np) {
+                                                 T* __restrict__ xp, T* __restrict__ yp, T* __restrict__ zp,
+                                                 T* __restrict__ uxp, T* __restrict__ uyp, T* __restrict__ uzp,
+                                                 T* __restrict__ gaminv, int64_t np) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np) return;
-  double gi = gaminv[i];
-  if (gi == 0.) return;
-  double x = xp[i], y = yp[i], z = zp[i], ux = uxp[i], uy = uyp[i], uz = uzp[i];
-  double ex, ey, ez;
-  if (COND) {
-    if (!gather_e_cond(phi, g, ce, x, y, z, ex, ey, ez)) ex = ey = ez = 0.;
-  } else {
-    gather_e(phi, g, x, y, z, ex, ey, ez);
+  T gi = gaminv[i];
+  if (gi == (T)0) return;
+  T x = xp[i], y = yp[i], z = zp[i], ux = uxp[i], uy = uyp[i], uz = uzp[i];
+  T ex, ey, ez;
+  {
+    double exd, eyd, ezd;
+    if (COND) {
+      if (!gather_e_cond(phi, g, ce, (double)x, (double)y, (double)z, exd, eyd, ezd)) exd = eyd = ezd = 0.;
+    } else {
+      gather_e(phi, g, (double)x, (double)y, (double)z, exd, eyd, ezd);
+    }
+    ex = (T)exd;
+    ey = (T)eyd;
+    ez = (T)ezd;
   }
   // fetche3d zeroes E before the gather (w3d.F:11015): E = 0 + gathered
-  ex = 0. + ex;
-  ey = 0. + ey;
-  ez = 0. + ez;
-  double bx = 0., by = 0., bz = 0.;
-  const double halfdt = 0.5 * P.dt, dtl = CENTER == 1 ? 0. : -halfdt, dtr = CENTER == 2 ? 0. : halfdt;
+  ex = (T)0 + ex;
+  ey = (T)0 + ey;
+  ez = (T)0 + ez;
+  T bx = 0, by = 0, bz = 0;
+  const T dt = (T)P.dt;
+  const T halfdt = (T)(0.5 * P.dt), dtl = CENTER == 1 ? (T)0 : -halfdt, dtr = CENTER == 2 ? (T)0 : halfdt;
   if (P.czs) {
     // applyquad (top_lattice.F:2985-3120), one overlap level
-    const double vz = uz * gi;
-    const double a = vz * (dtr - dtl);
-    const double dzi = fabs(1. / copysign(fabs(a) + 1.0e-36, a));
-    int iz = (int)fmax(0., (z - P.zlmin) * (1. / P.dzl) + 0.5);
+    const T vz = uz * gi;
+    const T a = vz * (dtr - dtl);
+    const T dzi = fabs((T)1 / copysign(fabs(a) + (T)1.0e-36, a));
+    int iz = (int)fmax((T)0, (z - (T)P.zlmin) * (T)(1. / P.dzl) + (T)0.5);
     if (iz > P.nzl) iz = P.nzl;
-    const double zs = __ldg(P.czs + iz), ze = __ldg(P.cze + iz);
-    const double z1 = z + vz * dtl, z2 = z + vz * dtr;
-    const double zl = fmin(z1, z2);
-    const double fl = (zl >= zs && zl < ze) ? 1. : 0.;
-    const double zr = fmax(z1, z2);
-    const double fr = (zr >= zs && zr < ze) ? 1. : 0.;
-    double frac = fl;
+    const T zs = (T)__ldg(P.czs + iz), ze = (T)__ldg(P.cze + iz);
+    const T z1 = z + vz * dtl, z2 = z + vz * dtr;
+    const T zl = fmin(z1, z2);
+    const T fl = (zl >= zs && zl < ze) ? (T)1 : (T)0;
+    const T zr = fmax(z1, z2);
+    const T fr = (zr >= zs && zr < ze) ? (T)1 : (T)0;
+    T frac = fl;
     if (fl > fr) frac = (ze - zl) * dzi;
     if (fr > fl) frac = (zr - zs) * dzi;
-    if (frac > 0.) {
-      const double db = __ldg(P.cdb + iz);
+    if (frac > (T)0) {
+      const T db = (T)__ldg(P.cdb + iz);
       bx = bx + db * frac * y;
       by = by + db * frac * x;
     }
   }
   // epush3d (half step), bpush3d (ibpush = 1), epush3d (half step)
-  const double cst = P.q * halfdt / P.m;
+  const T cst = (T)(P.q * (0.5 * P.dt) / P.m);
   if (CENTER != 1) {
     ux = ux + ex * cst;
     uy = uy + ey * cst;
     uz = uz + ez * cst;
   }
-  const double cb = P.q * (CENTER == 0 ? P.dt : halfdt) * 0.5 / P.m;
-  const double tx = gi * bx * cb, ty = gi * by * cb, tz = gi * bz * cb;
-  const double tsqi = 2. / (1. + tx * tx + ty * ty + tz * tz);
-  const double sx = tx * tsqi, sy = ty * tsqi, sz = tz * tsqi;
-  const double uxppr = ux + uy * tz - uz * ty;
-  const double uyppr = uy + uz * tx - ux * tz;
-  const double uzppr = uz + ux * ty - uy * tx;
+  const T cb = (T)(P.q * (CENTER == 0 ? P.dt : 0.5 * P.dt) * 0.5 / P.m);
+  const T tx = gi * bx * cb, ty = gi * by * cb, tz = gi * bz * cb;
+  const T tsqi = (T)2 / ((T)1 + tx * tx + ty * ty + tz * tz);
+  const T sx = tx * tsqi, sy = ty * tsqi, sz = tz * tsqi;
+  const T uxppr = ux + uy * tz - uz * ty;
+  const T uyppr = uy + uz * tx - ux * tz;
+  const T uzppr = uz + ux * ty - uy * tx;
   ux = ux + uyppr * sz - uzppr * sy;
   uy = uy + uzppr * sx - uxppr * sz;
   uz = uz + uxppr * sy - uyppr * sx;
@@ -603,16 +616,18 @@ __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ p
   uy = uy + ey * cst;
   uz = uz + ez * cst;
   // xpush3d
-  x = x + ux * gi * P.dt;
-  y = y + uy * gi * P.dt;
-  z = z + uz * gi * P.dt;
+  x = x + ux * gi * dt;
+  y = y + uy * gi * dt;
+  z = z + uz * gi * dt;
   // periz (top.F:4015-4035)
-  const double syslen = P.zmmax - P.zmmin, sysleni = 1. / syslen;
-  if (z < P.zmmin) z = z + syslen * (int)((P.zmmax - z) * sysleni);
-  if (z > P.zmmax) z = z - syslen * (int)((z - P.zmmin) * sysleni);
+  const T zmmin = (T)P.zmmin, zmmax = (T)P.zmmax;
+  const T syslen = (T)(P.zmmax - P.zmmin), sysleni = (T)(1. / (P.zmmax - P.zmmin));
+  if (z < zmmin) z = z + syslen * (T)(int)((zmmax - z) * sysleni);
+  if (z > zmmax) z = z - syslen * (T)(int)((z - zmmin) * sysleni);
   // stckxy3d round aperture
-  const double rx = x - P.prwallx, ry = y - P.prwally;
-  if (rx * rx + ry * ry >= P.prwall * P.prwall) gaminv[i] = 0.;
+  const T rx = x - (T)P.prwallx, ry = y - (T)P.prwally;
+  const T prw = (T)P.prwall;
+  if (rx * rx + ry * ry >= prw * prw) gaminv[i] = (T)0;
   xp[i] = x;
   yp[i] = y;
   zp[i] = z;
@@ -624,25 +639,26 @@ __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ p
 // Cell key of particlesortxyzwithcopy (top.F:5095-5130):
 // ix + (nx+1)*(iy + (ny+1)*iz); lost particles get the key past the last
 // node so that a stable sort moves them behind the live ones.
-__global__ void k_cell_keys(const double* __restrict__ xp, const double* __restrict__ yp,
-                            const double* __restrict__ zp, const double* __restrict__ gaminv, int64_t np, GridP g,
-                            int64_t* __restrict__ key) {
+template <typename T>
+__global__ void k_cell_keys(const T* __restrict__ xp, const T* __restrict__ yp, const T* __restrict__ zp,
+                            const T* __restrict__ gaminv, int64_t np, GridP g, int64_t* __restrict__ key) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np) return;
-  if (gaminv[i] == 0.) {
+  if (gaminv[i] == (T)0) {
     key[i] = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
     return;
   }
   int ii, jj, kk;
   double f;
-  cellfrac((xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, f);
-  cellfrac((yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, f);
-  cellfrac((zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, f);
+  cellfrac(((double)xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, f);
+  cellfrac(((double)yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, f);
+  cellfrac(((double)zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, f);
   key[i] = (int64_t)ii + (int64_t)(g.nx + 1) * ((int64_t)jj + (int64_t)(g.ny + 1) * kk);
 }
 
 // dst[k][i] = src[k][perm[i]] for the 7 particle arrays.
-__global__ void k_permute(const int64_t* __restrict__ perm, int64_t np, wg_particles src, wg_particles dst) {
+template <typename PS>
+__global__ void k_permute(const int64_t* __restrict__ perm, int64_t np, PS src, PS dst) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np) return;
   const int64_t j = perm[i];
@@ -726,11 +742,12 @@ __device__ __forceinline__ void zm_add(double* dst, const double* m, bool warp_u
 // shared memory when the grid fits there, then added to the outputs. The
 // floating-point addition order is not fixed, so the sums agree with the
 // serial ones to rounding, not bit for bit.
-__global__ void __launch_bounds__(256) k_zmoments(const double* __restrict__ xp, const double* __restrict__ yp,
-                                                  const double* __restrict__ zp, const double* __restrict__ uxp,
-                                                  const double* __restrict__ uyp, const double* __restrict__ uzp,
-                                                  const double* __restrict__ gaminv, const double* __restrict__ uxo,
-                                                  const double* __restrict__ uyo, const double* __restrict__ uzo,
+template <typename T>
+__global__ void __launch_bounds__(256) k_zmoments(const T* __restrict__ xp, const T* __restrict__ yp,
+                                                  const T* __restrict__ zp, const T* __restrict__ uxp,
+                                                  const T* __restrict__ uyp, const T* __restrict__ uzp,
+                                                  const T* __restrict__ gaminv, const T* __restrict__ uxo,
+                                                  const T* __restrict__ uyo, const T* __restrict__ uzo,
                                                   int64_t np, ZMomP P, double* __restrict__ g_out,
                                                   double* __restrict__ zm_out) {
   extern __shared__ double sh[];
@@ -745,7 +762,7 @@ __global__ void __launch_bounds__(256) k_zmoments(const double* __restrict__ xp,
   const int64_t nround = (np + stride - 1) / stride;
   for (int64_t r = 0; r < nround; ++r) {
     const int64_t i = r * stride + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < np && gaminv[i] != 0.;
+    const bool live = i < np && gaminv[i] != (T)0;
     double x = 0., y = 0., z = 0., ux = 0., uy = 0., uz = 1., gi = 0.;
     if (live) {
       x = xp[i];
@@ -773,7 +790,7 @@ __global__ void __launch_bounds__(256) k_zmoments(const double* __restrict__ xp,
     const bool uniform = __all_sync(0xffffffffu, in && iz == iz0);
     if (!uniform && !in) continue;
     const double vzgi = 1. / (uz * gi + 1.0e-36);
-    const double ux_o = in ? uxo[i] : 0., uy_o = in ? uyo[i] : 0., uz_o = in ? uzo[i] : 0.;
+    const double ux_o = in ? (double)uxo[i] : 0., uy_o = in ? (double)uyo[i] : 0., uz_o = in ? (double)uzo[i] : 0.;
 #pragma unroll 1
     for (int side = 0; side < 2; ++side) {
       double dtx = ((iz + side) * P.dzm - z + P.zbeam + P.zmmntmin) * vzgi;
@@ -798,18 +815,18 @@ constexpr int kMomN = 11;
 
 // Per-block partial sums of the moments of live particles (getzmmnt,
 // top.F:690-721 with x' = ux/(uz+SMALLPOS)); fixed reduction tree per block.
-__global__ void k_moments(const double* __restrict__ xp, const double* __restrict__ yp,
-                          const double* __restrict__ uxp, const double* __restrict__ uyp,
-                          const double* __restrict__ uzp, const double* __restrict__ gaminv, int64_t np,
-                          double* __restrict__ part) {
+template <typename T>
+__global__ void k_moments(const T* __restrict__ xp, const T* __restrict__ yp, const T* __restrict__ uxp,
+                          const T* __restrict__ uyp, const T* __restrict__ uzp, const T* __restrict__ gaminv,
+                          int64_t np, double* __restrict__ part) {
   __shared__ double sm[kMomN][256];
   double s[kMomN];
 #pragma unroll
   for (int k = 0; k < kMomN; ++k) s[k] = 0.;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
-    if (gaminv[i] == 0.) continue;
-    const double vzi = 1. / (uzp[i] + 1.0e-36);
-    const double x = xp[i], y = yp[i], xpr = uxp[i] * vzi, ypr = uyp[i] * vzi;
+    if (gaminv[i] == (T)0) continue;
+    const double vzi = 1. / ((double)uzp[i] + 1.0e-36);
+    const double x = xp[i], y = yp[i], xpr = (double)uxp[i] * vzi, ypr = (double)uyp[i] * vzi;
     s[0] += 1.;
     s[1] += x;
     s[2] += y;
@@ -862,9 +879,23 @@ GridP gridp(const wg_ctx* c) {
                c->grid.zmmin, 0.};
 }
 
+// Element type of a particle struct.
+template <typename PS>
+struct PElem;
+template <>
+struct PElem<wg_particles> {
+  using T = double;
+};
+template <>
+struct PElem<wg_particles_f32> {
+  using T = float;
+};
+
 }  // namespace
 
-int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
+template <typename PS>
+int deposit_t(wg_ctx* c, const PS* p, int zero_first) {
+  using T = typename PElem<PS>::T;
   if (!p || (p->np > 0 && (!p->x || !p->y || !p->z || !p->gaminv)) || p->np < 0) {
     set_error("wg_deposit: null particle arrays");
     return WG_EINVAL;
@@ -877,7 +908,7 @@ int deposit(wg_ctx* c, const wg_particles* p, int zero_first) {
   if (p->np > 0) {
     const int64_t maxblocks = 2147483647LL;
     if (cdiv64(p->np, 256) > maxblocks) { set_error("wg_deposit: too many particles"); return WG_ETOOLARGE; }
-    { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, c->racc); c->prof_end(pe); }
+    { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<T><<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, c->racc); c->prof_end(pe); }
   }
   double gg = p->w * p->q;
   gg = gg / c->dx;
@@ -913,7 +944,9 @@ int deposit_begin(wg_ctx* c) {
   return WG_OK;
 }
 
-int deposit_add(wg_ctx* c, const wg_particles* p) {
+template <typename PS>
+int deposit_add_t(wg_ctx* c, const PS* p) {
+  using T = typename PElem<PS>::T;
   if (!p || (p->np > 0 && (!p->x || !p->y || !p->z || !p->gaminv)) || p->np < 0) {
     set_error("wg_deposit_add: null particle arrays");
     return WG_EINVAL;
@@ -934,7 +967,7 @@ int deposit_add(wg_ctx* c, const wg_particles* p) {
   c->dep_gg_set = true;
   if (p->np == 0) return WG_OK;
   if (cdiv64(p->np, 256) > 2147483647LL) { set_error("wg_deposit_add: too many particles"); return WG_ETOOLARGE; }
-  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, c->stream>>>(p->x, p->y, p->z, p->gaminv, p->np, gridp(c), c->racc); c->prof_end(pe); }
+  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_DEPOSIT, (double)p->np); k_deposit<T><<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, c->stream>>>(p->x, p->y, p->z, p->gaminv, p->np, gridp(c), c->racc); c->prof_end(pe); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }
@@ -1031,7 +1064,9 @@ int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double
   return WG_OK;
 }
 
-int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
+template <typename PS>
+int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm) {
+  using T = typename PElem<PS>::T;
   if (!p || !prm || p->np < 0 ||
       (p->np > 0 && (!p->x || !p->y || !p->z || !p->ux || !p->uy || !p->uz || !p->gaminv))) {
     set_error("wg_advance: null arguments");
@@ -1051,21 +1086,22 @@ int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
   CondE ce{};
   if (c->correctede) WG_TRY(prepare_correctede(c, &ce));
   auto kern = c->correctede
-                  ? (prm->center == WG_CENTER_HALFV    ? k_advance<1, true>
-                     : prm->center == WG_CENTER_SYNCHV ? k_advance<2, true>
-                                                       : k_advance<0, true>)
-                  : (prm->center == WG_CENTER_HALFV    ? k_advance<1, false>
-                     : prm->center == WG_CENTER_SYNCHV ? k_advance<2, false>
-                                                       : k_advance<0, false>);
+                  ? (prm->center == WG_CENTER_HALFV    ? k_advance<T, 1, true>
+                     : prm->center == WG_CENTER_SYNCHV ? k_advance<T, 2, true>
+                                                       : k_advance<T, 0, true>)
+                  : (prm->center == WG_CENTER_HALFV    ? k_advance<T, 1, false>
+                     : prm->center == WG_CENTER_SYNCHV ? k_advance<T, 2, false>
+                                                       : k_advance<T, 0, false>);
   { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, ce, p->x, p->y, p->z, p->ux, p->uy,
                                                   p->uz, p->gaminv, p->np); c->prof_end(pe); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }
 
-int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* uyo, const double* uzo, double dt,
-             double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt, double zmmntdtextmax,
-             double* zmmnts0, double* zmmnts) {
+template <typename PS, typename T = typename PElem<PS>::T>
+int zmoments_t(wg_ctx* c, const PS* p, const T* uxo, const T* uyo, const T* uzo, double dt, double dtscale,
+               double zbeam, double zmmntmin, double zmmntmax, int nzmmnt, double zmmntdtextmax, double* zmmnts0,
+               double* zmmnts) {
   if (!p || p->np < 0 || !zmmnts0 || !zmmnts ||
       (p->np > 0 && (!p->x || !p->y || !p->z || !p->ux || !p->uy || !p->uz || !p->gaminv || !uxo || !uyo || !uzo))) {
     set_error("wg_zmoments: null arguments");
@@ -1099,9 +1135,9 @@ int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* 
   if (p->np > 0) {
     const bool in_smem = nzmmnt + 1 <= kZMSmemPlanes;
     const size_t smem = (size_t)(kZM + (in_smem ? (nzmmnt + 1) * kZM : 0)) * sizeof(double);
-    WG_TRY_CUDA(cudaFuncSetAttribute(k_zmoments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    WG_TRY_CUDA(cudaFuncSetAttribute(k_zmoments<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned blocks = in_smem ? 148u : 592u;
-    { ++c->nlaunch; k_zmoments<<<blocks, 256, smem, s>>>(p->x, p->y, p->z, p->ux, p->uy, p->uz, p->gaminv, uxo, uyo, uzo, p->np, P, c->zmom, c->zmom + kZM); }
+    { ++c->nlaunch; k_zmoments<T><<<blocks, 256, smem, s>>>(p->x, p->y, p->z, p->ux, p->uy, p->uz, p->gaminv, uxo, uyo, uzo, p->np, P, c->zmom, c->zmom + kZM); }
     WG_TRY_CUDA(cudaGetLastError());
   }
   WG_TRY_CUDA(cudaMemcpyAsync(zmmnts0, c->zmom, kZM * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1111,11 +1147,13 @@ int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* 
   return WG_OK;
 }
 
-int moments(wg_ctx* c, const wg_particles* p, double* out) {
+template <typename PS>
+int moments_t(wg_ctx* c, const PS* p, double* out) {
+  using T = typename PElem<PS>::T;
   if (!p || !out || p->np < 0) { set_error("wg_moments: null arguments"); return WG_EINVAL; }
   cudaStream_t s = c->stream;
   const int nb = c->mom_blocks;
-  { ++c->nlaunch; k_moments<<<nb, 256, 0, s>>>(p->x, p->y, p->ux, p->uy, p->uz, p->gaminv, p->np, c->dmom); }
+  { ++c->nlaunch; k_moments<T><<<nb, 256, 0, s>>>(p->x, p->y, p->ux, p->uy, p->uz, p->gaminv, p->np, c->dmom); }
   { ++c->nlaunch; k_moments_final<<<1, 32, 0, s>>>(c->dmom, nb, c->dmom + (size_t)nb * kMomN); }
   WG_TRY_CUDA(cudaGetLastError());
   WG_TRY_CUDA(cudaMemcpyAsync(out, c->dmom + (size_t)nb * kMomN, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1125,23 +1163,55 @@ int moments(wg_ctx* c, const wg_particles* p, double* out) {
 
 int moments_scratch_doubles(int nb) { return nb * kMomN + 8; }
 
-int cell_keys(wg_ctx* c, const wg_particles* p, int64_t* keys) {
+template <typename PS>
+int cell_keys_t(wg_ctx* c, const PS* p, int64_t* keys) {
+  using T = typename PElem<PS>::T;
   if (!p || !keys || p->np < 0) { set_error("wg_particle_keys: null arguments"); return WG_EINVAL; }
   if (p->np == 0) return WG_OK;
-  { ++c->nlaunch; k_cell_keys<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(p->x, p->y, p->z, p->gaminv, p->np, gridp(c), keys); }
+  { ++c->nlaunch; k_cell_keys<T><<<cdiv64(p->np, 256), 256, 0, c->stream>>>(p->x, p->y, p->z, p->gaminv, p->np, gridp(c), keys); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }
 
-int permute(wg_ctx* c, const int64_t* perm, const wg_particles* src, const wg_particles* dst) {
+template <typename PS>
+int permute_t(wg_ctx* c, const int64_t* perm, const PS* src, const PS* dst) {
   if (!perm || !src || !dst || src->np != dst->np || src->np < 0) {
     set_error("wg_particle_permute: bad arguments");
     return WG_EINVAL;
   }
   if (src->np == 0) return WG_OK;
-  { ++c->nlaunch; k_permute<<<cdiv64(src->np, 256), 256, 0, c->stream>>>(perm, src->np, *src, *dst); }
+  { ++c->nlaunch; k_permute<PS><<<cdiv64(src->np, 256), 256, 0, c->stream>>>(perm, src->np, *src, *dst); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
+}
+
+int deposit(wg_ctx* c, const wg_particles* p, int zero_first) { return deposit_t(c, p, zero_first); }
+int deposit_f32(wg_ctx* c, const wg_particles_f32* p, int zero_first) { return deposit_t(c, p, zero_first); }
+int deposit_add(wg_ctx* c, const wg_particles* p) { return deposit_add_t(c, p); }
+int deposit_add_f32(wg_ctx* c, const wg_particles_f32* p) { return deposit_add_t(c, p); }
+int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) { return advance_t(c, p, prm); }
+int advance_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm) { return advance_t(c, p, prm); }
+int moments(wg_ctx* c, const wg_particles* p, double* out) { return moments_t(c, p, out); }
+int moments_f32(wg_ctx* c, const wg_particles_f32* p, double* out) { return moments_t(c, p, out); }
+int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* uyo, const double* uzo, double dt,
+             double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt, double zmmntdtextmax,
+             double* zmmnts0, double* zmmnts) {
+  return zmoments_t(c, p, uxo, uyo, uzo, dt, dtscale, zbeam, zmmntmin, zmmntmax, nzmmnt, zmmntdtextmax, zmmnts0,
+                    zmmnts);
+}
+int zmoments_f32(wg_ctx* c, const wg_particles_f32* p, const float* uxo, const float* uyo, const float* uzo,
+                 double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt,
+                 double zmmntdtextmax, double* zmmnts0, double* zmmnts) {
+  return zmoments_t(c, p, uxo, uyo, uzo, dt, dtscale, zbeam, zmmntmin, zmmntmax, nzmmnt, zmmntdtextmax, zmmnts0,
+                    zmmnts);
+}
+int cell_keys(wg_ctx* c, const wg_particles* p, int64_t* keys) { return cell_keys_t(c, p, keys); }
+int cell_keys_f32(wg_ctx* c, const wg_particles_f32* p, int64_t* keys) { return cell_keys_t(c, p, keys); }
+int permute(wg_ctx* c, const int64_t* perm, const wg_particles* src, const wg_particles* dst) {
+  return permute_t(c, perm, src, dst);
+}
+int permute_f32(wg_ctx* c, const int64_t* perm, const wg_particles_f32* src, const wg_particles_f32* dst) {
+  return permute_t(c, perm, src, dst);
 }
 
 // ---- deposition into caller memory with no allocation ----------------------
@@ -1212,7 +1282,7 @@ int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int
   k_zero_u64<<<1, 32, 0, s>>>(flag, 1);
   const double dx = (G.xmmax - G.xmmin) / G.nx, dy = (G.ymmax - G.ymmin) / G.ny, dz = (G.zmmax - G.zmmin) / G.nz;
   GridP g{G.nx, G.ny, G.nz, dx, dy, dz, G.xmmin, G.ymmin, G.zmmin, 0.};
-  if (p->np > 0) k_deposit<<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, acc);
+  if (p->np > 0) k_deposit<double><<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, acc);
   double gg = p->w * p->q;
   gg = gg / dx;
   gg = gg / dy;

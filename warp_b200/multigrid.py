@@ -261,7 +261,7 @@ class MultiGridB200(FieldSolver):
             self._rho.zero_()
         for pg in groups:
             s = pg.cstruct()
-            _lib.check(_lib.lib.wg_deposit(self._h, ctypes.byref(s), int(first)))
+            _lib.check(pg.fn("wg_deposit")(self._h, ctypes.byref(s), int(first)))
             first = False
         if lfinalize_rho:
             _lib.check(_lib.lib.wg_finalize_rho(self._h))
@@ -276,7 +276,7 @@ class MultiGridB200(FieldSolver):
         """Accumulates particles start:stop of pgroup (wg_deposit_add)."""
         self._bind_stream()
         s = pgroup.cstruct(start, stop)
-        _lib.check(_lib.lib.wg_deposit_add(self._h, ctypes.byref(s)))
+        _lib.check(pgroup.fn("wg_deposit_add")(self._h, ctypes.byref(s)))
 
     def deposit_end(self, zero_first=True, lfinalize_rho=True):
         """Converts the accumulated pieces into rho (replacing it when
@@ -373,6 +373,8 @@ class MultiGridB200(FieldSolver):
         for v in ([views] if views is not None else
                   [[getattr(pg, k) for k in ("x", "y", "z", "ex", "ey", "ez")] for pg in groups]):
             n = int(v[0].shape[0])
+            # the gather reads FP64 positions (FP32 groups are widened)
+            v = [t.double().contiguous() for t in v[:3]] + v[3:]
             for e in v[3:]:
                 e.zero_()
             if n:
@@ -428,7 +430,7 @@ class MultiGridB200(FieldSolver):
         s = pgroup.cstruct(start, stop)
         p = _lib.PushParams(float(dt), float(prwall), float(prwallx), float(prwally),
                             int(self._lattice is not None), _lib.CENTERS[center])
-        _lib.check(_lib.lib.wg_advance(self._h, ctypes.byref(s), ctypes.byref(p)))
+        _lib.check(pgroup.fn("wg_advance")(self._h, ctypes.byref(s), ctypes.byref(p)))
 
     def zmoments(self, pgroup, uold, dt, zmmntmin, zmmntmax, nzmmnt, zbeam=0., dtscale=1., zmmntdtextmax=1e36):
         """The moment sums of getzmmnt (wg_zmoments): returns zmmnts0 (33,)
@@ -441,8 +443,9 @@ class MultiGridB200(FieldSolver):
         z0 = np.zeros(33)
         zm = np.zeros((int(nzmmnt) + 1, 33))
         dp = ctypes.POINTER(ctypes.c_double)
+        uold = [u.to(pgroup.dtype).contiguous() for u in uold]  # kept alive across the call
         uo = [ctypes.c_void_p(u.data_ptr()) for u in uold]
-        _lib.check(_lib.lib.wg_zmoments(self._h, ctypes.byref(s), uo[0], uo[1], uo[2], float(dt), float(dtscale),
+        _lib.check(pgroup.fn("wg_zmoments")(self._h, ctypes.byref(s), uo[0], uo[1], uo[2], float(dt), float(dtscale),
                                         float(zbeam), float(zmmntmin), float(zmmntmax), int(nzmmnt),
                                         float(zmmntdtextmax), z0.ctypes.data_as(dp), zm.ctypes.data_as(dp)))
         return z0, zm
@@ -453,7 +456,7 @@ class MultiGridB200(FieldSolver):
         self._bind_stream()
         s = pgroup.cstruct()
         out = (ctypes.c_double * 8)()
-        _lib.check(_lib.lib.wg_moments(self._h, ctypes.byref(s), out))
+        _lib.check(pgroup.fn("wg_moments")(self._h, ctypes.byref(s), out))
         keys = ("n", "xbar", "ybar", "xrms", "yrms", "epsx", "epsy")
         return {k: out[i] for i, k in enumerate(keys)}
 

@@ -1,10 +1,13 @@
 """Device-resident particle group (the role of top.pgroup) and the seeded
 semi-Gaussian beam loader used for the synthetic workloads.
 
-Arrays are float64 torch tensors on the CUDA device (SoA: x, y, z, ux, uy,
-uz, gaminv, ex, ey, ez). A lost particle has gaminv == 0, the stckxy3d
-convention (pywarp90/w3d.F:11520-11535); lost particles are skipped by the
-deposit, push and moments kernels.
+Arrays are torch tensors on the CUDA device (SoA: x, y, z, ux, uy, uz,
+gaminv, and ex, ey, ez for fetche). The particle arrays are float64, the
+reference's storage, or float32 for the mixed-precision form whose push runs
+in FP32 (dtype=torch.float32; the library's _f32 entry points); ex, ey, ez
+stay float64. A lost particle has gaminv == 0, the stckxy3d convention
+(pywarp90/w3d.F:11520-11535); lost particles are skipped by the deposit,
+push and moments kernels.
 """
 import math
 
@@ -19,8 +22,13 @@ FIELDS = ("x", "y", "z", "ux", "uy", "uz", "gaminv")
 
 
 class ParticleGroup:
-    def __init__(self, arrays, q=echarge, m=proton_mass, w=1.0, device="cuda", with_fields=True):
-        """arrays: dict of equal-length 1-D arrays (numpy or torch) for FIELDS."""
+    def __init__(self, arrays, q=echarge, m=proton_mass, w=1.0, device="cuda", with_fields=True,
+                 dtype=torch.float64):
+        """arrays: dict of equal-length 1-D arrays (numpy or torch) for
+        FIELDS, stored as `dtype` (torch.float64 or torch.float32)."""
+        if dtype not in (torch.float64, torch.float32):
+            raise ValueError("ParticleGroup: dtype must be torch.float64 or torch.float32")
+        self.dtype = dtype
         self.q, self.m, self.w = float(q), float(m), float(w)
         self.device = torch.device(device)
         if self.device.type == "cuda" and self.device.index is None:
@@ -28,7 +36,7 @@ class ParticleGroup:
         n = len(arrays["x"])
         for f in FIELDS:
             a = arrays[f]
-            t = torch.as_tensor(a, dtype=torch.float64).to(self.device).contiguous()
+            t = torch.as_tensor(a).to(device=self.device, dtype=dtype).contiguous()
             if t.shape != (n,):
                 raise ValueError("particle array %s has shape %s, expected (%d,)" % (f, tuple(t.shape), n))
             setattr(self, f, t)
@@ -42,12 +50,23 @@ class ParticleGroup:
     def np(self):
         return int(self.x.shape[0])
 
+    @property
+    def fp32(self):
+        return self.dtype == torch.float32
+
+    def fn(self, name):
+        """The library entry point `name` for this group's storage (the _f32
+        form for FP32 particles)."""
+        return getattr(_lib.lib, name + "_f32" if self.fp32 else name)
+
     def cstruct(self, start=0, stop=None):
-        """C view of particles start..stop-1 (all by default)."""
+        """C view of particles start..stop-1 (all by default): a
+        wg_particles, or a wg_particles_f32 for FP32 storage."""
         stop = self.np if stop is None else int(stop)
-        s = _lib.Particles()
+        s = _lib.ParticlesF32() if self.fp32 else _lib.Particles()
+        size = 4 if self.fp32 else 8
         for f in FIELDS:
-            setattr(s, f, getattr(self, f).data_ptr() + 8 * int(start))
+            setattr(s, f, getattr(self, f).data_ptr() + size * int(start))
         s.np = stop - int(start)
         s.q, s.m, s.w = self.q, self.m, self.w
         return s
@@ -65,21 +84,21 @@ class ParticleGroup:
             return
         keys = torch.empty(n, dtype=torch.int64, device=self.device)
         s = self.cstruct()
-        _lib.check(_lib.lib.wg_particle_keys(solver._h, ctypes.byref(s), ctypes.c_void_p(keys.data_ptr())))
+        _lib.check(self.fn("wg_particle_keys")(solver._h, ctypes.byref(s), ctypes.c_void_p(keys.data_ptr())))
         perm = torch.argsort(keys, stable=True)
         nlive = n
         if compact:
             sentinel = (solver.nx + 1) * (solver.ny + 1) * (solver.nz + 1)
             nlive = int(torch.searchsorted(keys[perm], torch.tensor([sentinel], device=self.device)).item())
-        new = {f: torch.empty(nlive, dtype=torch.float64, device=self.device) for f in FIELDS}
-        d = _lib.Particles()
+        new = {f: torch.empty(nlive, dtype=self.dtype, device=self.device) for f in FIELDS}
+        d = _lib.ParticlesF32() if self.fp32 else _lib.Particles()
         for f in FIELDS:
             setattr(d, f, new[f].data_ptr())
         d.np = nlive
         s.np = nlive
         d.q, d.m, d.w = self.q, self.m, self.w
-        _lib.check(_lib.lib.wg_particle_permute(solver._h, ctypes.c_void_p(perm.data_ptr()), ctypes.byref(s),
-                                                ctypes.byref(d)))
+        _lib.check(self.fn("wg_particle_permute")(solver._h, ctypes.c_void_p(perm.data_ptr()), ctypes.byref(s),
+                                                  ctypes.byref(d)))
         for f in FIELDS:
             setattr(self, f, new[f])
         if hasattr(self, "ex") and self.ex.shape[0] != nlive:

@@ -28,7 +28,14 @@ class ESPIC:
     """Sets up solver, conductors, lattice and beam of a workload."""
 
     def __init__(self, cfg, precision="fp64", tolkind="mgerror", mgtol=1.e-6, mgmaxiters=100, device="cuda",
-                 particles=None, sort_interval=0):
+                 particles=None, sort_interval=0, particle_dtype=None):
+        """precision "fp64" is the reference's arithmetic throughout;
+        "mixed" runs the V-cycles in FP32 inside FP64 defect correction and
+        keeps the particles in FP32 with an FP32 push (particle_dtype, by
+        default float32 for "mixed" and float64 for "fp64")."""
+        import torch
+        if particle_dtype is None:
+            particle_dtype = torch.float32 if precision == "mixed" else torch.float64
         self.cfg = cfg
         c = cfg
         self.solver = MultiGridB200(c["nx"], c["ny"], c["nz"], c["xmmin"], c["xmmax"], c["ymmin"], c["ymmax"],
@@ -52,7 +59,7 @@ class ESPIC:
                                      angle_rms=c["angle_rms"], zmin=c["zmmin"], zmax=c["zmmax"],
                                      ekin_ev=c["ekin_ev"])
         w = beam_weight(c["current"], c["zmmax"] - c["zmmin"], c["npart"], ekin_ev=c["ekin_ev"])
-        self.pgroup = ParticleGroup(particles, q=echarge, m=proton_mass, w=w, device=device)
+        self.pgroup = ParticleGroup(particles, q=echarge, m=proton_mass, w=w, device=device, dtype=particle_dtype)
         self.solver.addpgroup(self.pgroup)
         self.sort_interval = int(sort_interval)
         self.it = 0
@@ -89,8 +96,9 @@ class ESPIC:
         """nsteps steps of the drop-in mode in which the host owns the
         particles (WARP keeps top.pgroup in host memory, and step(n) runs n
         steps): `host` maps each of x, y, z, ux, uy, uz, gaminv to a pinned
-        CPU float64 tensor. Every step reads the arrays from the host and
-        writes the advanced particles back.
+        CPU tensor of the particle group's dtype (float32 in the mixed
+        form). Every step reads the arrays from the host and writes the
+        advanced particles back.
 
         The arrays cross PCIe in `nchunks` chunks. Uploads run on one copy
         stream; each chunk is advanced and deposited as soon as it has
@@ -211,7 +219,7 @@ class ESPIC:
         s, pg = self.solver, self.pgroup
         arrays = {"p_" + k: v for k, v in pg.to_numpy().items()}
         meta = {"cfg": self.cfg, "it": self.it, "vsync": self.vsync, "sort_interval": self.sort_interval,
-                "precision": s.precision,
+                "precision": s.precision, "particle_dtype": "float32" if pg.fp32 else "float64",
                 "tolkind": s.tolkind, "mgtol": s.mgtol, "mgmaxiters": s.mgmaxiters, "q": pg.q, "m": pg.m,
                 "w": pg.w}
         with open(filename, "wb") as f:
@@ -229,8 +237,10 @@ def restart(filename, device="cuda"):
         meta = json.loads(bytes(d["meta"]).decode())
         parts = {k[2:]: d[k] for k in d.files if k.startswith("p_")}
         phi = d["phi"]
+    import torch
     run = ESPIC(meta["cfg"], precision=meta["precision"], tolkind=meta["tolkind"], mgtol=meta["mgtol"],
-                mgmaxiters=meta["mgmaxiters"], device=device, particles=parts, sort_interval=meta["sort_interval"])
+                mgmaxiters=meta["mgmaxiters"], device=device, particles=parts, sort_interval=meta["sort_interval"],
+                particle_dtype=getattr(torch, meta.get("particle_dtype", "float64")))
     run.pgroup.q, run.pgroup.m, run.pgroup.w = meta["q"], meta["m"], meta["w"]
     run.solver.phi = np.asfortranarray(phi)
     run.it = meta["it"]
