@@ -1,18 +1,21 @@
-"""The long-run FODO fixture (tests/golden/fodo_long_run.npz) is what the
-oracle computes: its first two lattice periods are recomputed here bit for
-bit (the oracle's threaded loops sum in a fixed order), and the particles
-drawn by the CPU generator are the fixture's."""
+"""The long-run FODO fixtures (tests/golden/fodo_long_run.npz, 20000
+particles, and fodo_long_run_200k.npz, 200000) are what the oracle computes:
+their first two lattice periods are recomputed here bit for bit (the
+oracle's threaded loops sum in a fixed order), and the particles drawn by
+the CPU generator are the fixtures'."""
 import os
 
 import numpy as np
+import pytest
 
 from tests import fodo_setup as F
 
-FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fodo_long_run.npz")
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def test_fixture_first_two_periods_recomputed_by_the_oracle():
-    g = np.load(FIXTURE)
+@pytest.mark.parametrize("name", ["fodo_long_run.npz", "fodo_long_run_200k.npz"])
+def test_fixture_first_two_periods_recomputed_by_the_oracle(name):
+    g = np.load(os.path.join(GOLDEN, name))
     npart, seed, mgtol = int(g["npart"]), int(g["seed"]), float(g["mgtol"])
     assert np.array_equal(F.host_beam(npart, seed)["x"][:8], g["x0"])
     r = F.oracle_run(npart, 2 * F.STEPS_PER_PERIOD, seed, mgtol)

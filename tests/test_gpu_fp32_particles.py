@@ -7,9 +7,10 @@ oracle.
   positions bit for bit, and the oracle's FP64 running sum within 1e-13.
 - Advance: E is gathered in FP64 at the FP32 positions, the kicks, rotation
   and drift run in FP32. After a halfv, two fullv and a synchv step with
-  quads and the pipe, positions and velocities agree with the oracle's FP64
-  push of the same starting values within 1e-6 of each component's largest
-  magnitude.
+  quads and the pipe (in a random phi of 1 kV rms, which makes the kicks
+  large), positions agree with the oracle's FP64 push of the same starting
+  values within 1e-6 and velocities within 1e-5 of each component's
+  largest magnitude (measured on the B200: 1.6e-7 and 2.1e-6).
 - Sort keys, the permutation and the moments see the same numbers as the
   FP64 path on the widened arrays."""
 import numpy as np
@@ -98,7 +99,7 @@ def test_advance_f32_against_the_fp64_oracle():
     print("FP32 push vs FP64 oracle after 4 steps (max abs error / max abs value):",
           " ".join("%s %.2e" % kv for kv in errs.items()))
     for k, e in errs.items():
-        assert e <= 1e-6, (k, e)
+        assert e <= (1e-6 if k in ("x", "y", "z") else 1e-5), (k, e)
 
 
 def test_sort_and_moments_f32_see_the_fp64_numbers():
