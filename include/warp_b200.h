@@ -237,6 +237,15 @@ int wg_advance(wg_ctx* ctx, const wg_particles* p, const wg_push_params* prm);
 int wg_deposit_f32(wg_ctx* ctx, const wg_particles_f32* p, int zero_first);
 int wg_deposit_add_f32(wg_ctx* ctx, const wg_particles_f32* p);
 int wg_advance_f32(wg_ctx* ctx, const wg_particles_f32* p, const wg_push_params* prm);
+/* wg_advance followed by wg_deposit_add of the advanced particles, in one
+ * pass over them (padvnc3d then setrho3d, w3d.F:1575 and 7757-7960, as
+ * step3d orders them): the new positions are deposited from registers into
+ * the open chunked deposit (wg_deposit_begin .. wg_deposit_end) with the same
+ * fixed-point weights, so rho is bit-identical to the separate calls. No
+ * reference counterpart as a single routine. WG_ESTATE without an open
+ * deposit. */
+int wg_advance_deposit(wg_ctx* ctx, const wg_particles* p, const wg_push_params* prm);
+int wg_advance_deposit_f32(wg_ctx* ctx, const wg_particles_f32* p, const wg_push_params* prm);
 /* getzmmnt global moments (top.F:521-1444): out[0] live count, 1 xbar,
  * 2 ybar, 3 xrms, 4 yrms, 5 epsx, 6 epsy (x' = ux/uz), 7 reserved. FP64,
  * deterministic order. */

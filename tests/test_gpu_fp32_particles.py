@@ -121,3 +121,69 @@ def test_sort_and_moments_f32_see_the_fp64_numbers():
     z64 = s.zmoments(g64, uold64, 1e-9, 0.0, 1.0, 64)
     for u, v in zip(z32, z64):
         assert np.allclose(u, v, rtol=1e-12, atol=1e-12 * np.max(np.abs(v)))
+
+
+def test_f32_wrap_keeps_particles_inside_z():
+    """(float)zmmax can round past zmmax: the FP32 wrap must still leave every
+    particle inside [zmmin, zmmax] (in FP64 terms), where the deposit's CIC
+    fractions stay in [0, 1] and no weight goes negative."""
+    from warp_b200.particles import ParticleGroup
+    s = H.make_solver(32, 32, 64, (-0.02, -0.02, -0.36), (0.02, 0.02, 0.36), (0, 0, 0, 0, 2, 2))
+    assert float(np.float32(0.36)) > 0.36  # the rounding that the wrap has to undo
+    n = 4096
+    rng = np.random.default_rng(4)
+    dt = 1e-9
+    z = np.concatenate([0.36 - rng.uniform(0, 2e-8, n // 2), -0.36 + rng.uniform(0, 2e-8, n // 2)])
+    uz = np.concatenate([rng.uniform(0, 4e1, n // 2), -rng.uniform(0, 4e1, n // 2)])
+    p = {"x": rng.uniform(-1e-3, 1e-3, n), "y": rng.uniform(-1e-3, 1e-3, n), "z": z, "ux": np.zeros(n),
+         "uy": np.zeros(n), "uz": uz, "gaminv": np.ones(n)}
+    pg = ParticleGroup(p, w=1.0, dtype=torch.float32)
+    for _ in range(20):
+        s.advance(pg, dt, center="fullv")
+        zz = pg.z.double().cpu().numpy()
+        assert zz.min() >= -0.36 and zz.max() <= 0.36
+    s.loadrho(pgroups=[pg])  # WG_EOVERFLOW on a negative weight
+    assert float(s.rho.sum()) * s.dx * s.dy * s.dz == pytest.approx(n * pg.q * pg.w, rel=1e-12)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_fused_advance_deposit_equals_advance_then_deposit(dtype):
+    """wg_advance_deposit: the same particles as wg_advance and the same rho,
+    bit for bit, as a deposit of the advanced particles, for sorted and
+    unsorted particles (shared box and direct accumulator paths)."""
+    from warp_b200 import pic
+    from warp_b200.lattice import fodo
+    from warp_b200.particles import ParticleGroup
+    cfg, s, p = _setup(300_000)
+    rng = np.random.default_rng(21)
+    s.phi = np.asfortranarray(10. * rng.standard_normal((s.nx + 3, s.ny + 3, s.nz + 3)))
+    s.setlattice(fodo(cfg["quad_gradient"], cfg["quad_length"], cfg["period"]))
+    dt = pic.timestep(cfg)
+    p["x"][:500] *= 8.6  # some are lost at the pipe
+    a, b = ParticleGroup(p, w=1e4, dtype=dtype), ParticleGroup(p, w=1e4, dtype=dtype)
+    b.sort(s)
+    a.sort(s)
+    for sort_first in (True, False):
+        if not sort_first:  # shuffled: boxes too large for shared memory
+            perm = torch.randperm(a.np, device=a.device)
+            for k in KEYS:
+                setattr(a, k, getattr(a, k)[perm].contiguous())
+                setattr(b, k, getattr(b, k)[perm].contiguous())
+        for center in ("halfv", "fullv", "fullv"):
+            s.advance(a, dt, prwall=cfg["pipe_radius"], center=center)
+            s.loadrho(pgroups=[a])
+            r1 = s.rho.cpu().numpy()
+            s.deposit_begin()
+            s.advance(b, dt, prwall=cfg["pipe_radius"], center=center, deposit=True)
+            s.deposit_end(zero_first=True)
+            r2 = s.rho.cpu().numpy()
+            assert np.array_equal(r1, r2), (sort_first, center)
+            for k in KEYS:
+                assert torch.equal(getattr(a, k), getattr(b, k)), (sort_first, center, k)
+    assert int((a.gaminv == 0).sum()) > 0
+    # without an open deposit the fused call is refused
+    import ctypes
+    from warp_b200 import _lib
+    prm = _lib.PushParams(dt, 1e30, 0., 0., 0, 0)
+    st = b.cstruct()
+    assert b.fn("wg_advance_deposit")(s._h, ctypes.byref(st), ctypes.byref(prm)) == -3

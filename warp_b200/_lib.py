@@ -107,6 +107,8 @@ SIGNATURES = {
     "wg_deposit_add_f32": [_vp, ctypes.POINTER(ParticlesF32)],
     "wg_advance_f32": [_vp, ctypes.POINTER(ParticlesF32), ctypes.POINTER(PushParams)],
     "wg_moments_f32": [_vp, ctypes.POINTER(ParticlesF32), _dp],
+    "wg_advance_deposit": [_vp, ctypes.POINTER(Particles), ctypes.POINTER(PushParams)],
+    "wg_advance_deposit_f32": [_vp, ctypes.POINTER(ParticlesF32), ctypes.POINTER(PushParams)],
     "wg_zmoments_f32": [_vp, ctypes.POINTER(ParticlesF32), _vp, _vp, _vp] + [_c.c_double] * 5 +
                        [_c.c_int, _c.c_double, _dp, _dp],
     "wg_particle_keys_f32": [_vp, ctypes.POINTER(ParticlesF32), _vp],

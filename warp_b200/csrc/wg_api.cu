@@ -38,6 +38,8 @@ int configure_kernels();
 int deposit_f32(wg_ctx* c, const wg_particles_f32* p, int zero_first);
 int deposit_add_f32(wg_ctx* c, const wg_particles_f32* p);
 int advance_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm);
+int advance_deposit(wg_ctx* c, const wg_particles* p, const wg_push_params* prm);
+int advance_deposit_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm);
 int moments_f32(wg_ctx* c, const wg_particles_f32* p, double* out);
 int zmoments_f32(wg_ctx* c, const wg_particles_f32* p, const float* uxo, const float* uyo, const float* uzo,
                  double dt, double dtscale, double zbeam, double zmmntmin, double zmmntmax, int nzmmnt,
@@ -606,6 +608,16 @@ int wg_deposit_add_f32(wg_ctx* c, const wg_particles_f32* p) {
 int wg_advance_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm) {
   if (!c) { set_error("null context"); return WG_EINVAL; }
   return advance_f32(c, p, prm);
+}
+
+int wg_advance_deposit(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return advance_deposit(c, p, prm);
+}
+
+int wg_advance_deposit_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm) {
+  if (!c) { set_error("null context"); return WG_EINVAL; }
+  return advance_deposit_f32(c, p, prm);
 }
 
 int wg_moments_f32(wg_ctx* c, const wg_particles_f32* p, double* out) {

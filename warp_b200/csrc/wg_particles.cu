@@ -59,10 +59,13 @@ constexpr int DEP_NT = 256, DEP_PPT = 16, DEP_BOX = 3072;
 // DEP_NT*DEP_PPT = 4096 contributions to a node, so the two 16-bit parts sum
 // below 2^28 and the high part below 2^26 (total below 2^58): no part
 // overflows, and the recombined 64-bit value is exact.
-struct DepBox {
-  unsigned lo[DEP_BOX], mid[DEP_BOX], hi[DEP_BOX];
+template <int NB>
+struct DepBoxN {
+  unsigned lo[NB], mid[NB], hi[NB];
 };
-__device__ inline void box_add(DepBox& b, int n, unsigned long long v) {
+using DepBox = DepBoxN<DEP_BOX>;
+template <int NB>
+__device__ inline void box_add(DepBoxN<NB>& b, int n, unsigned long long v) {
   const unsigned l = (unsigned)(v & 0xFFFFull), m = (unsigned)((v >> 16) & 0xFFFFull), h = (unsigned)(v >> 32);
   if (l) atomicAdd(&b.lo[n], l);
   if (m) atomicAdd(&b.mid[n], m);
@@ -82,7 +85,8 @@ __device__ inline bool dep_cell(const T* xp, const T* yp, const T* zp, const T* 
 }
 
 // Adds v to node (i, j, k) of the box or of the global accumulator.
-__device__ inline void dep_add(DepBox& box, bool use_box, int ox, int oy, int oz, int bx, int by,
+template <int NB>
+__device__ inline void dep_add(DepBoxN<NB>& box, bool use_box, int ox, int oy, int oz, int bx, int by,
                                unsigned long long* acc, const GridP& g, int i, int j, int k, unsigned long long v) {
   if (use_box)
     box_add(box, (i - ox) + bx * ((j - oy) + by * (k - oz)), v);
@@ -522,6 +526,93 @@ struct PushP {
   double zlmin, dzl;
 };
 
+// The deposit of one advanced particle per thread (the CTA's 256 particles)
+// into the fixed-point accumulator: the same cells, weights and integer
+// sums as k_deposit, so the accumulated charge is the same bit for bit. The
+// CTA's particles are consecutive, so when they are sorted by cell they
+// cover a small box of nodes: the weights go to a shared-memory copy of the
+// box (three 32-bit parts per node, as k_deposit) and the box is added to
+// the accumulator at the end; when the box is larger than ADV_BOX nodes
+// each lane adds to the accumulator directly. A warp whose 32 particles sit
+// in one cell sums them in registers first. All threads of the CTA call it.
+constexpr int ADV_BOX = 1024;
+__device__ inline void block_deposit(bool live, double x, double y, double z, const GridP& g,
+                                     unsigned long long* __restrict__ acc, DepBoxN<ADV_BOX>& box, int* bmin,
+                                     int* bmax) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  int ii = 0, jj = 0, kk = 0;
+  double u1 = 0., v1 = 0., w1 = 0.;
+  if (live) {
+    cellfrac((x - g.xmmin) * (1. / g.dx), g.nx, ii, u1);
+    cellfrac((y - g.ymmin) * (1. / g.dy), g.ny, jj, v1);
+    cellfrac((z - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, w1);
+  }
+  int lo[3] = {live ? ii : 0x7fffffff, live ? jj : 0x7fffffff, live ? kk : 0x7fffffff};
+  int hi[3] = {live ? ii : -1, live ? jj : -1, live ? kk : -1};
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+    hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
+  }
+  if (lane == 0 && hi[0] >= 0)
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&bmin[d], lo[d]);
+      atomicMax(&bmax[d], hi[d]);
+    }
+  __syncthreads();
+  const int ox = bmin[0], oy = bmin[1], oz = bmin[2];
+  const int bx = bmax[0] - ox + 2, by = bmax[1] - oy + 2, bz = bmax[2] - oz + 2;
+  const bool any = bmax[0] >= 0;
+  const bool use_box = any && (long long)bx * by * bz <= ADV_BOX;
+  if (use_box)
+    for (int n = tid; n < bx * by * bz; n += blockDim.x) {
+      box.lo[n] = 0u;
+      box.mid[n] = 0u;
+      box.hi[n] = 0u;
+    }
+  __syncthreads();
+  if (any) {
+    const double u0 = 1. - u1, v0 = 1. - v1, w0 = 1. - w1;
+    const int key = live ? ii + (g.nx + 1) * (jj + (g.ny + 1) * kk) : -1;
+    const int key0 = __shfl_sync(0xffffffffu, key, 0);
+    if (__all_sync(0xffffffffu, live && key == key0)) {
+      // one cell for the whole warp: lane n < 8 adds the warp's sum of node n
+      unsigned long long mine = 0ull;
+#pragma unroll
+      for (int n = 0; n < 8; ++n) {
+        const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
+        const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
+        unsigned long long v = (unsigned long long)llrint(wgt * kFixScale);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == n) mine = v;
+      }
+      if (lane < 8 && mine)
+        dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + (lane & 1), jj + ((lane >> 1) & 1), kk + (lane >> 2),
+                mine);
+    } else if (live) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int n = (j + lane) & 7;
+        const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
+        const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
+        const unsigned long long v = (unsigned long long)llrint(wgt * kFixScale);
+        if (v) dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + dx, jj + dy, kk + dz, v);
+      }
+    }
+  }
+  if (use_box) {
+    __syncthreads();
+    for (int n = tid; n < bx * by * bz; n += blockDim.x) {
+      const unsigned long long v =
+          ((unsigned long long)box.hi[n] << 32) + ((unsigned long long)box.mid[n] << 16) + box.lo[n];
+      if (v) {
+        const int lx = n % bx, ly = (n / bx) % by, lz = n / (bx * by);
+        atomicAdd(acc + (ox + lx) + (g.nx + 1) * ((oy + ly) + (g.ny + 1) * (oz + lz)), v);
+      }
+    }
+  }
+}
+
 // padvnc3d + particleboundaries3d for one particle per thread. CENTER 0 is
 // "fullv" (w3d.F:1862-1987): quad window (-dt/2, dt/2), half E kick, full-dt
 // Boris rotation, half E kick, drift. CENTER 1 is "halfv" (w3d.F:1989-2125),
@@ -538,16 +629,36 @@ struct PushP {
 // form, whose E is gathered in FP64 at the FP32 positions and then rounded.
 // The push constants (q dt / 2m, the lattice tables, the pipe radius) are
 // formed in FP64 and rounded once.
+// A z bound of the periodic wrap in the particle type: FP64 as given; in FP32
+// rounded towards the inside of [zmmin, zmmax] (a float rounded outward would
+// let a wrapped particle sit just past the grid, where its CIC weights leave
+// [0, 1]).
+template <typename T>
+__device__ __forceinline__ T inner_bound(double v, bool lower) {
+  if constexpr (sizeof(T) == 8) {
+    return v;
+  } else {
+    float f = (float)v;
+    if (lower && (double)f < v) f = nextafterf(f, INFINITY);
+    if (!lower && (double)f > v) f = nextafterf(f, -INFINITY);
+    return f;
+  }
+}
+
+// One particle of k_advance; returns whether it is live after the advance
+// (x, y, z are then its new position).
 template <typename T, int CENTER, bool COND>
-__global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ phi, GridP g, PushP P, CondE ce,
-                                                 T* __restrict__ xp, T* __restrict__ yp, T* __restrict__ zp,
-                                                 T* __restrict__ uxp, T* __restrict__ uyp, T* __restrict__ uzp,
-                                                 T* __restrict__ gaminv, int64_t np) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= np) return;
+__device__ __forceinline__ bool advance_one(const double* __restrict__ phi, const GridP& g, const PushP& P,
+                                            const CondE& ce, T* __restrict__ xp, T* __restrict__ yp,
+                                            T* __restrict__ zp, T* __restrict__ uxp, T* __restrict__ uyp,
+                                            T* __restrict__ uzp, T* __restrict__ gaminv, int64_t i, T& x, T& y,
+                                            T& z) {
   T gi = gaminv[i];
-  if (gi == (T)0) return;
-  T x = xp[i], y = yp[i], z = zp[i], ux = uxp[i], uy = uyp[i], uz = uzp[i];
+  if (gi == (T)0) return false;
+  x = xp[i];
+  y = yp[i];
+  z = zp[i];
+  T ux = uxp[i], uy = uyp[i], uz = uzp[i];
   T ex, ey, ez;
   {
     double exd, eyd, ezd;
@@ -610,7 +721,7 @@ __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ p
     uxp[i] = ux;
     uyp[i] = uy;
     uzp[i] = uz;
-    return;
+    return true;
   }
   ux = ux + ex * cst;
   uy = uy + ey * cst;
@@ -620,20 +731,55 @@ __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ p
   y = y + uy * gi * dt;
   z = z + uz * gi * dt;
   // periz (top.F:4015-4035)
-  const T zmmin = (T)P.zmmin, zmmax = (T)P.zmmax;
+  const T zmmin = inner_bound<T>(P.zmmin, true), zmmax = inner_bound<T>(P.zmmax, false);
   const T syslen = (T)(P.zmmax - P.zmmin), sysleni = (T)(1. / (P.zmmax - P.zmmin));
   if (z < zmmin) z = z + syslen * (T)(int)((zmmax - z) * sysleni);
   if (z > zmmax) z = z - syslen * (T)(int)((z - zmmin) * sysleni);
+  if constexpr (sizeof(T) == 4) {
+    // the FP32 wrap itself rounds: keep z inside [zmmin, zmmax], where the
+    // deposit's CIC fractions stay within [0, 1]
+    z = fmin(fmax(z, zmmin), zmmax);
+  }
   // stckxy3d round aperture
   const T rx = x - (T)P.prwallx, ry = y - (T)P.prwally;
   const T prw = (T)P.prwall;
-  if (rx * rx + ry * ry >= prw * prw) gaminv[i] = (T)0;
+  const bool lost = rx * rx + ry * ry >= prw * prw;
+  if (lost) gaminv[i] = (T)0;
   xp[i] = x;
   yp[i] = y;
   zp[i] = z;
   uxp[i] = ux;
   uyp[i] = uy;
   uzp[i] = uz;
+  return !lost;
+}
+
+// DEP: the advanced particles' charge is also added to the fixed-point
+// accumulator acc (block_deposit), as a deposit after the advance would.
+template <typename T, int CENTER, bool COND, bool DEP>
+__global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ phi, GridP g, PushP P, CondE ce,
+                                                 T* __restrict__ xp, T* __restrict__ yp, T* __restrict__ zp,
+                                                 T* __restrict__ uxp, T* __restrict__ uyp, T* __restrict__ uzp,
+                                                 T* __restrict__ gaminv, int64_t np,
+                                                 unsigned long long* __restrict__ acc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (!DEP) {
+    if (i >= np) return;
+    T x, y, z;
+    advance_one<T, CENTER, COND>(phi, g, P, ce, xp, yp, zp, uxp, uyp, uzp, gaminv, i, x, y, z);
+  } else {
+    __shared__ DepBoxN<ADV_BOX> box;
+    __shared__ int bmin[3], bmax[3];
+    if (threadIdx.x < 3) {
+      bmin[threadIdx.x] = 0x7fffffff;
+      bmax[threadIdx.x] = -1;
+    }
+    __syncthreads();
+    T x = 0, y = 0, z = 0;
+    const bool live = i < np && advance_one<T, CENTER, COND>(phi, g, P, ce, xp, yp, zp, uxp, uyp, uzp, gaminv, i,
+                                                             x, y, z);
+    block_deposit(live, (double)x, (double)y, (double)z, g, acc, box, bmin, bmax);
+  }
 }
 
 // Cell key of particlesortxyzwithcopy (top.F:5095-5130):
@@ -1064,8 +1210,11 @@ int fetch_e(wg_ctx* c, const double* x, const double* y, const double* z, double
   return WG_OK;
 }
 
+// deposit: also accumulate the advanced particles' charge into the open
+// chunked deposit (wg_deposit_begin .. wg_deposit_end), as wg_deposit_add
+// of the same particles after the advance would.
 template <typename PS>
-int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm) {
+int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = false) {
   using T = typename PElem<PS>::T;
   if (!p || !prm || p->np < 0 ||
       (p->np > 0 && (!p->x || !p->y || !p->z || !p->ux || !p->uy || !p->uz || !p->gaminv))) {
@@ -1080,20 +1229,38 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm) {
     set_error("wg_advance: center must be WG_CENTER_FULLV, WG_CENTER_HALFV or WG_CENTER_SYNCHV");
     return WG_EINVAL;
   }
+  if (deposit) {
+    if (!c->dep_open) {
+      set_error("wg_advance_deposit: no chunked deposit open (wg_deposit_begin)");
+      return WG_ESTATE;
+    }
+    double gg = p->w * p->q;
+    gg = gg / c->dx;
+    gg = gg / c->dy;
+    gg = gg / c->dz;
+    if (c->dep_gg_set && gg != c->dep_gg) {
+      set_error("wg_advance_deposit: the pieces of one deposit must share q and w");
+      return WG_EINVAL;
+    }
+    c->dep_gg = gg;
+    c->dep_gg_set = true;
+  }
   if (p->np == 0) return WG_OK;
+  if (cdiv64(p->np, 256) > 2147483647LL) { set_error("wg_advance: too many particles"); return WG_ETOOLARGE; }
   PushP P{p->q, p->m, prm->dt, c->grid.zmmin, c->grid.zmmax, prm->prwall, prm->prwallx, prm->prwally,
           prm->use_lattice ? c->czs : nullptr, c->cze, c->cdb, c->nzl, c->zlmin, c->dzl};
   CondE ce{};
   if (c->correctede) WG_TRY(prepare_correctede(c, &ce));
-  auto kern = c->correctede
-                  ? (prm->center == WG_CENTER_HALFV    ? k_advance<T, 1, true>
-                     : prm->center == WG_CENTER_SYNCHV ? k_advance<T, 2, true>
-                                                       : k_advance<T, 0, true>)
-                  : (prm->center == WG_CENTER_HALFV    ? k_advance<T, 1, false>
-                     : prm->center == WG_CENTER_SYNCHV ? k_advance<T, 2, false>
-                                                       : k_advance<T, 0, false>);
+  using K = void (*)(const double*, GridP, PushP, CondE, T*, T*, T*, T*, T*, T*, T*, int64_t, unsigned long long*);
+  // [correctede][deposit][center]
+  static const K kerns[2][2][3] = {
+      {{k_advance<T, 0, false, false>, k_advance<T, 1, false, false>, k_advance<T, 2, false, false>},
+       {k_advance<T, 0, false, true>, k_advance<T, 1, false, true>, k_advance<T, 2, false, true>}},
+      {{k_advance<T, 0, true, false>, k_advance<T, 1, true, false>, k_advance<T, 2, true, false>},
+       {k_advance<T, 0, true, true>, k_advance<T, 1, true, true>, k_advance<T, 2, true, true>}}};
+  const K kern = kerns[c->correctede ? 1 : 0][deposit ? 1 : 0][prm->center];
   { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, ce, p->x, p->y, p->z, p->ux, p->uy,
-                                                  p->uz, p->gaminv, p->np); c->prof_end(pe); }
+                                                  p->uz, p->gaminv, p->np, deposit ? c->racc : nullptr); c->prof_end(pe); }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }
@@ -1191,6 +1358,12 @@ int deposit_add(wg_ctx* c, const wg_particles* p) { return deposit_add_t(c, p); 
 int deposit_add_f32(wg_ctx* c, const wg_particles_f32* p) { return deposit_add_t(c, p); }
 int advance(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) { return advance_t(c, p, prm); }
 int advance_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm) { return advance_t(c, p, prm); }
+int advance_deposit(wg_ctx* c, const wg_particles* p, const wg_push_params* prm) {
+  return advance_t(c, p, prm, true);
+}
+int advance_deposit_f32(wg_ctx* c, const wg_particles_f32* p, const wg_push_params* prm) {
+  return advance_t(c, p, prm, true);
+}
 int moments(wg_ctx* c, const wg_particles* p, double* out) { return moments_t(c, p, out); }
 int moments_f32(wg_ctx* c, const wg_particles_f32* p, double* out) { return moments_t(c, p, out); }
 int zmoments(wg_ctx* c, const wg_particles* p, const double* uxo, const double* uyo, const double* uzo, double dt,

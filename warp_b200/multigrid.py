@@ -410,7 +410,8 @@ class MultiGridB200(FieldSolver):
                                            cdb.ctypes.data_as(_lib._dp), nzl, zlmin, dzl))
         self._lattice = (czs, cze, cdb, nzl, zlmin, dzl)
 
-    def advance(self, pgroup, dt, prwall=1.e30, prwallx=0., prwally=0., start=0, stop=None, center="fullv"):
+    def advance(self, pgroup, dt, prwall=1.e30, prwallx=0., prwally=0., start=0, stop=None, center="fullv",
+                deposit=False):
         """One fused particle advance of padvnc3d (w3d.F:1575) plus
         particleboundaries3d: gather E from phi, quad B (if a lattice is
         installed), the velocity push and drift that center selects, the
@@ -421,7 +422,10 @@ class MultiGridB200(FieldSolver):
         rotation, half E kick, drift. "synchv" (w3d.F:2187-2310): half E kick
         and half-dt rotation only, bringing velocities back to the
         positions' time. start/stop restrict it to a range of the group's
-        particles."""
+        particles. With deposit=True the advanced particles' charge is also
+        added to the deposit opened by deposit_begin(), in the same pass
+        (wg_advance_deposit): rho after deposit_end() is the same, bit for
+        bit, as a loadrho() of the advanced particles."""
         if center not in _lib.CENTERS:
             raise ValueError("center must be one of %s" % sorted(_lib.CENTERS))
         self._bind_stream()
@@ -430,7 +434,8 @@ class MultiGridB200(FieldSolver):
         s = pgroup.cstruct(start, stop)
         p = _lib.PushParams(float(dt), float(prwall), float(prwallx), float(prwally),
                             int(self._lattice is not None), _lib.CENTERS[center])
-        _lib.check(pgroup.fn("wg_advance")(self._h, ctypes.byref(s), ctypes.byref(p)))
+        _lib.check(pgroup.fn("wg_advance_deposit" if deposit else "wg_advance")(self._h, ctypes.byref(s),
+                                                                                ctypes.byref(p)))
 
     def zmoments(self, pgroup, uold, dt, zmmntmin, zmmntmax, nzmmnt, zbeam=0., dtscale=1., zmmntdtextmax=1e36):
         """The moment sums of getzmmnt (wg_zmoments): returns zmmnts0 (33,)

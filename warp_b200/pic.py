@@ -77,14 +77,26 @@ class ESPIC:
         return "halfv" if self.vsync else "fullv"
 
     def step(self, n=1):
+        """n steps of step3d: advance, particle boundaries, loadrho, solve.
+        The advance and the deposit run as one pass over the particles
+        (MultiGridB200.advance with deposit=True) when this run's group is
+        the solver's only species; rho is the same bit for bit."""
+        s, pg = self.solver, self.pgroup
+        fused = s.pgroups == [pg]
         for _ in range(n):
-            self.solver.advance(self.pgroup, self.dt, prwall=self.cfg["pipe_radius"], center=self._center())
+            if fused:
+                s.deposit_begin()
+            s.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], center=self._center(), deposit=fused)
             self.vsync = False
             if self.sort_interval > 0 and (self.it + 1) % self.sort_interval == 0:
-                # re-sort by cell (and drop lost particles) every sort_interval steps
-                self.pgroup.sort(self.solver)
-            self.solver.loadrho()
-            self.solver.solve()
+                # re-sort by cell (and drop lost particles) every sort_interval
+                # steps; the fixed-point deposit does not depend on the order
+                pg.sort(s)
+            if fused:
+                s.deposit_end(zero_first=True)
+            else:
+                s.loadrho()
+            s.solve()
             self.it += 1
 
     def step_host(self, host, nchunks=8):
@@ -148,8 +160,8 @@ class ESPIC:
                 a, b = edges[k], edges[k + 1]
                 main.wait_event(landed[k])
                 if b > a:
-                    s.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], start=a, stop=b, center=center)
-                    s.deposit_add(pg, a, b)
+                    s.advance(pg, self.dt, prwall=self.cfg["pipe_radius"], start=a, stop=b, center=center,
+                              deposit=True)
                 ev = torch.cuda.Event()
                 ev.record(main)
                 d2h.wait_event(ev)
