@@ -15,13 +15,15 @@ tests/golden/make_fodo_long_run.py) with 20000 and 200000 particles.
   (centred differences) and the phase space after 1000 steps against the
   plain run (which stands in for the oracle: it matches the fixture within
   1e-9 with the same V-cycle counts) are printed and bounded.
-- With 20000 particles (about 1.5 per occupied cell) single trajectories are
-  chaotic: any change of the order of the FP32 rounding grows to a
-  decorrelation of the phase space of about 1e-2 over 1000 steps, and the
-  emittance then moves by about 1e-2 / sqrt(N). An FP64 run started from the
-  FP32-rounded particles (FP64 afterwards) deviates from the oracle by as
-  much as the mixed form does, so the deviation there is the sensitivity of
-  this sparse beam, not a bias of the FP32 push; both are bounded.
+- With 20000 particles (about 1.5 per occupied cell) the mixed form's
+  emittance moves from the oracle's by about 1.7e-4 (measured), while an
+  FP64 run started from the FP32-rounded particles stays within 1e-6: the
+  difference is not the rounding of the start. It is the lost-particle set:
+  a halo particle at the pipe wall that the FP32 push keeps and the FP64
+  push absorbs (or the reverse) carries r^2 about six times the rms, which
+  moves the emittance of a 2e4-particle beam by about 1e-4. Over the
+  particles live in both runs the mixed form's final emittances agree with
+  the plain run's (the oracle's stand-in) within 1e-4.
 
 On the oracle the collective quantities respond linearly to small smooth
 changes of the field: a 1e-8 relative change of rho moves the emittance by
@@ -132,16 +134,32 @@ def test_fodo_1000_steps_mixed_against_oracle_200k():
     assert max(dps.values()) <= 5e-2
 
 
-def test_fodo_1000_steps_sparse_beam_sensitivity_20k():
+def _emittance(p, sel):
+    """4 sqrt(<dx^2><dx'^2> - <dx dx'>^2), x' = ux/uz, over the particles sel."""
+    out = []
+    for q, u in (("x", "ux"), ("y", "uy")):
+        a = p[q][sel]
+        ap = p[u][sel] / p["uz"][sel]
+        a, ap = a - a.mean(), ap - ap.mean()
+        out.append(4. * np.sqrt(np.mean(a * a) * np.mean(ap * ap) - np.mean(a * ap) ** 2))
+    return np.array(out)
+
+
+def test_fodo_1000_steps_sparse_beam_20k():
     torch.cuda.set_device(0)
     g = np.load(FIXTURE)
-    ex, ey, live, vc, _, _ = _run("mixed", g)
+    _, parts_p = _check_plain(g)
+    ex, ey, live, vc, _, parts_m = _run("mixed", g)
     dev_m = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
     ex, ey, live_r, vc, _, _ = _run("fp64", g, round_start=True)
     dev_r = max(_rel(ex, g["epsx"]), _rel(ey, g["epsy"]))
+    lp, lm = parts_p["gaminv"] != 0, parts_m["gaminv"] != 0
+    both = lp & lm
+    common = np.max(np.abs(_emittance(parts_m, both) / _emittance(parts_p, both) - 1.))
     print("20000 particles: max rel emittance deviation from the oracle: mixed %.2e, FP64 from FP32-rounded "
-          "particles %.2e" % (dev_m, dev_r))
-    assert np.max(np.abs(live - g["live"])) <= 2
-    assert dev_m <= 5e-4 and dev_r <= 5e-4
-    # the deviation is the beam's sensitivity to a rounding-sized change
-    assert dev_r >= 1e-5 and dev_m <= 5 * dev_r
+          "particles %.2e; lost differently %d; mixed vs plain over the common live set after 1000 steps %.2e"
+          % (dev_m, dev_r, int(np.sum(lp != lm)), common))
+    assert np.max(np.abs(live - g["live"])) <= 2 and int(np.sum(lp != lm)) <= 2
+    assert dev_r <= 1e-5
+    assert dev_m <= 5e-4
+    assert common <= 1e-4

@@ -535,10 +535,27 @@ struct PushP {
 // the accumulator at the end; when the box is larger than ADV_BOX nodes
 // each lane adds to the accumulator directly. A warp whose 32 particles sit
 // in one cell sums them in registers first. All threads of the CTA call it.
-constexpr int ADV_BOX = 1024;
+// A CTA adds at most 256 particles' weights (each below 2^46 + 1) to a node,
+// so the box holds two 32-bit parts per node, bits 0-22 and 23 up: each part
+// sums below 2^31, and the two adds per node weight are a third fewer shared
+// atomics than k_deposit's three parts.
+constexpr int ADV_BOX = 1536;
+struct AdvBox {
+  unsigned lo[ADV_BOX], hi[ADV_BOX];
+};
+__device__ inline void adv_add(AdvBox& box, bool use_box, int ox, int oy, int oz, int bx, int by,
+                               unsigned long long* acc, const GridP& g, int i, int j, int k, unsigned long long v) {
+  if (use_box) {
+    const int n = (i - ox) + bx * ((j - oy) + by * (k - oz));
+    const unsigned l = (unsigned)(v & 0x7FFFFFull), h = (unsigned)(v >> 23);
+    if (l) atomicAdd(&box.lo[n], l);
+    if (h) atomicAdd(&box.hi[n], h);
+  } else {
+    atomicAdd(acc + i + (g.nx + 1) * (j + (g.ny + 1) * k), v);
+  }
+}
 __device__ inline void block_deposit(bool live, double x, double y, double z, const GridP& g,
-                                     unsigned long long* __restrict__ acc, DepBoxN<ADV_BOX>& box, int* bmin,
-                                     int* bmax) {
+                                     unsigned long long* __restrict__ acc, AdvBox& box, int* bmin, int* bmax) {
   const int tid = threadIdx.x, lane = tid & 31;
   int ii = 0, jj = 0, kk = 0;
   double u1 = 0., v1 = 0., w1 = 0.;
@@ -566,7 +583,6 @@ __device__ inline void block_deposit(bool live, double x, double y, double z, co
   if (use_box)
     for (int n = tid; n < bx * by * bz; n += blockDim.x) {
       box.lo[n] = 0u;
-      box.mid[n] = 0u;
       box.hi[n] = 0u;
     }
   __syncthreads();
@@ -587,7 +603,7 @@ __device__ inline void block_deposit(bool live, double x, double y, double z, co
         if (lane == n) mine = v;
       }
       if (lane < 8 && mine)
-        dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + (lane & 1), jj + ((lane >> 1) & 1), kk + (lane >> 2),
+        adv_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + (lane & 1), jj + ((lane >> 1) & 1), kk + (lane >> 2),
                 mine);
     } else if (live) {
 #pragma unroll
@@ -596,15 +612,14 @@ __device__ inline void block_deposit(bool live, double x, double y, double z, co
         const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
         const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
         const unsigned long long v = (unsigned long long)llrint(wgt * kFixScale);
-        if (v) dep_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + dx, jj + dy, kk + dz, v);
+        if (v) adv_add(box, use_box, ox, oy, oz, bx, by, acc, g, ii + dx, jj + dy, kk + dz, v);
       }
     }
   }
   if (use_box) {
     __syncthreads();
     for (int n = tid; n < bx * by * bz; n += blockDim.x) {
-      const unsigned long long v =
-          ((unsigned long long)box.hi[n] << 32) + ((unsigned long long)box.mid[n] << 16) + box.lo[n];
+      const unsigned long long v = ((unsigned long long)box.hi[n] << 23) + box.lo[n];
       if (v) {
         const int lx = n % bx, ly = (n / bx) % by, lz = n / (bx * by);
         atomicAdd(acc + (ox + lx) + (g.nx + 1) * ((oy + ly) + (g.ny + 1) * (oz + lz)), v);
@@ -768,7 +783,7 @@ __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ p
     T x, y, z;
     advance_one<T, CENTER, COND>(phi, g, P, ce, xp, yp, zp, uxp, uyp, uzp, gaminv, i, x, y, z);
   } else {
-    __shared__ DepBoxN<ADV_BOX> box;
+    __shared__ AdvBox box;
     __shared__ int bmin[3], bmax[3];
     if (threadIdx.x < 3) {
       bmin[threadIdx.x] = 0x7fffffff;
