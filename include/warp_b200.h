@@ -310,17 +310,25 @@ int wg_launch_count(wg_ctx* ctx, int64_t* n);
 /* ---- learned warm start: BF16 tensor-core 3x3x3 convolutions (no
  * reference counterpart: WARP has no learned components) ------------------ */
 
-/* y[v][yoff+co] = relu?(bias[co] + sum_{t,ci} x[v+off_t][ci] * w[t][co][ci]),
- * optionally multiplied by (mask[v][co] > 0). x: [D][H][W][cin] bf16,
- * w: [27][cout][cin] bf16 (tap t = 9*(dz+1) + 3*(dy+1) + (dx+1)), bias fp32 or
- * NULL, y: [D][H][W][ystride] bf16. cin, cout multiples of 16, cout <= 256.
- * Zero padding outside the box. *err is set non-zero if a wait timed out. */
+/* y[v][yoff+co] = relu?(bias[co] + sum_{t,ci} x[v+off_t][ci] * W[t][co][ci]),
+ * optionally multiplied by (mask[v][co] > 0). x: [D][H][W][cin] bf16; w: the
+ * weights W packed as [27][cin/8][cout][8] bf16, i.e. w[t][g][co][j] =
+ * W[t][co][8g+j] (tap t = 9*(dz+1) + 3*(dy+1) + (dx+1)); bias fp32 or NULL;
+ * y: [D][H][W][ystride] bf16. cin, cout multiples of 16, cout <= 256; x, w, y
+ * 16-byte aligned. Zero padding outside the box. *err is set non-zero if a
+ * wait timed out. */
 int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
                  int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream);
-/* dw[t][co][ci] += sum_v dy[v][co] * x[v+off_t][ci] with channel-major
- * operands xT: [cin][D][H][W], dyT: [cout][D][H][W] (bf16), dw fp32. */
-int wg_conv3_wgrad(const void* xT, const void* dyT, int D, int H, int W, int cin, int cout, float* dw, int* err,
-                   void* stream);
+/* dw[t][co][ci] = sum_v dy[v][co] * x[v+off_t][ci] (fp32; overwritten), from
+ * x: [D][H][W][cin] and dy: [D][H][W][cout] bf16 (16-byte aligned), cin a
+ * multiple of 16 up to 256, cout a multiple of 16 up to 128. CTAs write
+ * partial sums to `scratch` (device, at least the size wg_conv3_wgrad_scratch
+ * reports) and a second kernel adds them in a fixed order: the result is the
+ * same bits on every run. *err is set non-zero if a wait timed out. */
+int wg_conv3_wgrad(const void* x, const void* dy, int D, int H, int W, int cin, int cout, float* dw, float* scratch,
+                   int64_t scratch_floats, int* err, void* stream);
+/* Floats of scratch wg_conv3_wgrad needs for (cin, cout) on the current device. */
+int wg_conv3_wgrad_scratch(int cin, int cout, int64_t* nfloats);
 
 #ifdef __cplusplus
 }

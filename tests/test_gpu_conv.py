@@ -51,7 +51,7 @@ def test_conv3_fwd_offset_and_mask():
     assert np.max(np.abs(got[..., 16:] - ref)) <= 1e-2 * np.max(np.abs(ref)) + 1e-2
 
 
-@pytest.mark.parametrize("cin,cout", [(32, 16), (192, 64)])
+@pytest.mark.parametrize("cin,cout", [(32, 16), (192, 64), (16, 16), (48, 16), (64, 128), (128, 128), (96, 32)])
 def test_conv3_dgrad_and_wgrad_match_oracle(cin, cout):
     from warp_b200 import unet
     D, H, W = 6, 5, 20
@@ -61,6 +61,8 @@ def test_conv3_dgrad_and_wgrad_match_oracle(cin, cout):
     dx = unet.conv3_fwd(dy.cuda(), unet.flip_transpose(w.cuda()), None, relu=False)
     dw = unet.conv3_wgrad(x.cuda(), dy.cuda())
     unet.check_errors(dx.device)
+    # fixed-order partial sums: the same bits on a second run
+    assert torch.equal(unet.conv3_wgrad(x.cuda(), dy.cuda()), dw)
     rdx = co.conv3_dgrad(dy.float().numpy(), w.float().numpy())
     rdw = co.conv3_wgrad(x.float().numpy(), dy.float().numpy())
     assert np.max(np.abs(dx.float().cpu().numpy() - rdx)) <= 1e-2 * np.max(np.abs(rdx)) + 1e-2

@@ -12,11 +12,8 @@ The V-cycle counts of both starts are measured and printed. On this problem
 the learned start saves no V-cycles, and the test records that rather than
 asserting a gain.
 
-The weight gradients are summed over the spatial tiles with float atomics,
-so two trainings from the same seed differ in the last bits, and now and
-then one collapses to the zero output (held-out ratio 1.000, where runs
-otherwise give about 0.3). The test then trains once more from another
-seed; the gain must show in one of the two.
+The weight gradients are summed in a fixed order, so a training is the same
+bits on every run: one seed, no retry.
 """
 import pytest
 import torch
@@ -32,12 +29,14 @@ def test_learned_warm_start_gain_and_convergence():
     out_scale = wt.fit_out_scale(srs, ds)
     ys = wt.targets(srs, ds, out_scale)
     nval = 8
-    for seed in (5, 6):
-        net, hist = wt.train(xs[nval:], ys[nval:], epochs=4, seed=seed, log=lambda *a: None)
-        mse, mse0 = wt.evaluate(net, xs[:nval], ys[:nval])
-        print("seed %d: held-out mse: learned %.4g, zero correction %.4g (ratio %.3f)" % (seed, mse, mse0, mse / mse0))
-        if mse < 0.8 * mse0:
-            break
+    net, hist = wt.train(xs[nval:], ys[nval:], epochs=4, seed=5, log=lambda *a: None)
+    mse, mse0 = wt.evaluate(net, xs[:nval], ys[:nval])
+    print("held-out mse: learned %.4g, zero correction %.4g (ratio %.3f)" % (mse, mse0, mse / mse0))
+    # a second training from the same seed gives the same weights
+    net2, _ = wt.train(xs[nval:nval + 8], ys[nval:nval + 8], epochs=1, seed=5, log=lambda *a: None)
+    net3, _ = wt.train(xs[nval:nval + 8], ys[nval:nval + 8], epochs=1, seed=5, log=lambda *a: None)
+    for k, v in net2.state_dict().items():
+        assert torch.equal(v, net3.state_dict()[k]), k
     assert hist[-1] < hist[0]
     assert mse < 0.8 * mse0
     ws = WarmStart(net, out_scale=out_scale, smooth="coarse4")

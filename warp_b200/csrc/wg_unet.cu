@@ -2,27 +2,22 @@
 // the learned multigrid warm start (a small 3D U-Net). No reference
 // counterpart: WARP has no learned components.
 //
-// Forward / data-gradient (k_conv3_mma): implicit GEMM
+// Forward / data gradient (k_conv3_tile): implicit GEMM
 //   Y[v][co] = sum_{t<27} sum_ci X[v + off_t][ci] * Wt[t][co][ci]   (+bias, ReLU)
-// with X and Y in NDHWC bf16 (channels fastest), zero padding at the box
-// edges. A CTA computes M = 128 consecutive output voxels by N = Cout
-// channels; the K loop runs over taps and 16-channel slices. Operand tiles
-// are staged in shared memory in the canonical K-major no-swizzle layout of
-// UMMA (8x16-byte core matrices), one elected thread issues
-// tcgen05.mma.cta_group::1.kind::f16 with FP32 accumulation in tensor memory,
-// completion is tracked with tcgen05.commit on mbarriers (bounded waits),
-// and the epilogue reads the accumulator back with tcgen05.ld. The data
-// gradient is the same kernel with the taps mirrored and Cin/Cout swapped in
-// the weights.
-//
-// Weight gradient (k_conv3_wgrad_mma): per tap t,
+// with X and Y in NDHWC bf16 (channels fastest) and zero padding at the box
+// edges, over output tiles whose input halo stays in shared memory for all
+// 27 taps. The data gradient is the same kernel with the taps mirrored and
+// Cin/Cout swapped in the weights.
+// Weight gradient (k_conv3_wgrad_tile + k_wgrad_reduce): per tap
 //   dW[t][co][ci] = sum_v dY[v][co] * X[v + off_t][ci]
-// a GEMM with K = voxels, from channel-major (CDHW) copies of dY and X so
-// both operands are K-major; CTAs take voxel chunks and add their FP32
-// partial sums to dW atomically.
+// over the same halo tiles, with fixed-order partial sums.
+// One elected thread issues tcgen05.mma.cta_group::1.kind::f16 (BF16 in,
+// FP32 accumulators in tensor memory); completion is tracked with
+// tcgen05.commit on mbarriers; every wait is bounded.
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "wg_internal.h"
@@ -30,9 +25,6 @@
 namespace wg {
 namespace {
 
-constexpr int CM = 128;      // output voxels per CTA (UMMA M)
-constexpr int CNT = 128;     // threads per CTA
-constexpr int CSTAGES = 4;   // shared-memory pipeline stages
 constexpr long long kSpinLimit = 1LL << 26;  // mbarrier poll limit before giving up
 
 __device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -108,237 +100,435 @@ __device__ inline void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Byte offset of element (row, k) (k < 16) in a K-major no-swizzle tile:
-// 8-row groups 256 B apart, the two 8-element K halves 128 B apart.
-__device__ inline uint32_t kmaj_off(int row, int k) {
-  return (uint32_t)((row >> 3) * 256 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
-}
+// ---- forward / data gradient: halo tiles, warp-specialised -----------------
+//
+// A tile is TX x TY output voxels of one z plane (M = 128 GEMM rows, row m =
+// voxel (x0 + m % TX, y0 + m / TX, z0)). Its input halo, (TX+2) x (TY+2) x 3
+// voxels of KC channels, sits in shared memory as [KC/8][z][y][x][8 channels]
+// (16 bytes per voxel and channel group). In that layout the A operand of
+// every tap (dx, dy, dz) is the same K-major, no-swizzle matrix shifted by
+// 16 * (dx + HX * (dy + HY * dz)) bytes: eight rows of a core matrix are eight
+// x-consecutive voxels (16 bytes apart), 8-row groups are HX voxels apart
+// (SBO = 16 * HX) and the two 8-channel halves of a 16-channel slice are one
+// channel-group plane apart (LBO = 16 * HVOX). So one halo load serves all 27
+// taps. The weights come pre-packed as [27][cin/8][cout][8]: the block of
+// one tap and one channel chunk is contiguous and is a K-major B operand
+// (SBO = 128, LBO = 16 * cout) as it lands, so it is brought in by one bulk
+// copy. Roles (320 threads):
+//   warps 0-3  halo loads (16-byte cp.async with zero fill outside the box),
+//   warp 4     one thread issues the tcgen05.mma of every tap and slice,
+//   warp 5     one thread streams the weight blocks (cp.async.bulk),
+//   warps 6-9  epilogue: tcgen05.ld of their TMEM lane quarter, bias, ReLU,
+//              mask, bf16 stores.
+// The CTA is persistent over tiles; the accumulator is double-buffered in
+// TMEM so the epilogue of one tile overlaps the MMAs of the next. Every wait
+// is bounded: on a time-out the role stops, sets the error flag, and the CTA
+// still frees its TMEM after its last MMA has completed.
+constexpr int TX = 8, TY = 16;
+constexpr int HX = TX + 2, HY = TY + 2;
+constexpr int FT = 320;
+constexpr int NLOAD = 128;
+constexpr int MAXHS = 4, MAXWS = 12;
+constexpr int kConvSmem = 227 * 1024;
 
-struct ConvArgs {
-  const __nv_bfloat16* x;   // [D][H][W][cin]
-  const __nv_bfloat16* w;   // [27][cout][cin]
-  const float* bias;        // [cout] or null
-  __nv_bfloat16* y;         // [D][H][W][ystride], channels yoff..yoff+cout-1 written
-  const __nv_bfloat16* mask;  // optional [D][H][W][mstride] activation: y *= (mask > 0)
+struct FwdArgs {
+  const __nv_bfloat16* x;     // [D][H][W][cin]
+  const __nv_bfloat16* w;     // [27][cin/8][cout][8]
+  const float* bias;          // [cout] or null
+  __nv_bfloat16* y;           // [D][H][W][ystride], channels yoff..yoff+cout-1 written
+  const __nv_bfloat16* mask;  // optional [D][H][W][mstride]: y *= (mask > 0)
   int D, H, W, cin, cout, ystride, yoff, mstride, relu;
+  int kc, nchunk, hs, ws;     // channels per chunk, chunks, halo stages, weight stages
+  int zg, hvox;               // z planes per work item, halo voxels (HX * HY * (zg + 2))
+  int ntx, nty, ntz;
+  long long ntiles;           // work items: ntx * nty * ntz
+  uint32_t tmem_cols;
   int* err;
 };
 
-// Forward / data-gradient implicit GEMM, N = cout (16..256, multiple of 16).
-__global__ void __launch_bounds__(CNT) k_conv3_mma(ConvArgs a) {
-  extern __shared__ __align__(1024) unsigned char sm[];
-  const int N = a.cout;
-  const int a_bytes = CM * 32;   // 128 rows x 16 bf16
-  const int b_bytes = N * 32;
-  const int stage_bytes = a_bytes + b_bytes;
-  __shared__ __align__(8) uint64_t bars[CSTAGES + 1];
-  __shared__ uint32_t tmem_base_s;
-  __shared__ int fail_s;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long nvox = (long long)a.D * a.H * a.W;
-  const long long v0 = (long long)blockIdx.x * CM;
-  uint32_t ncols = 32;
-  while ((int)ncols < N) ncols <<= 1;
-
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
-                 "r"(ncols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  if (tid == 0) {
-    for (int s = 0; s <= CSTAGES; ++s) mbar_init(&bars[s], 1);
-    fail_s = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = tmem_base_s;
-
-  // this thread's A row: output voxel v0 + tid
-  const long long vr = v0 + tid;
-  const bool row_ok = vr < nvox;
-  int rx = 0, ry = 0, rz = 0;
-  if (row_ok) {
-    rx = (int)(vr % a.W);
-    ry = (int)((vr / a.W) % a.H);
-    rz = (int)(vr / ((long long)a.W * a.H));
-  }
-  const int kslices = a.cin >> 4;
-  const int nsteps = 27 * kslices;
-  const uint32_t idesc = make_idesc(CM, N);
-  bool ok = true;
-  for (int j = 0; j < nsteps; ++j) {
-    const int s = j % CSTAGES;
-    unsigned char* st = sm + s * stage_bytes;
-    if (j >= CSTAGES) {
-      // the MMA that last read this stage must be done
-      if (!mbar_wait(&bars[s], (uint32_t)(((j / CSTAGES) - 1) & 1))) ok = false;
-    }
-    const int t = j / kslices, ks = j % kslices;
-    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-    // A: 16 channels of the shifted input voxel (zero outside the box)
-    {
-      uint4 lo = make_uint4(0, 0, 0, 0), hi = make_uint4(0, 0, 0, 0);
-      const int xx = rx + dx, yy = ry + dy, zz = rz + dz;
-      if (row_ok && xx >= 0 && xx < a.W && yy >= 0 && yy < a.H && zz >= 0 && zz < a.D) {
-        const uint4* src = reinterpret_cast<const uint4*>(
-            a.x + (((long long)zz * a.H + yy) * a.W + xx) * a.cin + ks * 16);
-        lo = src[0];
-        hi = src[1];
-      }
-      *reinterpret_cast<uint4*>(st + kmaj_off(tid, 0)) = lo;
-      *reinterpret_cast<uint4*>(st + kmaj_off(tid, 8)) = hi;
-    }
-    // B: weights of tap t, channels ks*16.., all N output channels
-    for (int i = tid; i < 2 * N; i += CNT) {
-      const int n = i >> 1, h = i & 1;
-      const uint4 v = *reinterpret_cast<const uint4*>(a.w + ((long long)t * N + n) * a.cin + ks * 16 + h * 8);
-      *reinterpret_cast<uint4*>(st + a_bytes + kmaj_off(n, h * 8)) = v;
-    }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t sa = smem_u32(st), sb = smem_u32(st + a_bytes);
-      umma_f16(tmem, make_sdesc(sa, 128, 256), make_sdesc(sb, 128, 256), idesc, j > 0 ? 1u : 0u);
-      umma_commit(&bars[s]);
-    }
-  }
-  // all MMAs done: the last commit covers every earlier MMA of this thread
-  if (tid == 0) umma_commit(&bars[CSTAGES]);
-  if (!mbar_wait(&bars[CSTAGES], 0)) ok = false;
-  tc_fence_after();
-  if (!ok) atomicOr(&fail_s, 1);
-  __syncthreads();
-  if (!fail_s) {
-    // epilogue: row m = 32*warp + lane, 16 columns at a time
-    const long long v = v0 + 32 * warp + lane;
-    for (int c0 = 0; c0 < N; c0 += 16) {
-      float f[16];
-      tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, f);
-      if (v < nvox) {
-        __nv_bfloat16 out[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          float r = f[i] + (a.bias ? a.bias[c0 + i] : 0.f);
-          if (a.relu) r = fmaxf(r, 0.f);
-          if (a.mask && !(__bfloat162float(a.mask[v * a.mstride + c0 + i]) > 0.f)) r = 0.f;
-          out[i] = __float2bfloat16_rn(r);
-        }
-        __nv_bfloat16* dst = a.y + v * a.ystride + a.yoff + c0;
-        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<uint4*>(&out[0]);
-        *reinterpret_cast<uint4*>(dst + 8) = *reinterpret_cast<uint4*>(&out[8]);
-      }
-    }
-  } else if (tid == 0) {
-    atomicOr(a.err, 1);
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+__device__ inline void cp_async16(uint32_t dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ inline void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+__device__ inline void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Untiled bulk copy global -> this CTA's shared memory, completing on bar.
+__device__ inline void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
 
-struct WgradArgs {
-  const __nv_bfloat16* xT;   // [cin][D][H][W]
-  const __nv_bfloat16* dyT;  // [cout][D][H][W]
-  float* dw;                 // [27][cout][cin], accumulated
-  int D, H, W, cin, cout, mpad;
-  long long chunk;           // voxels per CTA (multiple of 16)
-  int* err;
-};
+__device__ inline void tile_origin(const FwdArgs& a, long long t, int& x0, int& y0, int& z0) {
+  x0 = (int)(t % a.ntx) * TX;
+  y0 = (int)((t / a.ntx) % a.nty) * TY;
+  z0 = (int)(t / ((long long)a.ntx * a.nty)) * a.zg;
+}
 
-// Weight gradient of one tap (blockIdx.y) over one voxel chunk (blockIdx.x):
-// D[co][ci] = sum_v dY[co][v] * X[ci][v + off_t]; M = cout padded to 64/128,
-// N = cin.
-__global__ void __launch_bounds__(CNT) k_conv3_wgrad_mma(WgradArgs a) {
+__global__ void __launch_bounds__(FT, 1) k_conv3_tile(FwdArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int M = a.mpad, N = a.cin;
-  const int a_bytes = M * 32, b_bytes = N * 32, stage_bytes = a_bytes + b_bytes;
-  __shared__ __align__(8) uint64_t bars[CSTAGES + 1];
-  __shared__ uint32_t tmem_base_s;
+  __shared__ __align__(8) uint64_t hfull[MAXHS], hempty[MAXHS], wfull[MAXWS], wempty[MAXWS], afull[2], aempty[2],
+      fin;
+  __shared__ uint32_t tmem_s;
   __shared__ int fail_s;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int t = blockIdx.y;
-  const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-  const long long nvox = (long long)a.D * a.H * a.W;
-  const long long k0 = (long long)blockIdx.x * a.chunk;
-  const long long k1 = min(nvox, k0 + a.chunk);
-  uint32_t ncols = 32;
-  while ((int)ncols < N) ncols <<= 1;
+  const int HVOX = a.hvox;
+  const uint32_t halo_bytes = (uint32_t)HVOX * a.kc * 2, w_bytes = (uint32_t)a.cout * a.kc * 2;
+  unsigned char* halo = sm;
+  unsigned char* wring = sm + (size_t)a.hs * halo_bytes;
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
-                 "r"(ncols));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_s)),
+                 "r"(a.tmem_cols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int s = 0; s <= CSTAGES; ++s) mbar_init(&bars[s], 1);
+    for (int i = 0; i < a.hs; ++i) {
+      mbar_init(&hfull[i], NLOAD);
+      mbar_init(&hempty[i], 1);
+    }
+    for (int i = 0; i < a.ws; ++i) {
+      mbar_init(&wfull[i], 1);
+      mbar_init(&wempty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&afull[i], 1);
+      mbar_init(&aempty[i], 128);
+    }
+    mbar_init(&fin, 1);
     fail_s = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = tmem_base_s;
-  const uint32_t idesc = make_idesc(M, N);
-  const int nsteps = (int)((k1 - k0 + 15) / 16);
+  const uint32_t tmem = tmem_s;
   bool ok = true;
-  for (int j = 0; j < nsteps; ++j) {
-    const int s = j % CSTAGES;
-    unsigned char* st = sm + s * stage_bytes;
-    if (j >= CSTAGES && !mbar_wait(&bars[s], (uint32_t)(((j / CSTAGES) - 1) & 1))) ok = false;
-    const long long kb = k0 + 16LL * j;
-    // A: dY rows (output channels, zero above cout), 16 voxels each
-    for (int i = tid; i < M * 16; i += CNT) {
-      const int row = i >> 4, k = i & 15;
-      const long long v = kb + k;
-      __nv_bfloat16 e = __float2bfloat16_rn(0.f);
-      if (row < a.cout && v < k1) e = a.dyT[(long long)row * nvox + v];
-      *reinterpret_cast<__nv_bfloat16*>(st + kmaj_off(row, k)) = e;
-    }
-    // B: X rows (input channels) at the voxel shifted by the tap offset
-    for (int i = tid; i < N * 16; i += CNT) {
-      const int row = i >> 4, k = i & 15;
-      const long long v = kb + k;
-      __nv_bfloat16 e = __float2bfloat16_rn(0.f);
-      if (v < k1) {
-        const int x = (int)(v % a.W) + dx, y = (int)((v / a.W) % a.H) + dy, z = (int)(v / ((long long)a.W * a.H)) + dz;
-        if (x >= 0 && x < a.W && y >= 0 && y < a.H && z >= 0 && z < a.D)
-          e = a.xT[(long long)row * nvox + ((long long)z * a.H + y) * a.W + x];
+  if (warp < 4) {
+    // halo loads
+    const int cg8 = a.kc >> 3;
+    long long j = 0;
+    for (long long t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
+      int x0, y0, z0;
+      tile_origin(a, t, x0, y0, z0);
+      for (int c = 0; c < a.nchunk; ++c, ++j) {
+        const int hb = (int)(j % a.hs);
+        const long long r = j / a.hs;
+        if (r >= 1 && !mbar_wait(&hempty[hb], (uint32_t)((r - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        const uint32_t dst = smem_u32(halo + (size_t)hb * halo_bytes);
+        for (int p = tid; p < HVOX * cg8; p += NLOAD) {
+          const int cg = p % cg8, v = p / cg8;
+          const int gx = x0 - 1 + v % HX, gy = y0 - 1 + (v / HX) % HY, gz = z0 - 1 + v / (HX * HY);
+          const bool in = gx >= 0 && gx < a.W && gy >= 0 && gy < a.H && gz >= 0 && gz < a.D;
+          const __nv_bfloat16* src =
+              in ? a.x + (((long long)gz * a.H + gy) * a.W + gx) * a.cin + c * a.kc + cg * 8 : a.x;
+          cp_async16(dst + (uint32_t)(cg * HVOX + v) * 16u, src, in ? 16 : 0);
+        }
+        cp_async_wait_all();
+        fence_async_smem();
+        mbar_arrive(&hfull[hb]);
       }
-      *reinterpret_cast<__nv_bfloat16*>(st + a_bytes + kmaj_off(row, k)) = e;
     }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+  } else if (warp == 5) {
+    // weight blocks
+    if (lane == 0) {
+      long long q = 0;
+      for (long long t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
+        for (int c = 0; c < a.nchunk && ok; ++c) {
+          for (int tap = 0; tap < 27; ++tap, ++q) {
+            const int ws = (int)(q % a.ws);
+            const long long r = q / a.ws;
+            if (r >= 1 && !mbar_wait(&wempty[ws], (uint32_t)((r - 1) & 1))) {
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(&wfull[ws], w_bytes);
+            const __nv_bfloat16* src = a.w + ((size_t)tap * (a.cin >> 3) + (size_t)c * (a.kc >> 3)) * a.cout * 8;
+            bulk_g2s(smem_u32(wring + (size_t)ws * w_bytes), src, w_bytes, &wfull[ws]);
+          }
+        }
+      }
+    }
+  } else if (warp == 4) {
+    // MMA issue
+    if (lane == 0) {
+      const uint32_t idesc = make_idesc(128, a.cout);
+      long long j = 0, q = 0, li = 0;
+      for (long long t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x, ++li) {
+        const int ab = (int)(li & 1);
+        const long long ar = li >> 1;
+        if (ar >= 1 && !mbar_wait(&aempty[ab], (uint32_t)((ar - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t dcol = tmem + (uint32_t)(ab * a.zg * a.cout);
+        for (int c = 0; c < a.nchunk && ok; ++c, ++j) {
+          const int hb = (int)(j % a.hs);
+          if (!mbar_wait(&hfull[hb], (uint32_t)((j / a.hs) & 1))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          // Descriptors are built once per halo and weight slot; the start
+          // address field (bits 0-13, 16-byte units) is then advanced by plain
+          // adds (every shared address here is below 256 KB, so the field
+          // never carries into the next one).
+          const uint64_t ad0 = make_sdesc(smem_u32(halo + (size_t)hb * halo_bytes), (uint32_t)HVOX * 16u, HX * 16);
+          const int nsl = a.kc >> 4;
+          for (int tap = 0; tap < 27; ++tap, ++q) {
+            const int ws = (int)(q % a.ws);
+            if (!mbar_wait(&wfull[ws], (uint32_t)((q / a.ws) & 1))) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;  // offsets + 1
+            const uint64_t bd0 = make_sdesc(smem_u32(wring + (size_t)ws * w_bytes), (uint32_t)a.cout * 16u, 128u);
+            // one weight block feeds the zg planes of the work item
+            uint64_t adp = ad0 + (uint64_t)(dx + HX * (dy + HY * dz));
+            uint32_t dc = dcol;
+            for (int i = 0; i < a.zg; ++i, adp += HX * HY, dc += (uint32_t)a.cout) {
+              uint64_t ad = adp, bd = bd0;
+              for (int sl = 0; sl < nsl; ++sl, ad += 2 * HVOX, bd += 2 * a.cout)
+                umma_f16(dc, ad, bd, idesc, (c | tap | sl) ? 1u : 0u);
+            }
+            umma_commit(&wempty[ws]);
+          }
+          umma_commit(&hempty[hb]);
+        }
+        umma_commit(&afull[ab]);
+      }
+      // no MMA may still run when the TMEM is freed
+      umma_commit(&fin);
+      if (!mbar_wait(&fin, 0)) ok = false;
+    }
+  } else if (warp >= 6) {
+    // epilogue
+    const int qtr = warp & 3;
+    const int m = 32 * qtr + lane;
+    long long li = 0;
+    for (long long t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x, ++li) {
+      const int ab = (int)(li & 1);
+      if (!mbar_wait(&afull[ab], (uint32_t)((li >> 1) & 1))) {
+        ok = false;
+        break;
+      }
       tc_fence_after();
-      umma_f16(tmem, make_sdesc(smem_u32(st), 128, 256), make_sdesc(smem_u32(st + a_bytes), 128, 256), idesc,
-               j > 0 ? 1u : 0u);
-      umma_commit(&bars[s]);
+      int x0, y0, z0;
+      tile_origin(a, t, x0, y0, z0);
+      const int ox = x0 + (m % TX), oy = y0 + m / TX;
+      for (int i = 0; i < a.zg; ++i)
+      for (int c0 = 0; c0 < a.cout; c0 += 16) {
+        const bool valid = ox < a.W && oy < a.H && z0 + i < a.D;
+        const long long v = ((long long)(z0 + i) * a.H + oy) * a.W + ox;
+        float f[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * qtr) << 16) + (uint32_t)((ab * a.zg + i) * a.cout + c0), f);
+        if (valid) {
+          __nv_bfloat16 out[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            float r = f[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+            if (a.relu) r = fmaxf(r, 0.f);
+            if (a.mask && !(__bfloat162float(a.mask[v * a.mstride + c0 + i]) > 0.f)) r = 0.f;
+            out[i] = __float2bfloat16_rn(r);
+          }
+          __nv_bfloat16* dst = a.y + v * a.ystride + a.yoff + c0;
+          *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<uint4*>(&out[0]);
+          *reinterpret_cast<uint4*>(dst + 8) = *reinterpret_cast<uint4*>(&out[8]);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&aempty[ab]);
     }
   }
-  if (tid == 0) umma_commit(&bars[CSTAGES]);
-  if (nsteps > 0 && !mbar_wait(&bars[CSTAGES], 0)) ok = false;
-  tc_fence_after();
   if (!ok) atomicOr(&fail_s, 1);
+  tc_fence_before();
   __syncthreads();
-  if (!fail_s && nsteps > 0) {
-    // rows 0..M-1 live in TMEM lanes 0..M-1; warps 0..M/32-1 read them
-    if (32 * warp < M) {
-      const int row = 32 * warp + lane;
-      for (int c0 = 0; c0 < N; c0 += 16) {
-        float f[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, f);
-        if (row < a.cout)
-          for (int i = 0; i < 16; ++i) atomicAdd(&a.dw[((long long)t * a.cout + row) * a.cin + c0 + i], f[i]);
-      }
+  tc_fence_after();
+  if (tid == 0 && fail_s) atomicOr(a.err, 1);
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+}
+
+// ---- weight gradient: halo tiles, MN-major operands, fixed-order partials --
+//
+// dW[t][co][ci] = sum_v dY[v][co] * X[v + off_t][ci]: per tap a GEMM with
+// M = co (padded to 128 rows), N = ci and K = voxels. Both operands are read
+// in the NDHWC layout as MN-major UMMA matrices (a 16-byte row holds 8
+// channels of one voxel; eight K rows are eight voxels): the dY tile as
+// [co/8][128 voxels][8] (row groups SBO = 2048 B apart, K groups LBO = 128 B),
+// the X halo as in the forward kernel, [ci/8][z][y][x][8] (SBO = 16 * HVOX,
+// and the K groups of the tile's voxel order, one y row of 8 voxels each, are
+// LBO = 16 * HX apart), shifted per tap by the same byte offsets. A CTA takes
+// a group of TG taps (TG * cin TMEM columns of accumulators) and a fixed
+// share of the tiles, accumulates over them in TMEM, and writes its partial
+// sums to its own slice of a scratch array; k_wgrad_reduce then adds the
+// slices in a fixed order, so dW is the same bits on every run.
+struct WgArgs {
+  const __nv_bfloat16* x;   // [D][H][W][cin]
+  const __nv_bfloat16* dy;  // [D][H][W][cout]
+  float* part;              // [nsplit][27][cout][cin]
+  int D, H, W, cin, cout;
+  int kc, nchunk, tg, ntg, nsplit, hvox;
+  int ntx, nty;
+  long long ntiles;
+  uint32_t tmem_cols;
+  int* err;
+};
+
+constexpr int WG_ABYTES = 128 * 128 * 2;  // dY tile: 128 voxels x 128 (padded) channels
+
+__global__ void __launch_bounds__(FT, 1) k_conv3_wgrad_tile(WgArgs a) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t sfull[2], sempty[2], fin;
+  __shared__ uint32_t tmem_s;
+  __shared__ int fail_s;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int HVOX = a.hvox;
+  const uint32_t halo_bytes = (uint32_t)HVOX * a.kc * 2, stage_bytes = WG_ABYTES + halo_bytes;
+  const int tg0 = (blockIdx.x % a.ntg) * a.tg;                 // first tap of this CTA's group
+  const int ntap = min(a.tg, 27 - tg0);
+  const int split = blockIdx.x / a.ntg;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_s)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&sfull[i], NLOAD);
+      mbar_init(&sempty[i], 1);
     }
-  } else if (fail_s && tid == 0) {
-    atomicOr(a.err, 1);
+    mbar_init(&fin, 1);
+    fail_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+  tc_fence_after();
+  const uint32_t tmem = tmem_s;
+  bool ok = true;
+  if (warp < 4) {
+    // loads: the dY tile (all channels, zero above cout and outside the box)
+    // and the X halo of one channel chunk, per stage
+    const int cg8 = a.kc >> 3;
+    long long j = 0;
+    for (long long t = split; t < a.ntiles && ok; t += a.nsplit) {
+      const int x0 = (int)(t % a.ntx) * TX, y0 = (int)((t / a.ntx) % a.nty) * TY;
+      const int z0 = (int)(t / ((long long)a.ntx * a.nty));
+      for (int c = 0; c < a.nchunk; ++c, ++j) {
+        const int sb = (int)(j & 1);
+        const long long r = j >> 1;
+        if (r >= 1 && !mbar_wait(&sempty[sb], (uint32_t)((r - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        const uint32_t sa = smem_u32(sm + (size_t)sb * stage_bytes), sh = sa + WG_ABYTES;
+        for (int p = tid; p < 16 * 128; p += NLOAD) {
+          const int cog = p >> 7, m = p & 127;
+          const int gx = x0 + (m % TX), gy = y0 + m / TX;
+          const bool in = gx < a.W && gy < a.H && 8 * cog < a.cout;
+          const __nv_bfloat16* src = in ? a.dy + (((long long)z0 * a.H + gy) * a.W + gx) * a.cout + 8 * cog : a.dy;
+          cp_async16(sa + (uint32_t)(cog * 128 + m) * 16u, src, in ? 16 : 0);
+        }
+        for (int p = tid; p < HVOX * cg8; p += NLOAD) {
+          const int cg = p % cg8, v = p / cg8;
+          const int gx = x0 - 1 + v % HX, gy = y0 - 1 + (v / HX) % HY, gz = z0 - 1 + v / (HX * HY);
+          const bool in = gx >= 0 && gx < a.W && gy >= 0 && gy < a.H && gz >= 0 && gz < a.D;
+          const __nv_bfloat16* src =
+              in ? a.x + (((long long)gz * a.H + gy) * a.W + gx) * a.cin + c * a.kc + cg * 8 : a.x;
+          cp_async16(sh + (uint32_t)(cg * HVOX + v) * 16u, src, in ? 16 : 0);
+        }
+        cp_async_wait_all();
+        fence_async_smem();
+        mbar_arrive(&sfull[sb]);
+      }
+    }
+  } else if (warp == 4) {
+    if (lane == 0) {
+      // M = 128 (co), N = kc (ci of the chunk), both operands MN-major
+      const uint32_t idesc = make_idesc(128, a.kc) | (1u << 15) | (1u << 16);
+      long long j = 0;
+      bool first = true;
+      for (long long t = split; t < a.ntiles && ok; t += a.nsplit) {
+        for (int c = 0; c < a.nchunk && ok; ++c, ++j) {
+          const int sb = (int)(j & 1);
+          if (!mbar_wait(&sfull[sb], (uint32_t)((j >> 1) & 1))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(sm + (size_t)sb * stage_bytes), sh = sa + WG_ABYTES;
+          const uint64_t ad0 = make_sdesc(sa, 128u, 2048u);
+          const uint64_t bd0 = make_sdesc(sh, (uint32_t)HX * 16u, (uint32_t)HVOX * 16u);
+          for (int i = 0; i < ntap; ++i) {
+            const int tap = tg0 + i;
+            const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+            const uint64_t bt = bd0 + (uint64_t)(dx + HX * (dy + HY * dz));
+            const uint32_t dcol = tmem + (uint32_t)(i * a.cin + c * a.kc);
+            // K = 128 voxels of the tile in 8 steps of two y rows
+            for (int k = 0; k < 8; ++k)
+              umma_f16(dcol, ad0 + (uint64_t)(16 * k), bt + (uint64_t)(2 * k * HX), idesc,
+                       (first && k == 0) ? 0u : 1u);
+          }
+          umma_commit(&sempty[sb]);
+          // the first MMA of every accumulator column block overwrites it
+          if (c == a.nchunk - 1) first = false;
+        }
+      }
+      umma_commit(&fin);
+      if (!mbar_wait(&fin, 0)) ok = false;
+    }
+  } else if (warp >= 6) {
+    // wait for the last MMA (fin is committed after it), then write the
+    // partial sums of rows co < cout
+    const int qtr = warp & 3;
+    const int co = 32 * qtr + lane;
+    if (!mbar_wait(&fin, 0)) ok = false;
+    tc_fence_after();
+    const bool any = split < a.ntiles;
+    for (int i = 0; i < ntap && ok; ++i)
+      for (int c0 = 0; c0 < a.cin; c0 += 16) {
+        float f[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * qtr) << 16) + (uint32_t)(i * a.cin + c0), f);
+        if (co < a.cout) {
+          float* dst = a.part + (((size_t)split * 27 + tg0 + i) * a.cout + co) * a.cin + c0;
+#pragma unroll
+          for (int q = 0; q < 16; ++q) dst[q] = any ? f[q] : 0.f;
+        }
+      }
+  }
+  if (!ok) atomicOr(&fail_s, 1);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (tid == 0 && fail_s) atomicOr(a.err, 1);
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+}
+
+// dw[i] = sum over the splits of part[s][i], in split order.
+__global__ void k_wgrad_reduce(const float* __restrict__ part, float* __restrict__ dw, size_t n, int nsplit) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int s = 0; s < nsplit; ++s) acc += part[(size_t)s * n + i];
+    dw[i] = acc;
+  }
+}
+
+// Work split of the weight gradient: taps per CTA group (their accumulators
+// fill at most 512 TMEM columns), tap groups, and tile splits per group.
+void wgrad_plan(int cin, int nsm, int* tg, int* ntg, int* nsplit) {
+  *tg = std::min(27, 512 / cin);
+  *ntg = (27 + *tg - 1) / *tg;
+  *nsplit = std::max(1, (nsm + *ntg - 1) / *ntg);
 }
 
 }  // namespace
@@ -355,40 +545,137 @@ int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, con
     set_error("wg_conv3_fwd: bad arguments (cin, cout multiples of 16, cout <= 256, 16-byte aligned rows)");
     return WG_EINVAL;
   }
-  ConvArgs a{(const __nv_bfloat16*)x, (const __nv_bfloat16*)w, bias, (__nv_bfloat16*)y,
-             (const __nv_bfloat16*)mask, D, H, W, cin, cout, ystride, yoff, mstride, relu, err};
-  const long long nvox = (long long)D * H * W;
-  const int smem = CSTAGES * (CM * 32 + cout * 32);
-  static bool attr = false;
-  if (!attr) {
-    WG_TRY_CUDA(cudaFuncSetAttribute(k_conv3_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-    attr = true;
+  if (((uintptr_t)x | (uintptr_t)w | (uintptr_t)y) & 15) {
+    set_error("wg_conv3_fwd: x, w and y must be 16-byte aligned");
+    return WG_EINVAL;
   }
-  k_conv3_mma<<<(unsigned)((nvox + CM - 1) / CM), CNT, smem, (cudaStream_t)stream>>>(a);
+  // dynamic shared memory: the opt-in limit less the kernel's static part
+  int dev = 0, nsm = 0, optin = 0;
+  WG_TRY_CUDA(cudaGetDevice(&dev));
+  WG_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  WG_TRY_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  WG_TRY_CUDA(cudaFuncGetAttributes(&fa, k_conv3_tile));
+  const int smem_max = std::min(kConvSmem, optin - (int)fa.sharedSizeBytes);
+  FwdArgs a{};
+  a.x = (const __nv_bfloat16*)x;
+  a.w = (const __nv_bfloat16*)w;
+  a.bias = bias;
+  a.y = (__nv_bfloat16*)y;
+  a.mask = (const __nv_bfloat16*)mask;
+  a.D = D;
+  a.H = H;
+  a.W = W;
+  a.cin = cin;
+  a.cout = cout;
+  a.ystride = ystride;
+  a.yoff = yoff;
+  a.mstride = mstride;
+  a.relu = relu;
+  a.err = err;
+  // channels per halo chunk: the largest of 64, 48, 32, 16 that divides cin
+  a.kc = cin % 64 == 0 ? 64 : cin % 48 == 0 ? 48 : cin % 32 == 0 ? 32 : 16;
+  a.nchunk = cin / a.kc;
+  // z planes per work item: each weight block then feeds zg accumulators
+  // (2 * zg * cout TMEM columns, double-buffered). Take the largest zg <= 4
+  // whose two halo stages leave room for at least four weight stages; zg = 1
+  // with the fewest stages that fit otherwise.
+  const int w_bytes = cout * a.kc * 2;
+  a.zg = 0;
+  for (int zg = 4; zg >= 1 && !a.zg; --zg) {
+    const int hb = HX * HY * (zg + 2) * a.kc * 2;
+    if (2 * zg * cout <= 512 && 2 * hb + 4 * w_bytes <= smem_max && zg <= D) a.zg = zg;
+  }
+  if (!a.zg) a.zg = 1;
+  a.hvox = HX * HY * (a.zg + 2);
+  const int halo_bytes = a.hvox * a.kc * 2;
+  a.hs = 2;
+  while (a.hs < MAXHS && (a.hs + 1) * halo_bytes + 4 * w_bytes <= smem_max / 2) ++a.hs;
+  a.ws = std::min(MAXWS, (smem_max - a.hs * halo_bytes) / w_bytes);
+  if (a.ws < 2) {
+    set_error("wg_conv3_fwd: cout too large for the shared-memory stages");
+    return WG_EINVAL;
+  }
+  uint32_t cols = 32;
+  while ((int)cols < 2 * a.zg * cout) cols <<= 1;
+  a.tmem_cols = cols;
+  a.ntx = (W + TX - 1) / TX;
+  a.nty = (H + TY - 1) / TY;
+  a.ntz = (D + a.zg - 1) / a.zg;
+  a.ntiles = (long long)a.ntx * a.nty * a.ntz;
+  const int smem = a.hs * halo_bytes + a.ws * w_bytes;
+  WG_TRY_CUDA(cudaFuncSetAttribute(k_conv3_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const long long grid = std::min<long long>(a.ntiles, nsm);
+  k_conv3_tile<<<(unsigned)grid, FT, smem, (cudaStream_t)stream>>>(a);
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }
 
-int wg_conv3_wgrad(const void* xT, const void* dyT, int D, int H, int W, int cin, int cout, float* dw, int* err,
-                   void* stream) {
-  if (!xT || !dyT || !dw || !err || D < 1 || H < 1 || W < 1 || cin < 16 || cin % 16 || cin > 256 || cout < 1 ||
-      cout > 128) {
-    set_error("wg_conv3_wgrad: bad arguments (cin multiple of 16 up to 256, cout <= 128)");
+int wg_conv3_wgrad_scratch(int cin, int cout, int64_t* nfloats) {
+  if (!nfloats || cin < 16 || cin % 16 || cin > 256 || cout < 16 || cout % 16 || cout > 128) {
+    set_error("wg_conv3_wgrad_scratch: bad arguments (cin multiple of 16 up to 256, cout multiple of 16 up to 128)");
     return WG_EINVAL;
   }
-  // M = 128 keeps accumulator row m in TMEM lane m (output channels padded with zeros)
-  const int mpad = 128;
-  const long long nvox = (long long)D * H * W;
-  const long long chunk = 4096;
-  WgradArgs a{(const __nv_bfloat16*)xT, (const __nv_bfloat16*)dyT, dw, D, H, W, cin, cout, mpad, chunk, err};
-  const int smem = CSTAGES * (mpad * 32 + cin * 32);
-  static bool attr = false;
-  if (!attr) {
-    WG_TRY_CUDA(cudaFuncSetAttribute(k_conv3_wgrad_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-    attr = true;
+  int dev = 0, nsm = 0, tg, ntg, nsplit;
+  WG_TRY_CUDA(cudaGetDevice(&dev));
+  WG_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  wgrad_plan(cin, nsm, &tg, &ntg, &nsplit);
+  *nfloats = (int64_t)nsplit * 27 * cout * cin;
+  return WG_OK;
+}
+
+int wg_conv3_wgrad(const void* x, const void* dy, int D, int H, int W, int cin, int cout, float* dw, float* scratch,
+                   int64_t scratch_floats, int* err, void* stream) {
+  if (!x || !dy || !dw || !scratch || !err || D < 1 || H < 1 || W < 1 || cin < 16 || cin % 16 || cin > 256 ||
+      cout < 16 || cout % 16 || cout > 128) {
+    set_error("wg_conv3_wgrad: bad arguments (cin multiple of 16 up to 256, cout multiple of 16 up to 128)");
+    return WG_EINVAL;
   }
-  dim3 grid((unsigned)((nvox + chunk - 1) / chunk), 27);
-  k_conv3_wgrad_mma<<<grid, CNT, smem, (cudaStream_t)stream>>>(a);
+  if (((uintptr_t)x | (uintptr_t)dy) & 15) {
+    set_error("wg_conv3_wgrad: x and dy must be 16-byte aligned");
+    return WG_EINVAL;
+  }
+  int dev = 0, nsm = 0, optin = 0;
+  WG_TRY_CUDA(cudaGetDevice(&dev));
+  WG_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  WG_TRY_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  WgArgs a{};
+  a.x = (const __nv_bfloat16*)x;
+  a.dy = (const __nv_bfloat16*)dy;
+  a.part = scratch;
+  a.D = D;
+  a.H = H;
+  a.W = W;
+  a.cin = cin;
+  a.cout = cout;
+  a.err = err;
+  a.kc = cin % 64 == 0 ? 64 : cin % 48 == 0 ? 48 : cin % 32 == 0 ? 32 : 16;
+  a.nchunk = cin / a.kc;
+  a.hvox = HX * HY * 3;
+  wgrad_plan(cin, nsm, &a.tg, &a.ntg, &a.nsplit);
+  if (scratch_floats < (int64_t)a.nsplit * 27 * cout * cin) {
+    set_error("wg_conv3_wgrad: scratch smaller than wg_conv3_wgrad_scratch reports");
+    return WG_EINVAL;
+  }
+  uint32_t cols = 32;
+  while ((int)cols < a.tg * cin) cols <<= 1;
+  a.tmem_cols = cols;
+  a.ntx = (W + TX - 1) / TX;
+  a.nty = (H + TY - 1) / TY;
+  a.ntiles = (long long)a.ntx * a.nty * D;
+  const int smem = 2 * (WG_ABYTES + a.hvox * a.kc * 2);
+  cudaFuncAttributes fa{};
+  WG_TRY_CUDA(cudaFuncGetAttributes(&fa, k_conv3_wgrad_tile));
+  if (smem > optin - (int)fa.sharedSizeBytes) {
+    set_error("wg_conv3_wgrad: shared-memory stages do not fit");
+    return WG_EINVAL;
+  }
+  WG_TRY_CUDA(cudaFuncSetAttribute(k_conv3_wgrad_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_conv3_wgrad_tile<<<(unsigned)(a.ntg * a.nsplit), FT, smem, (cudaStream_t)stream>>>(a);
+  WG_TRY_CUDA(cudaGetLastError());
+  const size_t n = (size_t)27 * cout * cin;
+  k_wgrad_reduce<<<(unsigned)std::min<size_t>((n + 255) / 256, 1024), 256, 0, (cudaStream_t)stream>>>(scratch, dw, n,
+                                                                                                     a.nsplit);
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }

@@ -62,6 +62,10 @@ class ESPIC:
         self.pgroup = ParticleGroup(particles, q=echarge, m=proton_mass, w=w, device=device, dtype=particle_dtype)
         self.solver.addpgroup(self.pgroup)
         self.sort_interval = int(sort_interval)
+        # optional learned initial guess (warp_b200.unet.WarmStart): applied
+        # to phi after the deposit, before each solve; the multigrid then
+        # finishes the solve from it
+        self.warmstart = None
         self.it = 0
         # velocities at the positions' time (true after loading and synchv)
         self.vsync = True
@@ -96,6 +100,8 @@ class ESPIC:
                 s.deposit_end(zero_first=True)
             else:
                 s.loadrho()
+            if self.warmstart is not None:
+                self.warmstart.guess(s)
             s.solve()
             self.it += 1
 

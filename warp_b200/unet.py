@@ -45,6 +45,14 @@ def _stream(device):
     return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 
 
+def pack_weights(w):
+    """[27, Cout, Cin] -> [27, Cin/8, Cout, 8]: the layout wg_conv3_fwd reads,
+    in which the weights of one tap and one block of input channels are
+    contiguous."""
+    t, cout, cin = w.shape
+    return w.view(t, cout, cin // 8, 8).permute(0, 2, 1, 3).contiguous()
+
+
 def conv3_fwd(x, w, bias=None, relu=False, out=None, yoff=0, mask=None):
     """x: [D,H,W,Cin] bf16; w: [27,Cout,Cin] bf16; bias fp32 [Cout] or None.
     Writes channels yoff..yoff+Cout-1 of `out` ([D,H,W,Ctot] bf16)."""
@@ -52,6 +60,7 @@ def conv3_fwd(x, w, bias=None, relu=False, out=None, yoff=0, mask=None):
     cout = w.shape[1]
     assert x.dtype == torch.bfloat16 and w.dtype == torch.bfloat16 and x.is_contiguous() and w.is_contiguous()
     assert w.shape == (27, cout, cin)
+    wp = pack_weights(w)
     if out is None:
         out = torch.empty((D, H, W, cout), dtype=torch.bfloat16, device=x.device)
     assert out.is_contiguous() and out.shape[:3] == (D, H, W)
@@ -59,22 +68,36 @@ def conv3_fwd(x, w, bias=None, relu=False, out=None, yoff=0, mask=None):
         assert mask.is_contiguous() and mask.shape[:3] == (D, H, W)
     err = _errbuf(x.device)
     _lib.check(_lib.lib.wg_conv3_fwd(
-        x.data_ptr(), D, H, W, cin, w.data_ptr(), bias.data_ptr() if bias is not None else None, cout,
+        x.data_ptr(), D, H, W, cin, wp.data_ptr(), bias.data_ptr() if bias is not None else None, cout,
         out.data_ptr(), out.shape[3], yoff, mask.data_ptr() if mask is not None else None,
         mask.shape[3] if mask is not None else 0, int(relu), err.data_ptr(), _stream(x.device)))
     return out
 
 
+_SCRATCH = {}
+
+
+def _wgrad_scratch(cin, cout, device):
+    """Partial-sum scratch of wg_conv3_wgrad, kept per (device, cin, cout)."""
+    key = (device, cin, cout)
+    t = _SCRATCH.get(key)
+    if t is None:
+        n = ctypes.c_int64()
+        _lib.check(_lib.lib.wg_conv3_wgrad_scratch(cin, cout, ctypes.byref(n)))
+        t = _SCRATCH[key] = torch.empty(n.value, dtype=torch.float32, device=device)
+    return t
+
+
 def conv3_wgrad(x, dy):
-    """dW[t][co][ci] = sum_v dy[v][co] x[v+off_t][ci] (fp32)."""
+    """dW[t][co][ci] = sum_v dy[v][co] x[v+off_t][ci] (fp32), deterministic."""
     D, H, W, cin = x.shape
     cout = dy.shape[3]
-    xT = x.permute(3, 0, 1, 2).contiguous()
-    dyT = dy.permute(3, 0, 1, 2).contiguous()
-    dw = torch.zeros((27, cout, cin), dtype=torch.float32, device=x.device)
+    assert x.is_contiguous() and dy.is_contiguous()
+    dw = torch.empty((27, cout, cin), dtype=torch.float32, device=x.device)
+    scratch = _wgrad_scratch(cin, cout, x.device)
     err = _errbuf(x.device)
-    _lib.check(_lib.lib.wg_conv3_wgrad(xT.data_ptr(), dyT.data_ptr(), D, H, W, cin, cout, dw.data_ptr(),
-                                       err.data_ptr(), _stream(x.device)))
+    _lib.check(_lib.lib.wg_conv3_wgrad(x.data_ptr(), dy.data_ptr(), D, H, W, cin, cout, dw.data_ptr(),
+                                       scratch.data_ptr(), scratch.numel(), err.data_ptr(), _stream(x.device)))
     return dw
 
 
@@ -168,12 +191,22 @@ class WarmStart:
     # 4x4x4 blocks, then trilinear interpolation back.
     SMOOTH = ("none", "box2", "coarse4")
 
-    def __init__(self, net, out_scale=1.0, smooth="coarse4"):
+    def __init__(self, net, out_scale=1.0, smooth="coarse4", factor=1):
+        """factor 1: the network runs on the solver's grid (nodes 0..n-1 per
+        axis). factor 2: it runs on that grid coarsened twice in each
+        direction -- the inputs are means over 2x2x2 node blocks, and the
+        predicted correction is interpolated back trilinearly (cell-centred,
+        the transfer pair of avg_pool3d and interpolate(align_corners=False))
+        -- so a network trained on 128x128x256 grids serves 256x256x512."""
         if smooth not in self.SMOOTH:
             raise ValueError("smooth must be one of %s" % (self.SMOOTH,))
+        if factor not in (1, 2):
+            raise ValueError("factor must be 1 or 2")
         self.net = net
         self.out_scale = float(out_scale)
         self.smooth = smooth
+        self.factor = factor
+        self._rbuf = None
 
     def lowpass(self, d):
         """d: [D,H,W] float32 prediction -> filtered copy."""
@@ -192,11 +225,20 @@ class WarmStart:
     def _core_phi(phi):
         return phi[1:-2, 1:-2, 1:-2].permute(2, 1, 0)
 
+    def _coarsen(self, u):
+        """[D,H,W] on the solver's nodes -> the network's grid."""
+        if self.factor == 1:
+            return u
+        return torch.nn.functional.avg_pool3d(u[None, None], 2)[0, 0]
+
     def inputs(self, solver):
         """([D,H,W,2] bf16 inputs, s_r) from the solver's rho and phi (phi
-        holds phi^(n-1))."""
-        r = solver.residual_field()[:-1, :-1, :-1].permute(2, 1, 0)
-        p = self._core_phi(solver.phi)
+        holds phi^(n-1)), on the network's grid."""
+        n = (solver.nx + 1) * (solver.ny + 1) * (solver.nz + 1)
+        if self._rbuf is None or self._rbuf.numel() != n or self._rbuf.device != solver.device:
+            self._rbuf = torch.empty(n, dtype=torch.float64, device=solver.device)
+        r = self._coarsen(solver.residual_field(out=self._rbuf)[:-1, :-1, :-1].permute(2, 1, 0))
+        p = self._coarsen(self._core_phi(solver.phi))
         s_r = float(torch.sqrt(torch.mean(r * r)).item()) or 1.0
         s_p = float(torch.sqrt(torch.mean(p * p)).item()) or 1.0
         x = torch.empty(r.shape + (2,), dtype=torch.bfloat16, device=r.device)
@@ -221,6 +263,9 @@ class WarmStart:
         the nodes 0..n-1; the solver's boundary handling sets the rest."""
         x, s_r = self.inputs(solver)
         d = self.lowpass(self.predict(x))
+        if self.factor == 2:
+            d = torch.nn.functional.interpolate(d[None, None], scale_factor=2, mode="trilinear",
+                                                align_corners=False)[0, 0]
         # Dirichlet boundary planes keep their values: the solver never
         # updates them, so a change there would change the problem
         b = solver.bounds
@@ -239,7 +284,10 @@ class WarmStart:
                 "out_scale": self.out_scale, "smooth": self.smooth}
 
     @classmethod
-    def load(cls, state, device="cuda"):
+    def load(cls, state, device="cuda", factor=1):
+        """From state() or from a file written with torch.save(state())."""
+        if isinstance(state, str):
+            state = torch.load(state, map_location="cpu")
         net = UNet3D(device=device)
         net.load_state_dict({k: v.float().to(device) for k, v in state["weights"].items()})
-        return cls(net, out_scale=state["out_scale"], smooth=state.get("smooth", "coarse4"))
+        return cls(net, out_scale=state["out_scale"], smooth=state.get("smooth", "coarse4"), factor=factor)

@@ -56,13 +56,14 @@ def beam_run(workload, rng, gen, device, npart=None, mgtol=1e-8, sort_interval=4
     return run, {"current": current, "emittance": emit, "mismatch": mismatch}
 
 
-def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=4, skip=2, npart=None, log=print):
+def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=8, skip=2, npart=None, log=print):
     """Returns (inputs [n] of [D,H,W,2] bf16, residual scales s_r [n],
-    raw corrections phi^n - phi^(n-1) [n] of [D,H,W] float32, meta)."""
+    scaled corrections (phi^n - phi^(n-1)) / s_r [n] of [D,H,W] bf16, meta).
+    Stored in bf16 on the device: 25 MB a snapshot on the 128x128x256 grid."""
     rng = np.random.default_rng(seed)
     gen = torch.Generator(device=device).manual_seed(seed)
     ws = WarmStart(None)
-    xs, srs, ds, meta = [], [], [], []
+    xs, srs, zs, meta = [], [], [], []
     t0 = time.time()
     while len(xs) < n:
         run, m = beam_run(workload, rng, gen, device, npart)
@@ -74,25 +75,27 @@ def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=4, skip=2, 
                 x, s_r = ws.inputs(s)
                 phi_prev = s.phi.clone()
                 s.solve()
-                ds.append((WarmStart._core_phi(s.phi) - WarmStart._core_phi(phi_prev)).float().contiguous())
+                d = WarmStart._core_phi(s.phi) - WarmStart._core_phi(phi_prev)
+                zs.append((d * (1.0 / s_r)).to(torch.bfloat16).contiguous())
                 xs.append(x)
                 srs.append(s_r)
                 meta.append(dict(m, step=k))
+                del phi_prev, d
             else:
                 s.solve()
         del run
     log("snapshots: %d in %.1f s" % (len(xs), time.time() - t0))
-    return xs, srs, ds, meta
+    return xs, srs, zs, meta
 
 
-def fit_out_scale(srs, ds):
+def fit_out_scale(srs, zs):
     """Median over snapshots of rms(phi^n - phi^(n-1)) / s_r."""
-    r = [float(torch.sqrt(torch.mean(d * d)).item()) / s for d, s in zip(ds, srs)]
-    return float(np.median(r))
+    return float(np.median([float(torch.sqrt(torch.mean(z.float() ** 2)).item()) for z in zs]))
 
 
-def targets(srs, ds, out_scale):
-    return [(d * (1.0 / (s * out_scale))).to(torch.bfloat16).contiguous() for d, s in zip(ds, srs)]
+def targets(srs, zs, out_scale):
+    """Training targets (phi^n - phi^(n-1)) / (s_r * out_scale), bf16."""
+    return [(z.float() * (1.0 / out_scale)).to(torch.bfloat16).contiguous() for z in zs]
 
 
 def _pad16(x2):
@@ -116,7 +119,12 @@ def guess_loss(pred, y, lap_weight):
     return torch.mean(e * e) + lap_weight * torch.mean(laplacian(e) ** 2)
 
 
-def train(xs, ys, epochs=6, lr=2e-3, seed=0, device="cuda", lap_weight=1.0, log=print):
+def train(xs, ys, epochs=6, lr=1e-3, seed=0, device="cuda", lap_weight=1.0, clip=1.0, log=print):
+    """Adam over the snapshots in a seeded order, the gradient norm clipped
+    to `clip` (without it a first large step can silence the ReLUs of a
+    layer, and the network then outputs a constant). The gradients come from
+    the library's kernels, summed in a fixed order, so a training is the same
+    bits on every run."""
     net = UNet3D(seed=seed, device=device)
     opt = torch.optim.Adam(net.parameters(), lr=lr)
     n = len(xs)
@@ -130,6 +138,7 @@ def train(xs, ys, epochs=6, lr=2e-3, seed=0, device="cuda", lap_weight=1.0, log=
             loss = guess_loss(pred, ys[i], lap_weight)
             opt.zero_grad(set_to_none=True)
             loss.backward()
+            torch.nn.utils.clip_grad_norm_(net.parameters(), clip)
             opt.step()
             tot += float(loss.item())
         check_errors(torch.device(device))
@@ -190,6 +199,11 @@ def vcycle_study(ws, workload="D", nbeams=2, steps=6, seed=1000, device="cuda", 
 
 
 def main():
+    """Generates the snapshots, trains, and studies the V-cycles on fresh beams
+    of the training workload (factor 1) and, with --study-b, of the
+    256x256x512 workload with the network on its grid coarsened by two
+    (factor 2). Writes the weights to --out and the results (JSON) to
+    --json."""
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="D")
     ap.add_argument("--snapshots", type=int, default=400)
@@ -201,12 +215,14 @@ def main():
     ap.add_argument("--study-steps", type=int, default=6)
     ap.add_argument("--lap-weight", type=float, default=1.0)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--study-b", action="store_true")
+    ap.add_argument("--json", default=None)
     args = ap.parse_args()
     torch.cuda.set_device(0)
-    xs, srs, ds, meta = snapshots(args.snapshots, workload=args.workload, seed=args.seed, npart=args.npart)
-    out_scale = fit_out_scale(srs, ds)
-    ys = targets(srs, ds, out_scale)
-    del ds
+    xs, srs, zs, meta = snapshots(args.snapshots, workload=args.workload, seed=args.seed, npart=args.npart)
+    out_scale = fit_out_scale(srs, zs)
+    ys = targets(srs, zs, out_scale)
+    del zs
     nval = max(1, len(xs) // 10)
     t0 = time.time()
     net, hist = train(xs[nval:], ys[nval:], epochs=args.epochs, seed=args.seed, lap_weight=args.lap_weight)
@@ -219,11 +235,19 @@ def main():
                                  npart=args.npart, precision=args.precision)
     best = min(study, key=lambda k: study[k]["vcycles_learned"])
     ws = WarmStart(net, out_scale=out_scale, smooth=best)
-    print(json.dumps({"workload": args.workload, "snapshots": len(xs), "heldout": nval, "epochs": args.epochs,
-                      "lap_weight": args.lap_weight,
-                      "out_scale": out_scale, "train_s": train_s, "heldout_mse": mse,
-                      "heldout_mse_zero_guess": mse0, "ratio": mse / mse0, "train": hist, "study": study}))
     torch.save(ws.state(), args.out)
+    res = {"workload": args.workload, "snapshots": len(xs), "heldout": nval, "epochs": args.epochs,
+           "lap_weight": args.lap_weight, "out_scale": out_scale, "train_s": train_s, "heldout_mse": mse,
+           "heldout_mse_zero_guess": mse0, "ratio": mse / mse0, "train": hist, "study": study, "smooth": best}
+    if args.study_b:
+        del xs, ys
+        torch.cuda.empty_cache()
+        wsb = WarmStart(net, out_scale=out_scale, smooth=best, factor=2)
+        res["study_B"] = vcycle_study(wsb, workload="B", nbeams=1, steps=args.study_steps, precision=args.precision)
+    print(json.dumps(res))
+    if args.json:
+        with open(args.json, "w") as f:
+            json.dump(res, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -24,8 +24,10 @@ WORKLOADS = {
     "A": dict(nx=32, ny=32, nz=64, npart=200_000, radius=2e-3, mismatch=0.0, nsteps=50, rods=False),
     "B": dict(nx=256, ny=256, nz=512, npart=50_000_000, radius=4e-3, mismatch=0.2, nsteps=1000, rods=False),
     "E": dict(nx=256, ny=256, nz=1024, npart=200_000_000, radius=4e-3, mismatch=0.2, nsteps=1000, rods=True),
-    # the box of B at half resolution: training grid of the learned warm start
-    "D": dict(nx=128, ny=128, nz=256, npart=4_000_000, radius=4e-3, mismatch=0.2, nsteps=8, rods=False),
+    # the box of B at half resolution: training grid of the learned warm start;
+    # 5e7 particles give the same particles per cell as B's beam seen on this
+    # grid (B restricted by two), where the network is applied
+    "D": dict(nx=128, ny=128, nz=256, npart=50_000_000, radius=4e-3, mismatch=0.2, nsteps=8, rods=False),
 }
 
 COMMON = dict(xmmin=-0.04, xmmax=0.04, ymmin=-0.04, ymmax=0.04, zmmin=0.0, zmmax=1.0, ekin_ev=1.0e6,
