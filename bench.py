@@ -29,11 +29,11 @@ METRIC = "PIC steps/s, 256²×512 grid/5e7 ptcl: plain vs learned+mixed @1e-6 re
 WORKLOAD = "B"
 # particles are re-sorted by cell every SORT_INTERVAL steps (inside the timed steps)
 SORT_INTERVAL = 10
-# DRAM bytes (read + write) per finest-level node of one k_sor_bulk<float>
-# half sweep (bulk nodes and the colour's subgrid points), from an ncu
-# --set full capture of one launch on the 257x257x513-node level:
-# 311.2 MB read + 94.6 MB written
-SOR_F32_TRAFFIC_PER_NODE = (311.19488e6 + 94.622976e6) / (257 * 257 * 513)
+# DRAM bytes (read + write) per finest-level node of one launch, from ncu
+# captures of one launch on the 257x257x513-node level: k_sor_bulk<float>
+# (one half sweep, bulk nodes and the colour's subgrid points): 311.2 MB read
+# + 94.6 MB written.
+TRAFFIC_PER_NODE = {"k_sor_bulk<float>": (311.19488e6 + 94.622976e6) / (257 * 257 * 513)}
 
 
 def parse():
@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--forms", default="plain,mixed")
+    ap.add_argument("--forms", default="plain,mixed,learned")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2,
@@ -126,17 +126,52 @@ class Clocks:
                 "samples": len(rows)}
 
 
+WEIGHTS = os.path.join(ROOT, "warp_b200", "weights", "warmstart_D.pt")
+
+
+class TimedGuess:
+    """The learned guess with CUDA-event timing of every call."""
+
+    def __init__(self, ws):
+        self.ws = ws
+        self.events = []
+
+    def guess(self, solver):
+        import torch
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        self.ws.guess(solver)
+        b.record()
+        self.events.append((a, b))
+
+    def ms(self):
+        import torch
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in self.events]
+
+
 def run_form(name, cfg, beam, steps, warmup, dev, prof):
+    """One form of the step: plain (FP64 throughout), mixed (FP32 V-cycles in
+    FP64 defect correction, FP32 particles and push) or learned (mixed with
+    the learned initial guess before every solve: the U-Net trained on the
+    128x128x256 workload, applied on this grid coarsened by two)."""
     import torch
 
     from warp_b200 import _lib
     from warp_b200.pic import ESPIC
-    precision = {"plain": "fp64", "mixed": "mixed"}[name]
+    precision = {"plain": "fp64", "mixed": "mixed", "learned": "mixed"}[name]
     run = ESPIC(cfg, precision=precision, tolkind="relres", mgtol=1e-6, device=dev, particles=beam,
                 sort_interval=SORT_INTERVAL)
+    timed = None
+    if name == "learned":
+        from warp_b200.unet import WarmStart
+        timed = TimedGuess(WarmStart.load(WEIGHTS, device=dev, factor=2))
     run.generate()
     s = run.solver
+    run.warmstart = timed
     run.step(warmup)
+    if timed is not None:
+        timed.events.clear()
     stream = torch.cuda.current_stream()
     h = s._h
     n0 = _lib.ctypes.c_int64()
@@ -155,13 +190,17 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
     _lib.check(_lib.lib.wg_launch_count(h, _lib.ctypes.byref(n1)))
     out = {"ms_per_step": ms / steps, "vcycles_per_solve": vc / steps, "launches": n1.value - n0.value,
            "live": run.pgroup.nlive(), "relres": s.relres}
+    if timed is not None:
+        g = timed.ms()
+        out["guess_ms"] = sum(g) / len(g)
+        out["weights"] = os.path.relpath(WEIGHTS, ROOT)
     if prof:
         # kernel durations from CUDA events on the launching stream, over the
         # same number of further steps (event timing runs the V-cycles kernel
         # by kernel instead of from the captured graph)
-        kinds = {"sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE, "deposit": _lib.PROF_DEPOSIT,
-                 "resid0": _lib.PROF_RESID0, "restrict0": _lib.PROF_RESTRICT0, "expand0": _lib.PROF_EXPAND0,
-                 "corr": _lib.PROF_CORR, "coarse": _lib.PROF_COARSE}
+        kinds = {"sorpass0": _lib.PROF_SORPASS0, "sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE,
+                 "deposit": _lib.PROF_DEPOSIT, "resid0": _lib.PROF_RESID0, "restrict0": _lib.PROF_RESTRICT0,
+                 "expand0": _lib.PROF_EXPAND0, "corr": _lib.PROF_CORR, "coarse": _lib.PROF_COARSE}
         mask = 0
         for v in kinds.values():
             mask |= 1 << v
@@ -255,9 +294,80 @@ def reference_arm(args, cfg, world):
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def config_c(args, dev):
+    """Config C: the standalone multigrid solve on the 512^3 grid (64 Gaussian
+    blobs, grounded cylinder and 8 spheres at seeded potentials) to a 1e-10
+    relative residual from phi = 0, FP64 and mixed. Reports solve time,
+    V-cycles and the finest-level smoother's HBM GB/s (per-launch CUDA
+    events). One JSON line; `value` is the mixed form's solves/s."""
+    import torch
+
+    from warp_b200 import _lib
+    from warp_b200.constants import eps0
+    from warp_b200.multigrid import MultiGridB200
+    from warp_b200.workloads import CONFIG_C, blobs_rho, config_c_shapes
+    n = CONFIG_C["n"]
+    peak, peak_kind = measured_peaks()
+    forms = {}
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    for prec in ("fp64", "mixed"):
+        s = MultiGridB200(n, n, n, 0., 1., 0., 1., 0., 1., bounds=(0, 0, 0, 0, 0, 0), mgtol=CONFIG_C["mgtol"],
+                          tolkind="relres", mgmaxiters=200, precision=prec, mgverbose=-1, device=dev)
+        for sh in config_c_shapes():
+            s.installconductor(sh)
+        blobs_rho(s, CONFIG_C["nblob"], CONFIG_C["blob_seed"], eps0 * 1e4)
+        s.solve()  # conductor set-up and graph capture
+        ms = []
+        for _ in range(max(args.steps, 1)):
+            s.phi.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            s.solve()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        assert s.converged
+        vc, rr = s.mgiters, s.relres
+        s.phi.zero_()
+        _lib.check(_lib.lib.wg_prof_enable(s._h, (1 << _lib.PROF_SORPASS0) | (1 << _lib.PROF_SOR0)))
+        s.solve()
+        k = {}
+        for name, kind in (("sorpass0", _lib.PROF_SORPASS0), ("sor0", _lib.PROF_SOR0)):
+            t, c, u = _lib.ctypes.c_double(), _lib.ctypes.c_int64(), _lib.ctypes.c_double()
+            _lib.check(_lib.lib.wg_prof_read(s._h, kind, _lib.ctypes.byref(t), _lib.ctypes.byref(c),
+                                             _lib.ctypes.byref(u)))
+            k[name] = (t.value, c.value, u.value)
+        _lib.check(_lib.lib.wg_prof_enable(s._h, 0))
+        t, c, u = k["sorpass0"] if k["sorpass0"][1] else k["sor0"]
+        bpn = (12.0 if prec == "mixed" else 24.0) if k["sorpass0"][1] else (6.0 if prec == "mixed" else 12.0)
+        gbs = bpn * u / (t * 1e-3) / 1e9 if c else None
+        forms[prec] = {"ms_per_solve": sum(ms) / len(ms), "vcycles": vc, "relres": rr,
+                       "smoother": {"kernel": ("k_sor_pass" if k["sorpass0"][1] else "k_sor_bulk") +
+                                    ("<float>" if prec == "mixed" else "<double>"),
+                                    "launches": c, "us_per_launch": 1e3 * t / c if c else None,
+                                    "bytes_per_node_per_launch": bpn, "achieved_gbs": gbs,
+                                    "frac": gbs / peak if gbs else None}}
+        del s
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    return {"metric": "multigrid solve, 512^3 grid, cylinder + 8 spheres, 64 blobs, to 1e-10 relres",
+            "value": 1000.0 / forms["mixed"]["ms_per_solve"], "unit": "solves/s", "n_gpus": 1,
+            "steps": max(args.steps, 1), "higher_is_better": True, "dtype": "f32+f64",
+            "data": "synthetic (seeded Gaussian blobs)", "config": {"workload": "C: 512x512x512 cells"},
+            "forms": forms, "peak": peak, "peak_kind": peak_kind, "clocks": clk}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.workload == "C":
+        import torch
+        torch.cuda.set_device(local)
+        if rank == 0:
+            print(json.dumps(config_c(args, "cuda:%d" % local)))
+        return 0
     from warp_b200.workloads import workload
     cfg = workload(args.workload) if args.npart is None else workload(args.workload, npart=args.npart)
     if args.impl == "reference":
@@ -277,6 +387,10 @@ def main():
     beam = semigaussian(cfg["npart"], seed=cfg["seed"] + rank, radius=cfg["radius"], mismatch=cfg["mismatch"],
                         angle_rms=cfg["angle_rms"], zmin=cfg["zmmin"], zmax=cfg["zmmax"], ekin_ev=cfg["ekin_ev"])
     forms = [f for f in args.forms.split(",") if f]
+    skipped = {}
+    if "learned" in forms and not os.path.exists(WEIGHTS):
+        forms.remove("learned")
+        skipped["learned"] = "no trained weights at %s" % os.path.relpath(WEIGHTS, ROOT)
     headline = forms[-1]
     results = {}
     clocks = None
@@ -302,32 +416,46 @@ def main():
     e2e_ms = max_over_ranks(e2e_ms, world, dev)
     peak, peak_kind = measured_peaks()
     kern = results[headline]["kernels"]
-    sor = kern["sor0"]
-    # algorithmic bytes of one red or black half sweep of the finest level
-    # (one profiled unit per node): read phi of every node, read rhs and
-    # write phi of the half being updated = 16 B/node FP64, 8 B/node FP32
-    bytes_per_node = 8.0 if headline == "mixed" else 16.0
-    sor_kernel = "k_sor_bulk<%s> (finest level, one red or black half sweep)" % (
-        "float" if headline == "mixed" else "double")
+    fp32 = headline != "plain"
+    # The dominant level-0 smoother launch and its algorithmic bytes per node
+    # (the per-sweep counts of the hot-path table: a full red+black sweep moves
+    # 24 B/node in FP64, 12 B/node in FP32; a half sweep half of that).
+    if kern["sorpass0"]["launches"]:
+        sor = kern["sorpass0"]
+        bytes_per_node = 12.0 if fp32 else 24.0
+        sor_kernel = "k_sor_pass<%s> (finest level, one red+black pass)" % ("float" if fp32 else "double")
+    else:
+        sor = kern["sor0"]
+        bytes_per_node = 6.0 if fp32 else 12.0
+        sor_kernel = "k_sor_bulk<%s> (finest level, one red or black half sweep)" % ("float" if fp32 else "double")
     achieved = None
     if sor["launches"]:
         per_launch_bytes = bytes_per_node * sor["units"] / sor["launches"]
         achieved = per_launch_bytes / (sor["ms"] / sor["launches"] * 1e-3) / 1e9
+    tpn = TRAFFIC_PER_NODE.get(sor_kernel.split(" ")[0])
     roofline = {"bound": "hbm", "kernel": sor_kernel, "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                 "peak_kind": peak_kind,
-                "traffic": (SOR_F32_TRAFFIC_PER_NODE * sor["units"] / sor["launches"]
-                            if headline == "mixed" and sor["launches"] else None),
+                "traffic": (tpn * sor["units"] / sor["launches"] if tpn and sor["launches"] else None),
                 "bytes_per_node_per_launch": bytes_per_node}
+    ratios = {}
+    if "plain" in results:
+        p = results["plain"]
+        for f in ("mixed", "learned"):
+            if f in results:
+                ratios["steps_per_s_%s_over_plain" % f] = p["ms_per_step"] / results[f]["ms_per_step"]
+                ratios["vcycles_plain_over_%s" % f] = p["vcycles_per_solve"] / results[f]["vcycles_per_solve"]
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if headline == "plain" else "f32+f64",
             "data": "synthetic (seeded semi-Gaussian beam)",
             "config": job_config(cfg, world), "form": headline,
-            "forms": results, "gpu_launches": results[headline]["launches"],
+            "forms": results, "ratios": ratios, "gpu_launches": results[headline]["launches"],
             "e2e": {"value": 1000.0 / e2e_ms * world, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": roofline, "clocks": clk}
+    if skipped:
+        line["skipped_forms"] = skipped
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.cpu_steps > 0:
         # the oracle continues the GPU run from its current particles and
         # phi for a few full steps (a bounded sample of the same workload)

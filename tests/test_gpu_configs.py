@@ -15,8 +15,6 @@ the smaller sizes in the other test files.
   +-20 kV. Checks: the rods hold their voltage exactly, the solve converges,
   and charge is conserved.
 """
-import math
-
 import numpy as np
 import pytest
 import torch
@@ -25,24 +23,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _blobs_rho(solver, nblob, seed, eps0):
-    """Sum of seeded Gaussian blobs (sigma 2-20 cells, amplitude U[-1,1])
-    written into solver.rho on the device, from separable 1-D factors."""
-    rng = np.random.default_rng(seed)
-    dev = solver.device
-    x = torch.linspace(solver.xmmin, solver.xmmax, solver.nx + 1, device=dev, dtype=torch.float64)
-    y = torch.linspace(solver.ymmin, solver.ymmax, solver.ny + 1, device=dev, dtype=torch.float64)
-    z = torch.linspace(solver.zmmin, solver.zmmax, solver.nz + 1, device=dev, dtype=torch.float64)
-    rho = torch.zeros((solver.nx + 1, solver.ny + 1, solver.nz + 1), dtype=torch.float64, device=dev)
-    for _ in range(nblob):
-        c = [rng.uniform(lo + 0.2 * (hi - lo), hi - 0.2 * (hi - lo)) for lo, hi in
-             ((solver.xmmin, solver.xmmax), (solver.ymmin, solver.ymmax), (solver.zmmin, solver.zmmax))]
-        sig = rng.uniform(2, 20) * solver.dx
-        amp = rng.uniform(-1, 1)
-        gx = torch.exp(-(x - c[0]) ** 2 / (2 * sig * sig))
-        gy = torch.exp(-(y - c[1]) ** 2 / (2 * sig * sig))
-        gz = torch.exp(-(z - c[2]) ** 2 / (2 * sig * sig))
-        rho += amp * gx[:, None, None] * gy[None, :, None] * gz[None, None, :]
-    solver.rho.copy_(rho * (eps0 * 1e4))
+    from warp_b200.workloads import blobs_rho
+    blobs_rho(solver, nblob, seed, eps0 * 1e4)
 
 
 def _interior_check(solver):
@@ -56,17 +38,11 @@ def _interior_check(solver):
 
 
 def test_config_C_512cubed_fp64_and_mixed():
-    from warp_b200 import conductors as C
     from warp_b200.constants import eps0
     from warp_b200.multigrid import MultiGridB200
     torch.cuda.set_device(0)
-    rng = np.random.default_rng(2024)
-    shapes = [C.ZCylinderOut(radius=0.45, length=10.0, voltage=0.0, xcent=0.5, ycent=0.5, zcent=0.5)]
-    for _ in range(8):
-        r = rng.uniform(0.03, 0.06)
-        ang, rad = rng.uniform(0, 2 * math.pi), rng.uniform(0, 0.3)
-        shapes.append(C.Sphere(radius=r, voltage=rng.uniform(-1, 1), xcent=0.5 + rad * math.cos(ang),
-                               ycent=0.5 + rad * math.sin(ang), zcent=rng.uniform(0.2, 0.8)))
+    from warp_b200.workloads import config_c_shapes
+    shapes = config_c_shapes()
     phis, iters = {}, {}
     for prec in ("fp64", "mixed"):
         s = MultiGridB200(512, 512, 512, 0., 1., 0., 1., 0., 1., bounds=(0, 0, 0, 0, 0, 0), mgtol=1e-10,

@@ -181,6 +181,8 @@ class ESPIC:
             self.vsync = False
             if it + 1 < nsteps:
                 upload()
+            if self.warmstart is not None:
+                self.warmstart.guess(s)
             s.solve()
             self.it += 1
         main.wait_stream(d2h)

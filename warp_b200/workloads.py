@@ -83,3 +83,48 @@ def beam_weight(current, length, n, ekin_ev=1e6, mass=proton_mass, charge=echarg
     gamma = 1. + ekin_ev * echarge / (mass * clight * clight)
     v = math.sqrt(1. - 1. / (gamma * gamma)) * clight
     return current * length / (charge * v * n)
+
+
+# Config C: the standalone multigrid solve on a 512^3 grid over the unit
+# cube, Dirichlet on every face; rho a sum of 64 seeded Gaussian blobs (sigma
+# 2-20 cells, amplitudes uniform in [-1, 1]); conductors a grounded cylinder
+# and 8 spheres at seeded potentials in [-1, 1] V; solved to a 1e-10 relative
+# residual.
+CONFIG_C = dict(n=512, nblob=64, blob_seed=7, shape_seed=2024, mgtol=1e-10)
+
+
+def config_c_shapes(seed=CONFIG_C["shape_seed"]):
+    """The grounded cylinder and 8 spheres of config C (conductors module
+    shapes, unit cube)."""
+    from . import conductors as C
+    rng = np.random.default_rng(seed)
+    shapes = [C.ZCylinderOut(radius=0.45, length=10.0, voltage=0.0, xcent=0.5, ycent=0.5, zcent=0.5)]
+    for _ in range(8):
+        r = rng.uniform(0.03, 0.06)
+        ang, rad = rng.uniform(0, 2 * math.pi), rng.uniform(0, 0.3)
+        shapes.append(C.Sphere(radius=r, voltage=rng.uniform(-1, 1), xcent=0.5 + rad * math.cos(ang),
+                               ycent=0.5 + rad * math.sin(ang), zcent=rng.uniform(0.2, 0.8)))
+    return shapes
+
+
+def blobs_rho(solver, nblob, seed, scale):
+    """Sum of seeded Gaussian blobs (sigma 2-20 cells, amplitude U[-1,1])
+    times `scale`, written into solver.rho on its device from separable 1-D
+    factors."""
+    import torch
+    rng = np.random.default_rng(seed)
+    dev = solver.device
+    x = torch.linspace(solver.xmmin, solver.xmmax, solver.nx + 1, device=dev, dtype=torch.float64)
+    y = torch.linspace(solver.ymmin, solver.ymmax, solver.ny + 1, device=dev, dtype=torch.float64)
+    z = torch.linspace(solver.zmmin, solver.zmmax, solver.nz + 1, device=dev, dtype=torch.float64)
+    rho = torch.zeros((solver.nx + 1, solver.ny + 1, solver.nz + 1), dtype=torch.float64, device=dev)
+    for _ in range(nblob):
+        c = [rng.uniform(lo + 0.2 * (hi - lo), hi - 0.2 * (hi - lo)) for lo, hi in
+             ((solver.xmmin, solver.xmmax), (solver.ymmin, solver.ymmax), (solver.zmmin, solver.zmmax))]
+        sig = rng.uniform(2, 20) * solver.dx
+        amp = rng.uniform(-1, 1)
+        gx = torch.exp(-(x - c[0]) ** 2 / (2 * sig * sig))
+        gy = torch.exp(-(y - c[1]) ** 2 / (2 * sig * sig))
+        gz = torch.exp(-(z - c[2]) ** 2 / (2 * sig * sig))
+        rho += amp * gx[:, None, None] * gy[None, :, None] * gz[None, None, :]
+    solver.rho.copy_(rho * scale)
