@@ -68,3 +68,12 @@ def test_misuse_raises():
         fs.unregistersolver()
     with pytest.raises(NotImplementedError):
         fs.FieldSolver().solve()
+
+
+def test_lprecalccoeffs_is_refused_clearly():
+    """A deck that sets lprecalccoeffs gets NotImplementedError with the
+    reason, before any device work."""
+    import pytest
+    from warp_b200.multigrid import MultiGridB200
+    with pytest.raises(NotImplementedError, match="lprecalccoeffs"):
+        MultiGridB200(8, 8, 8, 0., 1., 0., 1., 0., 1., lprecalccoeffs=True)

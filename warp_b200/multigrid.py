@@ -48,7 +48,12 @@ class MultiGridB200(FieldSolver):
     def __init__(self, nx, ny, nz, xmmin, xmmax, ymmin, ymmax, zmmin, zmmax, bounds=(0, 0, 0, 0, 0, 0),
                  mgparam=1.2, mgtol=1.e-6, mgmaxiters=100, mgmaxlevels=101, downpasses=1, uppasses=1,
                  lcndbndy=True, icndbndy=2, mgform=1, mgverbose=0, precision="fp64", tolkind="mgerror",
-                 device=None, use_graphs=True, use_pdl=True, use_fused_pass=True):
+                 device=None, use_graphs=True, use_pdl=True, use_fused_pass=True, lprecalccoeffs=False):
+        if lprecalccoeffs:
+            raise NotImplementedError(
+                "MultiGridB200: lprecalccoeffs (precalculatecoefficients3d, f3d_mgrid.F:4330) is not supported; "
+                "its 9 stored coefficients per node would multiply the HBM traffic of every sweep, so the "
+                "coefficients are formed on the fly (the reference's default, lprecalccoeffs = false)")
         if icndbndy != 2:
             raise ValueError("MultiGridB200 supports icndbndy = 2 (quadratic subgrid stencil) only")
         if mgform != 1:

@@ -85,11 +85,15 @@ class ParticleGroup:
         keys = torch.empty(n, dtype=torch.int64, device=self.device)
         s = self.cstruct()
         _lib.check(self.fn("wg_particle_keys")(solver._h, ctypes.byref(s), ctypes.c_void_p(keys.data_ptr())))
+        sentinel = (solver.nx + 1) * (solver.ny + 1) * (solver.nz + 1)
+        if sentinel < 2 ** 31:
+            # 32-bit keys: half the radix passes of the 64-bit sort
+            keys = keys.to(torch.int32)
         perm = torch.argsort(keys, stable=True)
         nlive = n
         if compact:
-            sentinel = (solver.nx + 1) * (solver.ny + 1) * (solver.nz + 1)
-            nlive = int(torch.searchsorted(keys[perm], torch.tensor([sentinel], device=self.device)).item())
+            nlive = int(torch.searchsorted(keys[perm], torch.tensor([sentinel], device=self.device,
+                                                                     dtype=keys.dtype)).item())
         new = {f: torch.empty(nlive, dtype=self.dtype, device=self.device) for f in FIELDS}
         d = _lib.ParticlesF32() if self.fp32 else _lib.Particles()
         for f in FIELDS:
