@@ -407,6 +407,7 @@ def main():
             clk = clocks.stop()
             head_run = run
         else:
+            run.close()
             del run
             torch.cuda.empty_cache()
         results[f] = res

@@ -70,6 +70,16 @@ class ESPIC:
         # velocities at the positions' time (true after loading and synchv)
         self.vsync = True
 
+    def close(self):
+        """Unregisters the run's solver and drops its particles, so that the
+        device memory of both is freed once the run object goes (the
+        registry of registered solvers would keep them alive)."""
+        from .fieldsolver import getregisteredsolvers, unregistersolver
+        if self.solver in getregisteredsolvers():
+            unregistersolver(self.solver)
+        self.solver.pgroups = []
+        self.warmstart = None
+
     def generate(self):
         """Initial deposit and field solve (w3dgen -> step3d("w3dgen"))."""
         if self.sort_interval > 0:

@@ -83,6 +83,7 @@ def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=8, skip=2, 
                 del phi_prev, d
             else:
                 s.solve()
+        run.close()
         del run
     log("snapshots: %d in %.1f s" % (len(xs), time.time() - t0))
     return xs, srs, zs, meta
@@ -189,6 +190,7 @@ def vcycle_study(ws, workload="D", nbeams=2, steps=6, seed=1000, device="cuda", 
             s.solve()
             rows.append({"step": k, "vc_plain": n_plain, "vc_learned": s.mgiters, "relres_start_plain": r_plain,
                          "relres_start_learned": r_learned, "guess_ms": e0.elapsed_time(e1)})
+        run.close()
         del run
     vp = float(np.mean([r["vc_plain"] for r in rows]))
     vl = float(np.mean([r["vc_learned"] for r in rows]))
