@@ -198,7 +198,7 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
         # kernel durations from CUDA events on the launching stream, over the
         # same number of further steps (event timing runs the V-cycles kernel
         # by kernel instead of from the captured graph)
-        kinds = {"sorpass0": _lib.PROF_SORPASS0, "sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE,
+        kinds = {"sor0": _lib.PROF_SOR0, "advance": _lib.PROF_ADVANCE,
                  "deposit": _lib.PROF_DEPOSIT, "resid0": _lib.PROF_RESID0, "restrict0": _lib.PROF_RESTRICT0,
                  "expand0": _lib.PROF_EXPAND0, "corr": _lib.PROF_CORR, "coarse": _lib.PROF_COARSE}
         mask = 0
@@ -331,21 +331,18 @@ def config_c(args, dev):
         assert s.converged
         vc, rr = s.mgiters, s.relres
         s.phi.zero_()
-        _lib.check(_lib.lib.wg_prof_enable(s._h, (1 << _lib.PROF_SORPASS0) | (1 << _lib.PROF_SOR0)))
+        _lib.check(_lib.lib.wg_prof_enable(s._h, 1 << _lib.PROF_SOR0))
         s.solve()
-        k = {}
-        for name, kind in (("sorpass0", _lib.PROF_SORPASS0), ("sor0", _lib.PROF_SOR0)):
-            t, c, u = _lib.ctypes.c_double(), _lib.ctypes.c_int64(), _lib.ctypes.c_double()
-            _lib.check(_lib.lib.wg_prof_read(s._h, kind, _lib.ctypes.byref(t), _lib.ctypes.byref(c),
-                                             _lib.ctypes.byref(u)))
-            k[name] = (t.value, c.value, u.value)
+        t, c, u = _lib.ctypes.c_double(), _lib.ctypes.c_int64(), _lib.ctypes.c_double()
+        _lib.check(_lib.lib.wg_prof_read(s._h, _lib.PROF_SOR0, _lib.ctypes.byref(t), _lib.ctypes.byref(c),
+                                         _lib.ctypes.byref(u)))
         _lib.check(_lib.lib.wg_prof_enable(s._h, 0))
-        t, c, u = k["sorpass0"] if k["sorpass0"][1] else k["sor0"]
-        bpn = (12.0 if prec == "mixed" else 24.0) if k["sorpass0"][1] else (6.0 if prec == "mixed" else 12.0)
+        t, c, u = t.value, c.value, u.value
+        bpn = 6.0 if prec == "mixed" else 12.0
         gbs = bpn * u / (t * 1e-3) / 1e9 if c else None
         forms[prec] = {"ms_per_solve": sum(ms) / len(ms), "vcycles": vc, "relres": rr,
-                       "smoother": {"kernel": ("k_sor_pass" if k["sorpass0"][1] else "k_sor_bulk") +
-                                    ("<float>" if prec == "mixed" else "<double>"),
+                       "smoother": {"kernel": "k_sor_bulk" + ("<float>" if prec == "mixed" else "<double>") +
+                                    " (finest level, one red or black half sweep)",
                                     "launches": c, "us_per_launch": 1e3 * t / c if c else None,
                                     "bytes_per_node_per_launch": bpn, "achieved_gbs": gbs,
                                     "frac": gbs / peak if gbs else None}}
@@ -418,17 +415,13 @@ def main():
     peak, peak_kind = measured_peaks()
     kern = results[headline]["kernels"]
     fp32 = headline != "plain"
-    # The dominant level-0 smoother launch and its algorithmic bytes per node
-    # (the per-sweep counts of the hot-path table: a full red+black sweep moves
-    # 24 B/node in FP64, 12 B/node in FP32; a half sweep half of that).
-    if kern["sorpass0"]["launches"]:
-        sor = kern["sorpass0"]
-        bytes_per_node = 12.0 if fp32 else 24.0
-        sor_kernel = "k_sor_pass<%s> (finest level, one red+black pass)" % ("float" if fp32 else "double")
-    else:
-        sor = kern["sor0"]
-        bytes_per_node = 6.0 if fp32 else 12.0
-        sor_kernel = "k_sor_bulk<%s> (finest level, one red or black half sweep)" % ("float" if fp32 else "double")
+    # The dominant level-0 smoother launch, one red or black half sweep, and
+    # its algorithmic bytes per node: the hot-path table counts 24 B/node for
+    # a full red+black sweep in FP64 and 12 B/node in FP32, so a half sweep
+    # moves 12 and 6.
+    sor = kern["sor0"]
+    bytes_per_node = 6.0 if fp32 else 12.0
+    sor_kernel = "k_sor_bulk<%s> (finest level, one red or black half sweep)" % ("float" if fp32 else "double")
     achieved = None
     if sor["launches"]:
         per_launch_bytes = bytes_per_node * sor["units"] / sor["launches"]

@@ -66,11 +66,6 @@ typedef struct {
 #define WG_SOLVE_PDL 4    /* launch the solver's kernels with programmatic
                              dependent launch (each launch overlaps the end of
                              the previous kernel; same results) */
-#define WG_SOLVE_INPLACE 8 /* SOR passes as two in-place half sweeps on every
-                             level; without it a level whose half sweep is one
-                             launch (Dirichlet x and y, Dirichlet or periodic z,
-                             no Neumann-type subgrid points) takes each pass as
-                             one out-of-place launch (same results) */
 
 typedef struct {
   int mgiters;      /* V-cycles done */
@@ -302,7 +297,6 @@ int wg_particle_permute_f32(wg_ctx* ctx, const int64_t* perm, const wg_particles
 #define WG_PROF_EXPAND0 5   /* prolongation into the finest level (units: fine nodes) */
 #define WG_PROF_CORR 6      /* FP64 correction update of the mixed form (units: nodes) */
 #define WG_PROF_COARSE 7    /* all work below the finest level in one V-cycle (units: level-1 nodes) */
-#define WG_PROF_SORPASS0 8  /* one out-of-place SOR pass (red and black) on the finest level (units: nodes) */
 
 /* Starts CUDA-event timing of the kernel kinds in `mask` (bits 1<<WG_PROF_*),
  * clearing earlier records; mask 0 stops it. */

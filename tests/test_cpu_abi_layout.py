@@ -26,8 +26,7 @@ CONSTANTS = {
     "WG_CENTER_FULLV": "CENTER_FULLV", "WG_CENTER_HALFV": "CENTER_HALFV", "WG_CENTER_SYNCHV": "CENTER_SYNCHV",
     "WG_PROF_SOR0": "PROF_SOR0", "WG_PROF_DEPOSIT": "PROF_DEPOSIT", "WG_PROF_ADVANCE": "PROF_ADVANCE",
     "WG_PROF_RESID0": "PROF_RESID0", "WG_PROF_RESTRICT0": "PROF_RESTRICT0", "WG_PROF_EXPAND0": "PROF_EXPAND0",
-    "WG_PROF_CORR": "PROF_CORR", "WG_PROF_COARSE": "PROF_COARSE", "WG_PROF_SORPASS0": "PROF_SORPASS0",
-    "WG_SOLVE_INPLACE": "SOLVE_INPLACE",
+    "WG_PROF_CORR": "PROF_CORR", "WG_PROF_COARSE": "PROF_COARSE",
 }
 ERRORS = ["WG_EINVAL", "WG_ECUDA", "WG_ESTATE", "WG_EOVERFLOW", "WG_ENODEV", "WG_ENOMEM", "WG_ETOOLARGE"]
 

@@ -218,27 +218,3 @@ def test_gpu_setconductorvoltage_matches_oracle():
     assert np.array_equal(gphi, ophi)
     with pytest.raises(NotImplementedError):
         s.setconductorvoltage([0.0] * (s.nz + 1), condid=shapes[1].condid)
-
-
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("bounds", [(0, 0, 0, 0, 2, 2), (0, 0, 0, 0, 0, 0)])
-def test_gpu_fused_pass_equals_inplace_half_sweeps(precision, bounds):
-    """Each SOR pass as one out-of-place launch (k_sor_pass, the default)
-    gives the same bits and V-cycle counts as two in-place half sweeps, with
-    conductors (subgrid points of both colours, interior nodes), for periodic
-    and Dirichlet z."""
-    s, shapes, rho = _conductor_case()
-    out = []
-    for fused in (False, True):
-        sv = H.make_solver(s.nx, s.ny, s.nz, (s.xmmin, s.ymmin, s.zmmin), (s.xmmax, s.ymmax, s.zmmax), bounds,
-                           mgtol=1e-9, tolkind="relres", precision=precision, use_fused_pass=fused)
-        for sh in shapes:
-            sv.installconductor(sh)
-        sv.rho = rho
-        sv.solve()
-        n1 = sv.mgiters
-        sv.rho = rho * 1.01
-        sv.solve()  # warm start, graph replay
-        out.append((sv.phi.cpu().numpy(), n1, sv.mgiters))
-    assert out[0][1:] == out[1][1:]
-    assert np.array_equal(out[0][0], out[1][0])

@@ -36,7 +36,7 @@ class SolveOpts(ctypes.Structure):
                 ("flags", ctypes.c_int), ("mgmaxvcycles", ctypes.c_int)]
 
 
-SOLVE_GRAPH, SOLVE_PDL, SOLVE_INPLACE = 1, 4, 8
+SOLVE_GRAPH, SOLVE_PDL = 1, 4
 
 
 class SolveStats(ctypes.Structure):
@@ -120,7 +120,7 @@ SIGNATURES = {
 }
 
 PROF_SOR0, PROF_DEPOSIT, PROF_ADVANCE, PROF_RESID0, PROF_RESTRICT0, PROF_EXPAND0, PROF_CORR = 0, 1, 2, 3, 4, 5, 6
-PROF_COARSE, PROF_SORPASS0 = 7, 8
+PROF_COARSE = 7
 
 
 def _load():

@@ -196,8 +196,6 @@ void free_all(wg_ctx* c) {
   c->prof_ev.clear();
   for (Level& L : c->lv) {
     dfree(L.phi);
-    dfree(L.phi2);
-    dfree(L.phif2);
     dfree(L.rhs);
     dfree(L.res);
     dfree(L.phif);
@@ -283,7 +281,6 @@ int ensure_fp32_impl(wg_ctx* c) {
   c->cond_version += 1;
   for (Level& L : c->lv) {
     WG_TRY(dalloc(&L.phif, L.np));
-    WG_TRY(dalloc(&L.phif2, L.np));
     WG_TRY(dalloc(&L.rhsf, L.nr));
     WG_TRY(dalloc(&L.resf, L.np));
     for (DevSubgrid& S : L.sub)
@@ -341,7 +338,6 @@ int wg_create(const wg_grid* grid, wg_ctx** out) {
     L.np = (size_t)(L.d.nx + 3) * (L.d.ny + 3) * (L.d.nz + 3);
     L.nr = (size_t)(L.d.nx + 1) * (L.d.ny + 1) * (L.d.nz + 1);
     rc = dalloc(&L.phi, L.np);
-    if (rc == WG_OK) rc = dalloc(&L.phi2, L.np);
     if (rc == WG_OK) rc = dalloc(&L.rhs, L.nr);
     if (rc == WG_OK && l + 1 < dims.size()) rc = dalloc(&L.res, L.np);
     if (rc == WG_OK && l + 1 < dims.size()) rc = expand_tables(L, dims[l + 1]);

@@ -70,10 +70,6 @@ struct Level {
   double* phi = nullptr;
   double* rhs = nullptr;
   double* res = nullptr;
-  // second phi buffers of the out-of-place SOR pass (k_sor_pass); a V-cycle
-  // leaves phi in the first one
-  double* phi2 = nullptr;
-  float* phif2 = nullptr;
   float* phif = nullptr;
   float* rhsf = nullptr;
   float* resf = nullptr;

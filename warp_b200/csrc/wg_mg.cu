@@ -458,101 +458,6 @@ __global__ void __launch_bounds__(256) k_sor_bulk(T* __restrict__ phi, const T* 
                r[k] + (xm[k] + xp[k]) * cx + (ym[k] + yp[k]) * cy + (zm[k] + zp[k]) * cz + spm1 * c[k]);
 }
 
-// sorpass3d's two half sweeps (f3d_mgrid.F:1949-2093, 2229-2243) as one
-// out-of-place pass, pin -> pout, for a level where k_sor_bulk does the whole
-// half sweep (merged_ok). A block takes a PTX x PTY x PTZ tile of the padded
-// node box and stages the old phi of the tile and a 2-node halo in shared
-// memory. It forms the red half sweep on the tile and a 1-node halo (the red
-// values its black nodes read), then the black half sweep on the tile, and
-// writes every node of the tile: updated nodes their new value, the others
-// (faces, guards, conductor interior nodes) their old one. Each update uses
-// the operands and the expression of the in-place half sweeps -- red from old
-// black, black from new red -- so the result is the same bits. With periodic
-// z (even nz), a node on plane nz or a guard plane is computed as its source
-// plane (z taken mod nz), which writes the periodic images. Subgrid points
-// (NaN-boxed rhs) take condbndymg's formula with their old value as prevphi;
-// interior conductor nodes keep their value. ZERO: pin is all zeros (the
-// first pass of a correction solve); nothing of it is read.
-// One pass moves phi in, rhs in and phi out once (12 B/node in FP32), where
-// two in-place half sweeps move each of them twice.
-// Tile z extent: 8 planes for FP32, 4 for FP64 (static shared memory below
-// 48 KB: 34 KB and 44 KB).
-constexpr int PTX = 32, PTY = 8;
-template <typename T>
-struct PassTZ {
-  static constexpr int value = sizeof(T) == 4 ? 8 : 4;
-};
-constexpr int PPX = PTX + 4, PPY = PTY + 4, PQX = PTX + 2, PQY = PTY + 2;
-
-template <typename T, bool ZERO>
-__global__ void __launch_bounds__(256) k_sor_pass(const T* __restrict__ pin, T* __restrict__ pout,
-                                                  const T* __restrict__ rhs, int nx, int ny, int nz, int ixmin,
-                                                  int ixmax, int iymin, int iymax, int izmin, int izmax, int zper,
-                                                  T cx, T cy, T cz, T spm1, CondArgs<T> C, SorCoef sc, int voltfac_on,
-                                                  int lcndbndy) {
-  constexpr int PTZ = PassTZ<T>::value, PPZ = PTZ + 4, PQZ = PTZ + 2;
-  pdl_entry();
-  __shared__ T P[PPZ * PPY * PPX];
-  __shared__ T Q[PQZ * PQY * PQX];
-  const int tid = (int)(threadIdx.y * blockDim.x + threadIdx.x), nt = (int)(blockDim.x * blockDim.y);
-  const int x0 = -1 + (int)blockIdx.x * PTX, y0 = -1 + (int)blockIdx.y * PTY, z0 = -1 + (int)blockIdx.z * PTZ;
-  const int sy = nx + 3, sz = sy * (ny + 3), ry = nx + 1, rz = ry * (ny + 1);
-  auto zsrc = [&](int z) { return zper ? ((z % nz) + nz) % nz : z; };
-  auto inrange = [&](int x, int y, int z) {
-    return x >= ixmin && x <= ixmax && y >= iymin && y <= iymax && z >= izmin && z <= izmax;
-  };
-  // old phi of the tile and a 2-node halo (clamped into the padded box,
-  // where a clamped value is never an operand of an update)
-  for (int i = tid; i < PPZ * PPY * PPX; i += nt) {
-    if (ZERO) {
-      P[i] = (T)0;
-      continue;
-    }
-    const int lx = i % PPX, ly = (i / PPX) % PPY, lz = i / (PPX * PPY);
-    const int gx = min(max(x0 - 2 + lx, -1), nx + 1), gy = min(max(y0 - 2 + ly, -1), ny + 1);
-    const int gz = zper ? zsrc(z0 - 2 + lz) : min(max(z0 - 2 + lz, -1), nz + 1);
-    P[i] = pin[(gx + 1) + sy * (gy + 1) + sz * (gz + 1)];
-  }
-  __syncthreads();
-  // red half sweep on the tile and a 1-node halo
-  for (int i = tid; i < PQZ * PQY * PQX; i += nt) {
-    const int lx = i % PQX, ly = (i / PQX) % PQY, lz = i / (PQX * PQY);
-    const int gx = x0 - 1 + lx, gy = y0 - 1 + ly, gs = zsrc(z0 - 1 + lz);
-    const int pc = (lx + 1) + PPX * ((ly + 1) + PPY * (lz + 1));
-    T v = P[pc];
-    if (((gx + gy + gs) & 1) == 0 && inrange(gx, gy, gs)) {
-      const T r = rhs[gx + ry * gy + rz * gs];
-      const T xm = P[pc - 1], xp = P[pc + 1], ym = P[pc - PPX], yp = P[pc + PPX], zm = P[pc - PPX * PPY],
-              zp = P[pc + PPX * PPY];
-      if (!isbox(r))
-        v = r + (xm + xp) * cx + (ym + yp) * cy + (zm + zp) * cz + spm1 * v;
-      else if (!Box<T>::interior(r))
-        v = subgrid_value<T>(C, 0, (int)Box<T>::idx(r), xm, xp, ym, yp, zm, zp, v, sc, voltfac_on, lcndbndy);
-    }
-    Q[i] = v;
-  }
-  __syncthreads();
-  // black half sweep on the tile; every node of the tile is written
-  for (int i = tid; i < PTZ * PTY * PTX; i += nt) {
-    const int lx = i % PTX, ly = (i / PTX) % PTY, lz = i / (PTX * PTY);
-    const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-    if (gx > nx + 1 || gy > ny + 1 || gz > nz + 1) continue;
-    const int gs = zsrc(gz);
-    const int qc = (lx + 1) + PQX * ((ly + 1) + PQY * (lz + 1));
-    T v = Q[qc];
-    if (((gx + gy + gs) & 1) == 1 && inrange(gx, gy, gs)) {
-      const T r = rhs[gx + ry * gy + rz * gs];
-      const T xm = Q[qc - 1], xp = Q[qc + 1], ym = Q[qc - PQX], yp = Q[qc + PQX], zm = Q[qc - PQX * PQY],
-              zp = Q[qc + PQX * PQY];
-      if (!isbox(r))
-        v = r + (xm + xp) * cx + (ym + yp) * cy + (zm + zp) * cz + spm1 * v;
-      else if (!Box<T>::interior(r))
-        v = subgrid_value<T>(C, 1, (int)Box<T>::idx(r), xm, xp, ym, yp, zm, zp, v, sc, voltfac_on, lcndbndy);
-    }
-    pout[(gx + 1) + sy * (gy + 1) + sz * (gz + 1)] = v;
-  }
-}
-
 // The first (red) half sweep of a pass whose phi is all zeros, for a level
 // where k_sor_bulk does the whole half sweep (no Neumann-type subgrid
 // points, Dirichlet x and y, periodic z with an even nz or Dirichlet z). It
@@ -1170,7 +1075,6 @@ struct Arr;
 template <>
 struct Arr<double> {
   static double*& phi(Level& L) { return L.phi; }
-  static double*& alt(Level& L) { return L.phi2; }
   static double* rhs(Level& L) { return L.rhs; }
   static double* res(Level& L) { return L.res; }
   static double* srhs(DevSubgrid& S) { return S.rhs; }
@@ -1178,7 +1082,6 @@ struct Arr<double> {
 template <>
 struct Arr<float> {
   static float*& phi(Level& L) { return L.phif; }
-  static float*& alt(Level& L) { return L.phif2; }
   static float* rhs(Level& L) { return L.rhsf; }
   static float* res(Level& L) { return L.resf; }
   static float* srhs(DevSubgrid& S) { return S.rhsf; }
@@ -1224,9 +1127,6 @@ struct Solver {
   cudaStream_t s;
   bool capturing = false;
   bool pdl = false;  // launch with programmatic dependent launch
-  // levels whose phi currently sits in the second buffer (an odd number of
-  // out-of-place passes so far in this V-cycle)
-  std::vector<char> swapped;
   cudaError_t lerr = cudaSuccess;  // first launch error
 
   // One kernel launch on the solver's stream; with pdl set, the kernel may
@@ -1327,65 +1227,13 @@ struct Solver {
   }
 
   // Whether the first red half sweep of level l can start from an
-  // unzeroed phi and write all of it (k_sor_from_zero, or k_sor_pass from
-  // zero).
+  // unzeroed phi and write all of it (k_sor_from_zero).
   bool from_zero_ok(int l) const { return o->downpasses >= 1 && merged_ok(c->lv[l]); }
-
-  // Whether the passes of level l run out of place as one launch each
-  // (k_sor_pass).
-  bool fused_ok(const Level& L) const { return !(o->flags & WG_SOLVE_INPLACE) && merged_ok(L); }
-
-  // One sorpass3d as one out-of-place launch into the level's second buffer,
-  // which then becomes its phi.
-  template <typename T>
-  void sorpass_fused(int l, bool usev, bool phi_zero) {
-    Level& L = c->lv[l];
-    const SorCoef k = coef(L.d);
-    const bool zero = phi_zero && !usev;
-    const int zper = B.b[4] == 2 ? 1 : 0;
-    // cond_potmg: interior nodes to their voltage (0 below the finest level);
-    // a no-op on a zero phi, which the ZERO form does not read anyway
-    if (L.n_int && !zero)
-      launch(k_interior<T>, cdiv(L.n_int, 128), 128, 0, Arr<T>::phi(L), L.d.nx, L.d.ny, L.int_ijk, L.int_volt,
-             L.n_int, usev, L.d.nz, zper);
-    const Ranges R = ranges(L.d, B.b, true);
-    const int izmax = zper ? std::min(R.izmax, L.d.nz - 1) : R.izmax;
-    CondArgs<T> ca = cond_args<T>(L);
-    dim3 grd(cdiv(L.d.nx + 3, PTX), cdiv(L.d.ny + 3, PTY), cdiv(L.d.nz + 3, PassTZ<T>::value)), blk(32, 8);
-    int pe = zero ? -1 : prof_begin(l, WG_PROF_SORPASS0, (double)L.nr);
-    if (zero)
-      launch(k_sor_pass<T, true>, grd, blk, 0, (const T*)Arr<T>::phi(L), Arr<T>::alt(L), (const T*)Arr<T>::rhs(L),
-             L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, izmax, zper, (T)k.cx, (T)k.cy,
-             (T)k.cz, (T)k.spm1, ca, k, (int)usev, o->lcndbndy);
-    else
-      launch(k_sor_pass<T, false>, grd, blk, 0, (const T*)Arr<T>::phi(L), Arr<T>::alt(L), (const T*)Arr<T>::rhs(L),
-             L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, izmax, zper, (T)k.cx, (T)k.cy,
-             (T)k.cz, (T)k.spm1, ca, k, (int)usev, o->lcndbndy);
-    c->prof_end(pe);
-    std::swap(Arr<T>::phi(L), Arr<T>::alt(L));
-    if ((int)swapped.size() <= l) swapped.resize(l + 1, 0);
-    swapped[l] ^= 1;
-  }
-
-  // Puts level l's phi back into its first buffer after an odd number of
-  // out-of-place passes.
-  template <typename T>
-  void unswap(int l) {
-    if ((int)swapped.size() <= l || !swapped[l]) return;
-    Level& L = c->lv[l];
-    copy(Arr<T>::phi(L), Arr<T>::alt(L), L.np);
-    std::swap(Arr<T>::phi(L), Arr<T>::alt(L));
-    swapped[l] = 0;
-  }
 
   // sorpass3d (f3d_mgrid.F:1949-2093)
   template <typename T>
   void sorpass(int l, bool usev, bool phi_zero = false) {
     Level& L = c->lv[l];
-    if (fused_ok(L)) {
-      sorpass_fused<T>(l, usev, phi_zero);
-      return;
-    }
     const SorCoef k = coef(L.d);
     T* phi = Arr<T>::phi(L);
     const T* rhs = Arr<T>::rhs(L);
@@ -1529,7 +1377,6 @@ struct Solver {
       bc<T>(L, Arr<T>::phi(L), false);
     }
     for (int i = 0; i < o->uppasses; ++i) sorpass<T>(l, usev);
-    unswap<T>(l);
   }
 
   // expand3d (f3d_mgrid.F:1777-1947): adds level l+1's phi, interpolated,
@@ -1658,7 +1505,6 @@ int run_vcycle(Solver& S, bool usev) {
                            ((unsigned long long)o->uppasses << 17) ^ ((unsigned long long)o->lcndbndy << 25) ^
                            ((unsigned long long)usev << 28) ^
                            ((unsigned long long)S.pdl << 29) ^
-                           ((unsigned long long)((o->flags & WG_SOLVE_INPLACE) ? 1 : 0) << 30) ^
                            ((unsigned long long)c->cond_version << 32);
   if (!c->vgraph[gi] || c->vgraph_key[gi] != key) {
     if (c->vgraph[gi]) cudaGraphExecDestroy(c->vgraph[gi]);

@@ -48,7 +48,7 @@ class MultiGridB200(FieldSolver):
     def __init__(self, nx, ny, nz, xmmin, xmmax, ymmin, ymmax, zmmin, zmmax, bounds=(0, 0, 0, 0, 0, 0),
                  mgparam=1.2, mgtol=1.e-6, mgmaxiters=100, mgmaxlevels=101, downpasses=1, uppasses=1,
                  lcndbndy=True, icndbndy=2, mgform=1, mgverbose=0, precision="fp64", tolkind="mgerror",
-                 device=None, use_graphs=True, use_pdl=True, use_fused_pass=True, lprecalccoeffs=False):
+                 device=None, use_graphs=True, use_pdl=True, lprecalccoeffs=False):
         if lprecalccoeffs:
             raise NotImplementedError(
                 "MultiGridB200: lprecalccoeffs (precalculatecoefficients3d, f3d_mgrid.F:4330) is not supported; "
@@ -79,9 +79,6 @@ class MultiGridB200(FieldSolver):
         # replay V-cycles from captured CUDA graphs; programmatic dependent
         # launch of the solver's kernels
         self.use_graphs, self.use_pdl = bool(use_graphs), bool(use_pdl)
-        # each SOR pass (red and black half sweeps) as one out-of-place launch
-        # where the level allows it; False: two in-place half sweeps (same bits)
-        self.use_fused_pass = bool(use_fused_pass)
         self.mgiters, self.mgerror, self.relres, self.converged = 0, 0., -1., True
         self.conductordatalist = []
         self._conductors_installed = False
@@ -297,8 +294,7 @@ class MultiGridB200(FieldSolver):
             _lib.check(_lib.lib.wg_finalize_rho(self._h))
 
     def _opts(self):
-        flags = (_lib.SOLVE_GRAPH if self.use_graphs else 0) | (_lib.SOLVE_PDL if self.use_pdl else 0) | \
-            (0 if self.use_fused_pass else _lib.SOLVE_INPLACE)
+        flags = (_lib.SOLVE_GRAPH if self.use_graphs else 0) | (_lib.SOLVE_PDL if self.use_pdl else 0)
         return _lib.SolveOpts(self.mgparam, self.mgtol, self.mgmaxiters, self.mgmaxlevels, self.downpasses,
                               self.uppasses, int(self.lcndbndy), _PRECISION[self.precision],
                               _TOLKIND[self.tolkind], flags, int(getattr(self, "mgmaxvcycles", 0)))
