@@ -296,7 +296,9 @@ int wg_particle_permute_f32(wg_ctx* ctx, const int64_t* perm, const wg_particles
 #define WG_PROF_RESTRICT0 4 /* restriction from the finest level (units: fine nodes) */
 #define WG_PROF_EXPAND0 5   /* prolongation into the finest level (units: fine nodes) */
 #define WG_PROF_CORR 6      /* FP64 correction update of the mixed form (units: nodes) */
-#define WG_PROF_COARSE 7    /* all work below the finest level in one V-cycle (units: level-1 nodes) */
+#define WG_PROF_COARSE 7    /* all work below the finest level in one V-cycle (units: level-1 nodes);
+                               timed as a replay of its own captured graph with
+                               the solve's PDL setting, as it runs in a V-cycle */
 
 /* Starts CUDA-event timing of the kernel kinds in `mask` (bits 1<<WG_PROF_*),
  * clearing earlier records; mask 0 stops it. */

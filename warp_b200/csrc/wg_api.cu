@@ -184,6 +184,9 @@ void free_graphs(wg_ctx* c) {
     if (c->vgraph[i]) cudaGraphExecDestroy(c->vgraph[i]);
     c->vgraph[i] = nullptr;
     c->vgraph_key[i] = 0ull;
+    if (c->cgraph[i]) cudaGraphExecDestroy(c->cgraph[i]);
+    c->cgraph[i] = nullptr;
+    c->cgraph_key[i] = 0ull;
   }
 }
 

@@ -158,6 +158,10 @@ struct wg_ctx {
   cudaGraphExec_t vgraph[2] = {nullptr, nullptr};
   unsigned long long vgraph_key[2] = {0ull, 0ull};
   long long vgraph_kernels[2] = {0, 0};
+  // the work below level 0 of a V-cycle, captured for WG_PROF_COARSE timing
+  cudaGraphExec_t cgraph[2] = {nullptr, nullptr};
+  unsigned long long cgraph_key[2] = {0ull, 0ull};
+  long long cgraph_kernels[2] = {0, 0};
   long long cond_version = 1;  // bumped whenever device conductor arrays change
   // CUDA-event timing of selected kernel kinds (WG_PROF_* bits)
   int prof_mask = 0;

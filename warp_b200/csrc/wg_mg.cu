@@ -1127,6 +1127,7 @@ struct Solver {
   cudaStream_t s;
   bool capturing = false;
   bool pdl = false;  // launch with programmatic dependent launch
+  bool pdl_timed = false;  // the solve's PDL setting (pdl is off while profiling)
   cudaError_t lerr = cudaSuccess;  // first launch error
 
   // One kernel launch on the solver's stream; with pdl set, the kernel may
@@ -1336,6 +1337,69 @@ struct Solver {
     if (MODE == 0) bc<TO>(L, (TO*)out, false);
   }
 
+  // Everything vcycle(l) does below level l: the conductor marks of level
+  // l+1, its phi zeroed unless the first half sweep writes all of it, and
+  // vcycle(l+1).
+  template <typename T>
+  void coarse_region(int l) {
+    Level& Lc = c->lv[l + 1];
+    box<T>(l + 1);
+    if (!from_zero_ok(l + 1)) zero(Arr<T>::phi(Lc), Lc.np);
+    vcycle<T>(l + 1, false, true);
+  }
+
+  // For WG_PROF_COARSE: the region below level 0 replayed from a captured
+  // graph launched with the solve's PDL setting, so that its CUDA-event time
+  // is the time it takes inside a replayed V-cycle. (Profiling otherwise
+  // launches kernel by kernel, and these small kernels would then wait on
+  // the host's launches.) Recaptured when the options or conductors change.
+  template <typename T>
+  void coarse_from_graph() {
+    const int gi = sizeof(T) == 8 ? 0 : 1;
+    unsigned long long mp;
+    memcpy(&mp, &o->mgparam, sizeof(mp));
+    unsigned long long key = mp;
+    const long long parts[] = {o->mgmaxlevels, o->downpasses, o->uppasses, o->lcndbndy, c->cond_version,
+                               (long long)pdl_timed};
+    for (long long x : parts) key = (key ^ (unsigned long long)x) * 0x100000001B3ull;
+    key |= 1ull;
+    if (!c->cgraph[gi] || c->cgraph_key[gi] != key) {
+      if (c->cgraph[gi]) cudaGraphExecDestroy(c->cgraph[gi]);
+      c->cgraph[gi] = nullptr;
+      cudaError_t e = cudaSuccess;
+      if (!c->cap_stream) e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        if (lerr == cudaSuccess) lerr = e;
+        return;
+      }
+      Solver G = *this;
+      G.s = c->cap_stream;
+      G.capturing = true;
+      G.pdl = pdl_timed;
+      const long long n0 = c->nlaunch;
+      G.coarse_region<T>(0);
+      cudaGraph_t g;
+      e = cudaStreamEndCapture(c->cap_stream, &g);
+      c->cgraph_kernels[gi] = c->nlaunch - n0;
+      c->nlaunch = n0;
+      if (G.lerr != cudaSuccess) e = G.lerr;
+      if (e == cudaSuccess) {
+        e = cudaGraphInstantiate(&c->cgraph[gi], g, 0);
+        cudaGraphDestroy(g);
+      }
+      if (e != cudaSuccess) {
+        c->cgraph[gi] = nullptr;
+        if (lerr == cudaSuccess) lerr = e;
+        return;
+      }
+      c->cgraph_key[gi] = key;
+    }
+    cudaError_t e = cudaGraphLaunch(c->cgraph[gi], s);
+    if (e != cudaSuccess && lerr == cudaSuccess) lerr = e;
+    c->nlaunch += c->cgraph_kernels[gi];
+  }
+
   // vcycle (f3d_mgrid.F:1101-1591)
   template <typename T>
   // phi_zero: phi of level l is all zeros on entry
@@ -1368,10 +1432,11 @@ struct Solver {
                                                          L.rlo, L.rn, L.rw, ff);
       }
       c->prof_end(pr);
-      box<T>(l + 1);
-      if (!from_zero_ok(l + 1)) zero(Arr<T>::phi(Lc), Lc.np);
       int pc = (l == 0) ? prof_begin(0, WG_PROF_COARSE, (double)Lc.nr) : -1;
-      vcycle<T>(l + 1, false, true);
+      if (pc >= 0)
+        coarse_from_graph<T>();
+      else
+        coarse_region<T>(l);
       c->prof_end(pc);
       expand<T>(l);
       bc<T>(L, Arr<T>::phi(L), false);
@@ -1555,7 +1620,8 @@ int solve(wg_ctx* c, const wg_solve_opts* o, wg_solve_stats* st) {
   }
   Solver S{c, o, {}, c->stream, false};
   for (int k = 0; k < 6; ++k) S.B.b[k] = c->grid.bounds[k];
-  S.pdl = (o->flags & WG_SOLVE_PDL) && !c->prof_mask;
+  S.pdl_timed = (o->flags & WG_SOLVE_PDL) != 0;
+  S.pdl = S.pdl_timed && !c->prof_mask;
   cudaStream_t s = c->stream;
   Level& L0 = c->lv[0];
   const LevelDims& d = L0.d;
