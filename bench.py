@@ -129,20 +129,42 @@ class Clocks:
 WEIGHTS = os.path.join(ROOT, "warp_b200", "weights", "warmstart_D.pt")
 
 
+def load_warmstart(dev):
+    """The committed network, trained on the 128x128x256 workload coarsened
+    by train_factor, run on the 256x256x512 (and 256x256x1024) grids
+    coarsened by twice that, so that it sees the cell size it was trained
+    at."""
+    import torch
+
+    from warp_b200.unet import WarmStart
+    st = torch.load(WEIGHTS, map_location="cpu")
+    return WarmStart.load(st, device=dev, factor=2 * int(st.get("train_factor", 1)))
+
+
 class TimedGuess:
     """The learned guess with CUDA-event timing of every call."""
 
     def __init__(self, ws):
         self.ws = ws
         self.events = []
+        self.results = []  # (relres of phi^(n-1), relres of the guess, kept)
 
     def guess(self, solver):
         import torch
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        self.ws.guess(solver)
+        self.results.append(self.ws.guess(solver))
         b.record()
         self.events.append((a, b))
+
+    def summary(self):
+        r = self.results
+        if not r:
+            return {}
+        med = lambda v: sorted(v)[len(v) // 2]
+        return {"guess_kept_fraction": sum(1 for x in r if x[2]) / len(r),
+                "relres_start_plain_median": med([x[0] for x in r]),
+                "relres_start_learned_median": med([x[1] for x in r])}
 
     def ms(self):
         import torch
@@ -164,14 +186,14 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
                 sort_interval=SORT_INTERVAL)
     timed = None
     if name == "learned":
-        from warp_b200.unet import WarmStart
-        timed = TimedGuess(WarmStart.load(WEIGHTS, device=dev, factor=2))
+        timed = TimedGuess(load_warmstart(dev))
     run.generate()
     s = run.solver
     run.warmstart = timed
     run.step(warmup)
     if timed is not None:
         timed.events.clear()
+        timed.results.clear()
     stream = torch.cuda.current_stream()
     h = s._h
     n0 = _lib.ctypes.c_int64()
@@ -193,6 +215,7 @@ def run_form(name, cfg, beam, steps, warmup, dev, prof):
     if timed is not None:
         g = timed.ms()
         out["guess_ms"] = sum(g) / len(g)
+        out.update(timed.summary())
         out["weights"] = os.path.relpath(WEIGHTS, ROOT)
     if prof:
         # kernel durations from CUDA events on the launching stream, over the
@@ -356,6 +379,81 @@ def config_c(args, dev):
             "forms": forms, "peak": peak, "peak_kind": peak_kind, "clocks": clk}
 
 
+def config_e(args, dev):
+    """Config E: the combined run on the 256x256x1024 grid with 2e8 particles,
+    the FODO lattice and four electrostatic quadrupole rods (+-20 kV) inside
+    the grounded pipe. The combined form (learned guess + FP32 multigrid in
+    FP64 defect correction + FP32 push, fixed-point deposit) runs against the
+    plain FP64 form from the same seeded beam for args.steps steps. Every
+    `every` steps both bring their velocities to the positions' time
+    (synchv, the reference's special step) and record the emittances, the
+    live count and the field energy (getese3dfromrhophi). One JSON line:
+    ms/step and V-cycles of each form, the records, and the largest
+    relative differences of the combined form from the plain one."""
+    import torch
+
+    from warp_b200.particles import semigaussian_device
+    from warp_b200.pic import ESPIC
+    from warp_b200.workloads import workload
+    cfg = workload("E")
+    every = max(1, min(50, args.steps))
+    forms, recs = {}, {}
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    for name in ("plain", "combined"):
+        gen = torch.Generator(device=dev).manual_seed(cfg["seed"])
+        beam = semigaussian_device(cfg["npart"], gen, radius=cfg["radius"], mismatch=cfg["mismatch"],
+                                   angle_rms=cfg["angle_rms"], zmin=cfg["zmmin"], zmax=cfg["zmmax"],
+                                   ekin_ev=cfg["ekin_ev"], device=dev)
+        run = ESPIC(cfg, precision="fp64" if name == "plain" else "mixed", tolkind="relres", mgtol=1e-6,
+                    device=dev, particles=beam, sort_interval=SORT_INTERVAL)
+        del beam
+        timed = None
+        if name == "combined" and os.path.exists(WEIGHTS):
+            timed = TimedGuess(load_warmstart(dev))
+            run.warmstart = timed
+        run.generate()
+        rows, ms, vc, nsolve = [], 0.0, 0, 0
+        done = 0
+        while done < args.steps:
+            k = min(every, args.steps - done)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(k):
+                run.step()
+                vc += run.solver.mgiters
+                nsolve += 1
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            done += k
+            run.synchv()
+            m = run.moments()
+            rows.append({"it": run.it, "n": m["n"], "epsx": m["epsx"], "epsy": m["epsy"], "xrms": m["xrms"],
+                         "ese": run.solver.getese()})
+        out = {"ms_per_step": ms / args.steps, "vcycles_per_solve": vc / max(nsolve, 1)}
+        if timed is not None:
+            g = timed.ms()
+            out["guess_ms"] = sum(g) / len(g)
+            out.update(timed.summary())
+        forms[name], recs[name] = out, rows
+        run.close()
+        del run
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    diff = {}
+    for key in ("epsx", "epsy", "xrms", "ese"):
+        d = [abs(c[key] - p[key]) / abs(p[key]) for p, c in zip(recs["plain"], recs["combined"]) if p[key]]
+        diff[key] = {"max_rel": max(d) if d else None, "final_rel": d[-1] if d else None}
+    diff["n"] = {"final_plain": recs["plain"][-1]["n"], "final_combined": recs["combined"][-1]["n"]}
+    return {"metric": "combined form vs plain FP64, 256x256x1024 grid, 2e8 particles, FODO + 4 rods",
+            "value": 1000.0 / forms["combined"]["ms_per_step"], "unit": "steps/s", "n_gpus": 1,
+            "steps": args.steps, "higher_is_better": True, "dtype": "f32+f64",
+            "data": "synthetic (seeded semi-Gaussian beam)", "config": {"workload": "E: 256x256x1024 cells, 2e8 "
+                                                                        "protons, pipe + 4 rods + FODO"},
+            "forms": forms, "records_every": every, "records": recs, "combined_vs_plain": diff, "clocks": clk}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -364,6 +462,12 @@ def main():
         torch.cuda.set_device(local)
         if rank == 0:
             print(json.dumps(config_c(args, "cuda:%d" % local)))
+        return 0
+    if args.workload == "E" and args.impl != "reference":
+        import torch
+        torch.cuda.set_device(local)
+        if rank == 0:
+            print(json.dumps(config_e(args, "cuda:%d" % local)))
         return 0
     from warp_b200.workloads import workload
     cfg = workload(args.workload) if args.npart is None else workload(args.workload, npart=args.npart)

@@ -321,6 +321,13 @@ int wg_launch_count(wg_ctx* ctx, int64_t* n);
  * wait timed out. */
 int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
                  int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream);
+/* wg_conv3_fwd with y in FP32 ([D][H][W][ystride] float, ystride and yoff
+ * multiples of 4): the accumulator, bias, ReLU and mask without the rounding
+ * to bf16. The last layer of the learned guess writes this, so that the
+ * correction added to phi carries no bf16 rounding noise. */
+int wg_conv3_fwd_f32(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout,
+                     float* y, int ystride, int yoff, const void* mask, int mstride, int relu, int* err,
+                     void* stream);
 /* dw[t][co][ci] = sum_v dy[v][co] * x[v+off_t][ci] (fp32; overwritten), from
  * x: [D][H][W][cin] and dy: [D][H][W][cout] bf16 (16-byte aligned), cin a
  * multiple of 16 up to 256, cout a multiple of 16 up to 128. CTAs write

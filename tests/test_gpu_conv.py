@@ -51,6 +51,26 @@ def test_conv3_fwd_offset_and_mask():
     assert np.max(np.abs(got[..., 16:] - ref)) <= 1e-2 * np.max(np.abs(ref)) + 1e-2
 
 
+@pytest.mark.parametrize("dims,cin,cout", [((5, 6, 40), 16, 16), ((3, 5, 7), 48, 128)])
+def test_conv3_fwd_f32_output(dims, cin, cout):
+    """The FP32-output form: within FP32 accumulation error of the FP64
+    oracle (no bf16 rounding), and rounded to bf16 it equals the bf16-output
+    form bit for bit."""
+    from warp_b200 import unet
+    D, H, W = dims
+    x = _rand((D, H, W, cin), 11)
+    w = _rand((27, cout, cin), 12, 0.2)
+    b = torch.randn(cout, generator=torch.Generator().manual_seed(13))
+    yf = unet.conv3_fwd(x.cuda(), w.cuda(), b.cuda(), relu=True, out_dtype=torch.float32)
+    yb = unet.conv3_fwd(x.cuda(), w.cuda(), b.cuda(), relu=True)
+    unet.check_errors(yf.device)
+    assert yf.dtype == torch.float32
+    ref = co.conv3_fwd(x.float().numpy(), w.float().numpy(), b.numpy(), relu=True)
+    got = yf.cpu().numpy()
+    assert np.max(np.abs(got - ref)) <= 1e-5 * np.max(np.abs(ref)) + 1e-5
+    assert torch.equal(yf.to(torch.bfloat16), yb)
+
+
 @pytest.mark.parametrize("cin,cout", [(32, 16), (192, 64), (16, 16), (48, 16), (64, 128), (128, 128), (96, 32)])
 def test_conv3_dgrad_and_wgrad_match_oracle(cin, cout):
     from warp_b200 import unet

@@ -115,6 +115,8 @@ SIGNATURES = {
     "wg_particle_permute_f32": [_vp, _vp, ctypes.POINTER(ParticlesF32), ctypes.POINTER(ParticlesF32)],
     "wg_conv3_fwd": [_vp] + [_c.c_int] * 4 + [_vp, _vp, _c.c_int, _vp, _c.c_int, _c.c_int, _vp, _c.c_int, _c.c_int,
                      _vp, _vp],
+    "wg_conv3_fwd_f32": [_vp] + [_c.c_int] * 4 + [_vp, _vp, _c.c_int, _vp, _c.c_int, _c.c_int, _vp, _c.c_int,
+                         _c.c_int, _vp, _vp],
     "wg_conv3_wgrad": [_vp, _vp] + [_c.c_int] * 5 + [_vp, _vp, _c.c_int64, _vp, _vp],
     "wg_conv3_wgrad_scratch": [_c.c_int, _c.c_int, _i64p],
 }

@@ -229,6 +229,9 @@ void free_all(wg_ctx* c) {
     dfree(c->ef0[s]);
     dfree(c->efd[s]);
   }
+  if (c->enode) cudaFree(c->enode);
+  c->enode = nullptr;
+  c->enode_n = 0;
   if (c->hred) cudaFreeHost(c->hred);
   c->hred = nullptr;
 }

@@ -163,6 +163,9 @@ struct wg_ctx {
   unsigned long long cgraph_key[2] = {0ull, 0ull};
   long long cgraph_kernels[2] = {0, 0};
   long long cond_version = 1;  // bumped whenever device conductor arrays change
+  // node fields of the FP32 push (k_enode), (nx+1)(ny+1)(nz+1) float4
+  float4* enode = nullptr;
+  size_t enode_n = 0;
   // CUDA-event timing of selected kernel kinds (WG_PROF_* bits)
   int prof_mask = 0;
   std::vector<cudaEvent_t> prof_ev;  // start/stop pairs

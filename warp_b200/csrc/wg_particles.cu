@@ -317,6 +317,51 @@ __device__ inline void gather_e(const double* __restrict__ phi, const GridP& g, 
                 u1 * v1 * w1 * (P(i + 1, j + 1, k) - P(i + 1, j + 1, k + 2)));
 }
 
+// The FP32 push's field: E at every node 0..nx x 0..ny x 0..nz from the
+// centred differences of the FP64 phi, rounded to FP32, one float4 a node
+// (x, y, z, unused). gather_e's trilinear sum of node differences is the
+// trilinear sum of these node fields, so the FP32 advance reads 8 vector
+// loads a particle instead of 24 FP64 ones and interpolates in FP32.
+__global__ void k_enode(const double* __restrict__ phi, GridP g, float4* __restrict__ en) {
+  const int nx1 = g.nx + 1, ny1 = g.ny + 1;
+  const int64_t n = (int64_t)nx1 * ny1 * (g.nz + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = (int)(t % nx1), j = (int)((t / nx1) % ny1), k = (int)(t / ((int64_t)nx1 * ny1));
+  const int sy = g.nx + 3, sz = sy * (g.ny + 3);
+  const double* c = phi + ((i + 1) + sy * (j + 1) + (size_t)sz * (k + 1));
+  const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
+  en[t] = make_float4((float)(tdxi * (__ldg(c - 1) - __ldg(c + 1))), (float)(tdyi * (__ldg(c - sy) - __ldg(c + sy))),
+                      (float)(tdzi * (__ldg(c - sz) - __ldg(c + sz))), 0.f);
+}
+
+// gather_e from the node fields of k_enode, in FP32 (the cell and its
+// fractions as gather_e finds them).
+__device__ inline void gather_e_nodes(const float4* __restrict__ en, const GridP& g, double x, double y, double z,
+                                      float& ext, float& eyt, float& ezt) {
+  int i, j, k;
+  double u1d, v1d, w1d;
+  cellfrac((x - g.xmmin) * (1. / g.dx), g.nx, i, u1d);
+  cellfrac((y - g.ymmin) * (1. / g.dy), g.ny, j, v1d);
+  cellfrac((z - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, k, w1d);
+  const float u1 = (float)u1d, v1 = (float)v1d, w1 = (float)w1d;
+  const float u0 = 1.f - u1, v0 = 1.f - v1, w0 = 1.f - w1;
+  const int sy = g.nx + 1, sz = sy * (g.ny + 1);
+  const float4* b = en + (i + sy * j + (size_t)sz * k);
+  const float4 e000 = __ldg(b), e100 = __ldg(b + 1), e010 = __ldg(b + sy), e110 = __ldg(b + sy + 1);
+  const float4 e001 = __ldg(b + sz), e101 = __ldg(b + sz + 1), e011 = __ldg(b + sz + sy), e111 = __ldg(b + sz + sy + 1);
+  const float a000 = u0 * v0 * w0, a100 = u1 * v0 * w0, a010 = u0 * v1 * w0, a110 = u1 * v1 * w0;
+  const float a001 = u0 * v0 * w1, a101 = u1 * v0 * w1, a011 = u0 * v1 * w1, a111 = u1 * v1 * w1;
+  // fused multiply-adds written out (this file is compiled without
+  // contraction for the FP64 paths' sake)
+  ext = __fmaf_rn(a111, e111.x, __fmaf_rn(a011, e011.x, __fmaf_rn(a101, e101.x, __fmaf_rn(a001, e001.x,
+        __fmaf_rn(a110, e110.x, __fmaf_rn(a010, e010.x, __fmaf_rn(a100, e100.x, a000 * e000.x)))))));
+  eyt = __fmaf_rn(a111, e111.y, __fmaf_rn(a011, e011.y, __fmaf_rn(a101, e101.y, __fmaf_rn(a001, e001.y,
+        __fmaf_rn(a110, e110.y, __fmaf_rn(a010, e010.y, __fmaf_rn(a100, e100.y, a000 * e000.y)))))));
+  ezt = __fmaf_rn(a111, e111.z, __fmaf_rn(a011, e011.z, __fmaf_rn(a101, e101.z, __fmaf_rn(a001, e001.z,
+        __fmaf_rn(a110, e110.z, __fmaf_rn(a010, e010.z, __fmaf_rn(a100, e100.z, a000 * e000.z)))))));
+}
+
 // ---- lcorrectede: E next to conductors (sete3dwithconductor) -------------
 
 // Level-0 conductor data read by the corrected gather.
@@ -641,7 +686,8 @@ __device__ inline void block_deposit(bool live, double x, double y, double z, co
 // it from 1.97 to 1.83 ms for 5e7 particles on the B200.
 // T is the particle storage and push arithmetic: double is the reference's
 // arithmetic (bit-identical to the oracle); float is the push of the mixed
-// form, whose E is gathered in FP64 at the FP32 positions and then rounded.
+// form, whose E is interpolated in FP32 from the FP32 node fields of k_enode
+// (with lcorrectede: gathered in FP64 at the FP32 positions and rounded).
 // The push constants (q dt / 2m, the lattice tables, the pipe radius) are
 // formed in FP64 and rounded once.
 // A z bound of the periodic wrap in the particle type: FP64 as given; in FP32
@@ -663,7 +709,8 @@ __device__ __forceinline__ T inner_bound(double v, bool lower) {
 // One particle of k_advance; returns whether it is live after the advance
 // (x, y, z are then its new position).
 template <typename T, int CENTER, bool COND>
-__device__ __forceinline__ bool advance_one(const double* __restrict__ phi, const GridP& g, const PushP& P,
+__device__ __forceinline__ bool advance_one(const double* __restrict__ phi, const float4* __restrict__ en,
+                                            const GridP& g, const PushP& P,
                                             const CondE& ce, T* __restrict__ xp, T* __restrict__ yp,
                                             T* __restrict__ zp, T* __restrict__ uxp, T* __restrict__ uyp,
                                             T* __restrict__ uzp, T* __restrict__ gaminv, int64_t i, T& x, T& y,
@@ -675,7 +722,9 @@ __device__ __forceinline__ bool advance_one(const double* __restrict__ phi, cons
   z = zp[i];
   T ux = uxp[i], uy = uyp[i], uz = uzp[i];
   T ex, ey, ez;
-  {
+  if constexpr (sizeof(T) == 4 && !COND) {
+    gather_e_nodes(en, g, (double)x, (double)y, (double)z, ex, ey, ez);
+  } else {
     double exd, eyd, ezd;
     if (COND) {
       if (!gather_e_cond(phi, g, ce, (double)x, (double)y, (double)z, exd, eyd, ezd)) exd = eyd = ezd = 0.;
@@ -772,7 +821,8 @@ __device__ __forceinline__ bool advance_one(const double* __restrict__ phi, cons
 // DEP: the advanced particles' charge is also added to the fixed-point
 // accumulator acc (block_deposit), as a deposit after the advance would.
 template <typename T, int CENTER, bool COND, bool DEP>
-__global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ phi, GridP g, PushP P, CondE ce,
+__global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ phi, const float4* __restrict__ en,
+                                                    GridP g, PushP P, CondE ce,
                                                  T* __restrict__ xp, T* __restrict__ yp, T* __restrict__ zp,
                                                  T* __restrict__ uxp, T* __restrict__ uyp, T* __restrict__ uzp,
                                                  T* __restrict__ gaminv, int64_t np,
@@ -781,7 +831,7 @@ __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ p
   if constexpr (!DEP) {
     if (i >= np) return;
     T x, y, z;
-    advance_one<T, CENTER, COND>(phi, g, P, ce, xp, yp, zp, uxp, uyp, uzp, gaminv, i, x, y, z);
+    advance_one<T, CENTER, COND>(phi, en, g, P, ce, xp, yp, zp, uxp, uyp, uzp, gaminv, i, x, y, z);
   } else {
     __shared__ AdvBox box;
     __shared__ int bmin[3], bmax[3];
@@ -791,8 +841,8 @@ __global__ void __launch_bounds__(256, 4) k_advance(const double* __restrict__ p
     }
     __syncthreads();
     T x = 0, y = 0, z = 0;
-    const bool live = i < np && advance_one<T, CENTER, COND>(phi, g, P, ce, xp, yp, zp, uxp, uyp, uzp, gaminv, i,
-                                                             x, y, z);
+    const bool live = i < np && advance_one<T, CENTER, COND>(phi, en, g, P, ce, xp, yp, zp, uxp, uyp, uzp, gaminv,
+                                                             i, x, y, z);
     block_deposit(live, (double)x, (double)y, (double)z, g, acc, box, bmin, bmax);
   }
 }
@@ -1266,7 +1316,24 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = 
           prm->use_lattice ? c->czs : nullptr, c->cze, c->cdb, c->nzl, c->zlmin, c->dzl};
   CondE ce{};
   if (c->correctede) WG_TRY(prepare_correctede(c, &ce));
-  using K = void (*)(const double*, GridP, PushP, CondE, T*, T*, T*, T*, T*, T*, T*, int64_t, unsigned long long*);
+  // the FP32 push without lcorrectede gathers from node fields formed from
+  // phi on every call (k_enode)
+  const bool nodes = sizeof(T) == 4 && !c->correctede;
+  const size_t nn = (size_t)(c->grid.nx + 1) * (c->grid.ny + 1) * (c->grid.nz + 1);
+  if (nodes && c->enode_n < nn) {
+    if (c->enode) cudaFree(c->enode);
+    c->enode = nullptr;
+    c->enode_n = 0;
+    cudaError_t e = cudaMalloc((void**)&c->enode, nn * sizeof(float4));
+    if (e != cudaSuccess) {
+      c->enode = nullptr;
+      set_error(std::string("wg_advance: cudaMalloc of the node fields failed: ") + cudaGetErrorString(e));
+      return WG_ENOMEM;
+    }
+    c->enode_n = nn;
+  }
+  using K = void (*)(const double*, const float4*, GridP, PushP, CondE, T*, T*, T*, T*, T*, T*, T*, int64_t,
+                     unsigned long long*);
   // [correctede][deposit][center]
   static const K kerns[2][2][3] = {
       {{k_advance<T, 0, false, false>, k_advance<T, 1, false, false>, k_advance<T, 2, false, false>},
@@ -1274,8 +1341,18 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = 
       {{k_advance<T, 0, true, false>, k_advance<T, 1, true, false>, k_advance<T, 2, true, false>},
        {k_advance<T, 0, true, true>, k_advance<T, 1, true, true>, k_advance<T, 2, true, true>}}};
   const K kern = kerns[c->correctede ? 1 : 0][deposit ? 1 : 0][prm->center];
-  { ++c->nlaunch; int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np); kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), P, ce, p->x, p->y, p->z, p->ux, p->uy,
-                                                  p->uz, p->gaminv, p->np, deposit ? c->racc : nullptr); c->prof_end(pe); }
+  {
+    int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np);
+    if (nodes) {
+      ++c->nlaunch;
+      k_enode<<<cdiv64((int64_t)nn, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), c->enode);
+    }
+    ++c->nlaunch;
+    kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, nodes ? c->enode : nullptr, gridp(c), P, ce, p->x,
+                                                   p->y, p->z, p->ux, p->uy, p->uz, p->gaminv, p->np,
+                                                   deposit ? c->racc : nullptr);
+    c->prof_end(pe);
+  }
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
 }

@@ -136,6 +136,7 @@ struct FwdArgs {
   const __nv_bfloat16* w;     // [27][cin/8][cout][8]
   const float* bias;          // [cout] or null
   __nv_bfloat16* y;           // [D][H][W][ystride], channels yoff..yoff+cout-1 written
+  float* yf;                  // or, when set, the same in FP32 (y unused)
   const __nv_bfloat16* mask;  // optional [D][H][W][mstride]: y *= (mask > 0)
   int D, H, W, cin, cout, ystride, yoff, mstride, relu;
   int kc, nchunk, hs, ws;     // channels per chunk, chunks, halo stages, weight stages
@@ -333,17 +334,25 @@ __global__ void __launch_bounds__(FT, 1) k_conv3_tile(FwdArgs a) {
         float f[16];
         tmem_ld16(tmem + ((uint32_t)(32 * qtr) << 16) + (uint32_t)((ab * a.zg + i) * a.cout + c0), f);
         if (valid) {
-          __nv_bfloat16 out[16];
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             float r = f[i] + (a.bias ? a.bias[c0 + i] : 0.f);
             if (a.relu) r = fmaxf(r, 0.f);
             if (a.mask && !(__bfloat162float(a.mask[v * a.mstride + c0 + i]) > 0.f)) r = 0.f;
-            out[i] = __float2bfloat16_rn(r);
+            f[i] = r;
           }
-          __nv_bfloat16* dst = a.y + v * a.ystride + a.yoff + c0;
-          *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<uint4*>(&out[0]);
-          *reinterpret_cast<uint4*>(dst + 8) = *reinterpret_cast<uint4*>(&out[8]);
+          if (a.yf) {
+            float* dst = a.yf + v * a.ystride + a.yoff + c0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) reinterpret_cast<float4*>(dst)[q] = reinterpret_cast<float4*>(f)[q];
+          } else {
+            __nv_bfloat16 out[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) out[i] = __float2bfloat16_rn(f[i]);
+            __nv_bfloat16* dst = a.y + v * a.ystride + a.yoff + c0;
+            *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<uint4*>(&out[0]);
+            *reinterpret_cast<uint4*>(dst + 8) = *reinterpret_cast<uint4*>(&out[8]);
+          }
         }
       }
       tc_fence_before();
@@ -536,12 +545,14 @@ void wgrad_plan(int cin, int nsm, int* tg, int* ntg, int* nsplit) {
 
 using namespace wg;
 
-extern "C" {
-
-int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
-                 int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream) {
+namespace {
+// wg_conv3_fwd and wg_conv3_fwd_f32: y is bf16 or, with f32, float.
+int conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
+              int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream, bool f32) {
+  // a row of y starts 16-byte aligned: 8 bf16 or 4 float channels
+  const int ya = f32 ? 4 : 8;
   if (!x || !w || !y || !err || D < 1 || H < 1 || W < 1 || cin < 16 || cin % 16 || cout < 16 || cout > 256 ||
-      cout % 16 || ystride < yoff + cout || (yoff % 8) || (ystride % 8) || (mask && mstride < cout)) {
+      cout % 16 || ystride < yoff + cout || (yoff % ya) || (ystride % ya) || (mask && mstride < cout)) {
     set_error("wg_conv3_fwd: bad arguments (cin, cout multiples of 16, cout <= 256, 16-byte aligned rows)");
     return WG_EINVAL;
   }
@@ -561,7 +572,8 @@ int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, con
   a.x = (const __nv_bfloat16*)x;
   a.w = (const __nv_bfloat16*)w;
   a.bias = bias;
-  a.y = (__nv_bfloat16*)y;
+  a.y = f32 ? nullptr : (__nv_bfloat16*)y;
+  a.yf = f32 ? (float*)y : nullptr;
   a.mask = (const __nv_bfloat16*)mask;
   a.D = D;
   a.H = H;
@@ -609,6 +621,21 @@ int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, con
   k_conv3_tile<<<(unsigned)grid, FT, smem, (cudaStream_t)stream>>>(a);
   WG_TRY_CUDA(cudaGetLastError());
   return WG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+
+int wg_conv3_fwd(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout, void* y,
+                 int ystride, int yoff, const void* mask, int mstride, int relu, int* err, void* stream) {
+  return conv3_fwd(x, D, H, W, cin, w, bias, cout, y, ystride, yoff, mask, mstride, relu, err, stream, false);
+}
+
+int wg_conv3_fwd_f32(const void* x, int D, int H, int W, int cin, const void* w, const float* bias, int cout,
+                     float* y, int ystride, int yoff, const void* mask, int mstride, int relu, int* err,
+                     void* stream) {
+  return conv3_fwd(x, D, H, W, cin, w, bias, cout, y, ystride, yoff, mask, mstride, relu, err, stream, true);
 }
 
 int wg_conv3_wgrad_scratch(int cin, int cout, int64_t* nfloats) {

@@ -41,8 +41,10 @@ def beam_params(rng):
     return current, emit, mismatch
 
 
-def beam_run(workload, rng, gen, device, npart=None, mgtol=1e-8, sort_interval=4, precision="fp64"):
-    """A plain FP64 run of one randomized beam, with its initial field solved."""
+def beam_run(workload, rng, gen, device, npart=None, mgtol=1e-6, sort_interval=4, precision="mixed"):
+    """A run of one randomized beam, with its initial field solved (by
+    default as the learned form runs: mixed precision to a 1e-6 relative
+    residual)."""
     current, emit, mismatch = beam_params(rng)
     cfg = pic.workload(workload, current=current, mismatch=mismatch, angle_rms=emit / (2 * 4e-3),
                        seed=int(rng.integers(1 << 30)))
@@ -56,14 +58,21 @@ def beam_run(workload, rng, gen, device, npart=None, mgtol=1e-8, sort_interval=4
     return run, {"current": current, "emittance": emit, "mismatch": mismatch}
 
 
-def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=8, skip=2, npart=None, log=print):
+def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=8, skip=2, npart=None, log=print,
+              factor=1):
     """Returns (inputs [n] of [D,H,W,2] bf16, residual scales s_r [n],
-    scaled corrections (phi^n - phi^(n-1)) / s_r [n] of [D,H,W] bf16, meta).
-    Stored in bf16 on the device: 25 MB a snapshot on the 128x128x256 grid."""
+    masked scaled corrections m (phi^n - phi^(n-1)) / s_r [n] of [D,H,W]
+    bf16, meta, the mask m of the network grid). The runs solve as the
+    learned form does (mixed precision, 1e-6 relative residual), so the
+    inputs are those the network meets in use. factor: the network's grid is
+    the workload's coarsened that many times. Stored in bf16 on the device:
+    25 MB a snapshot on the 128x128x256 grid at factor 1. Every beam of a
+    workload has the same conductors, hence one mask."""
     rng = np.random.default_rng(seed)
     gen = torch.Generator(device=device).manual_seed(seed)
-    ws = WarmStart(None)
+    ws = WarmStart(None, factor=factor)
     xs, srs, zs, meta = [], [], [], []
+    mask = None
     t0 = time.time()
     while len(xs) < n:
         run, m = beam_run(workload, rng, gen, device, npart)
@@ -75,18 +84,19 @@ def snapshots(n, workload="D", seed=0, device="cuda", steps_per_beam=8, skip=2, 
                 x, s_r = ws.inputs(s)
                 phi_prev = s.phi.clone()
                 s.solve()
-                d = WarmStart._core_phi(s.phi) - WarmStart._core_phi(phi_prev)
-                zs.append((d * (1.0 / s_r)).to(torch.bfloat16).contiguous())
+                zs.append(ws.target(s, phi_prev, s_r))
                 xs.append(x)
                 srs.append(s_r)
                 meta.append(dict(m, step=k))
-                del phi_prev, d
+                if mask is None:
+                    mask = ws._net_mask(s).clone()
+                del phi_prev
             else:
                 s.solve()
         run.close()
         del run
     log("snapshots: %d in %.1f s" % (len(xs), time.time() - t0))
-    return xs, srs, zs, meta
+    return xs, srs, zs, meta, mask
 
 
 def fit_out_scale(srs, zs):
@@ -112,15 +122,19 @@ def laplacian(u):
             u[1:-1, 1:-1, 2:] - 6. * c)
 
 
-def guess_loss(pred, y, lap_weight):
+def guess_loss(pred, y, lap_weight, mask=None):
     """MSE of the correction plus lap_weight times the MSE of its Laplacian:
     the multigrid measures a guess by its residual, which the Laplacian of the
-    error dominates, so high-frequency error costs more than its size."""
+    error dominates, so high-frequency error costs more than its size. The
+    prediction counts on the unmasked nodes only (the guess adds nothing
+    elsewhere)."""
+    if mask is not None:
+        pred = pred * mask
     e = pred - y.float()
     return torch.mean(e * e) + lap_weight * torch.mean(laplacian(e) ** 2)
 
 
-def train(xs, ys, epochs=6, lr=1e-3, seed=0, device="cuda", lap_weight=1.0, clip=1.0, log=print):
+def train(xs, ys, epochs=6, lr=1e-3, seed=0, device="cuda", lap_weight=1.0, clip=1.0, log=print, mask=None):
     """Adam over the snapshots in a seeded order, the gradient norm clipped
     to `clip` (without it a first large step can silence the ReLUs of a
     layer, and the network then outputs a constant). The gradients come from
@@ -136,7 +150,7 @@ def train(xs, ys, epochs=6, lr=1e-3, seed=0, device="cuda", lap_weight=1.0, clip
         tot = 0.0
         for i in rng.permutation(n):
             pred = net(_pad16(xs[i]))
-            loss = guess_loss(pred, ys[i], lap_weight)
+            loss = guess_loss(pred, ys[i], lap_weight, mask)
             opt.zero_grad(set_to_none=True)
             loss.backward()
             torch.nn.utils.clip_grad_norm_(net.parameters(), clip)
@@ -151,22 +165,25 @@ def train(xs, ys, epochs=6, lr=1e-3, seed=0, device="cuda", lap_weight=1.0, clip
 
 
 @torch.no_grad()
-def evaluate(net, xs, ys):
+def evaluate(net, xs, ys, mask=None):
     """Held-out MSE of the network and of the zero prediction (the plain
-    warm start phi^(n-1))."""
+    warm start phi^(n-1)), on the unmasked nodes when a mask is given."""
     m, m0 = 0.0, 0.0
     for x2, y in zip(xs, ys):
         p = net(_pad16(x2))
+        if mask is not None:
+            p = p * mask
         m += float(torch.mean((p - y.float()) ** 2))
         m0 += float(torch.mean(y.float() ** 2))
     return m / len(xs), m0 / len(xs)
 
 
 @torch.no_grad()
-def vcycle_study(ws, workload="D", nbeams=2, steps=6, seed=1000, device="cuda", npart=None, precision="fp64",
-                 mgtol=1e-6):
+def vcycle_study(ws, workload="D", nbeams=2, steps=6, seed=1000, device="cuda", npart=None, precision="mixed",
+                 mgtol=1e-6, guard=False):
     """V-cycles to mgtol from the plain warm start and from the learned
-    guess, on the same rho^n, over fresh randomized beams."""
+    guess, on the same rho^n, over fresh randomized beams (guard: the
+    guess is taken back where it is the worse start, WarmStart.guess)."""
     rng = np.random.default_rng(seed)
     gen = torch.Generator(device=device).manual_seed(seed)
     rows = []
@@ -183,7 +200,7 @@ def vcycle_study(ws, workload="D", nbeams=2, steps=6, seed=1000, device="cuda", 
             n_plain = s.mgiters
             s.phi.copy_(phi_prev)
             e0.record()
-            ws.guess(s)
+            ws.guess(s, guard=guard)
             e1.record()
             torch.cuda.synchronize()
             r_learned = s.relresidual()
@@ -202,10 +219,10 @@ def vcycle_study(ws, workload="D", nbeams=2, steps=6, seed=1000, device="cuda", 
 
 def main():
     """Generates the snapshots, trains, and studies the V-cycles on fresh beams
-    of the training workload (factor 1) and, with --study-b, of the
-    256x256x512 workload with the network on its grid coarsened by two
-    (factor 2). Writes the weights to --out and the results (JSON) to
-    --json."""
+    of the training workload (the network on its grid coarsened by
+    --factor) and, with --study-b, of the 256x256x512 workload (coarsened by
+    twice that, the same cell size). Writes the weights to --out and the
+    results (JSON) to --json."""
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="D")
     ap.add_argument("--snapshots", type=int, default=400)
@@ -218,33 +235,39 @@ def main():
     ap.add_argument("--lap-weight", type=float, default=1.0)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--study-b", action="store_true")
+    ap.add_argument("--factor", type=int, default=1, choices=[1, 2, 4],
+                    help="the network's grid is the workload's coarsened this many times")
     ap.add_argument("--json", default=None)
     args = ap.parse_args()
     torch.cuda.set_device(0)
-    xs, srs, zs, meta = snapshots(args.snapshots, workload=args.workload, seed=args.seed, npart=args.npart)
+    xs, srs, zs, meta, mask = snapshots(args.snapshots, workload=args.workload, seed=args.seed, npart=args.npart,
+                                        factor=args.factor)
     out_scale = fit_out_scale(srs, zs)
     ys = targets(srs, zs, out_scale)
     del zs
     nval = max(1, len(xs) // 10)
     t0 = time.time()
-    net, hist = train(xs[nval:], ys[nval:], epochs=args.epochs, seed=args.seed, lap_weight=args.lap_weight)
+    net, hist = train(xs[nval:], ys[nval:], epochs=args.epochs, seed=args.seed, lap_weight=args.lap_weight,
+                      mask=mask)
     train_s = time.time() - t0
-    mse, mse0 = evaluate(net, xs[:nval], ys[:nval])
+    mse, mse0 = evaluate(net, xs[:nval], ys[:nval], mask)
     study = {}
     for sm in WarmStart.SMOOTH:
-        ws = WarmStart(net, out_scale=out_scale, smooth=sm)
+        ws = WarmStart(net, out_scale=out_scale, smooth=sm, factor=args.factor)
         study[sm] = vcycle_study(ws, workload=args.workload, nbeams=args.study_beams, steps=args.study_steps,
                                  npart=args.npart, precision=args.precision)
     best = min(study, key=lambda k: study[k]["vcycles_learned"])
-    ws = WarmStart(net, out_scale=out_scale, smooth=best)
+    ws = WarmStart(net, out_scale=out_scale, smooth=best, factor=args.factor)
+    ws.train_factor = args.factor
     torch.save(ws.state(), args.out)
-    res = {"workload": args.workload, "snapshots": len(xs), "heldout": nval, "epochs": args.epochs,
+    res = {"workload": args.workload, "factor": args.factor, "snapshots": len(xs), "heldout": nval,
+           "epochs": args.epochs,
            "lap_weight": args.lap_weight, "out_scale": out_scale, "train_s": train_s, "heldout_mse": mse,
            "heldout_mse_zero_guess": mse0, "ratio": mse / mse0, "train": hist, "study": study, "smooth": best}
     if args.study_b:
         del xs, ys
         torch.cuda.empty_cache()
-        wsb = WarmStart(net, out_scale=out_scale, smooth=best, factor=2)
+        wsb = WarmStart(net, out_scale=out_scale, smooth=best, factor=2 * args.factor)
         res["study_B"] = vcycle_study(wsb, workload="B", nbeams=1, steps=args.study_steps, precision=args.precision)
     print(json.dumps(res))
     if args.json:
