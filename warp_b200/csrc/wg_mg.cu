@@ -606,11 +606,14 @@ __global__ void k_condbndymgint(T* __restrict__ phi, int nx, int ny, int nz, con
 // The bulk residual for the thread's node column of block (bx, by, bz).
 // keep_sub: leave subgrid-point nodes unwritten (a merged kernel's
 // subgrid blocks write them).
+// wtz (MODE 0, periodic z with Dirichlet x and y): planes 0, 1 and nz-1 are
+// also written to their images nz, nz+1 and -1, which are then not written
+// from their own threads: the boundary copy that would follow is done.
 template <typename T, int MODE, typename TO, int ZPT>
 __device__ __forceinline__ void residual_bulk(const T* __restrict__ phi, const T* __restrict__ rhs,
                                               TO* __restrict__ out, int nx, int ny, int nz, int ixmin, int ixmax,
                                               int iymin, int iymax, int izmin, int izmax, T cx, T cy, T cz, T mgparam,
-                                              int bx, int by, int bz, bool keep_sub, T& m) {
+                                              int bx, int by, int bz, bool keep_sub, T& m, int wtz = 0) {
   // MODE 0 covers the padded array, the others the node array; ZPT planes
   // per thread with all loads issued first; 32-bit offsets
   const int g = (MODE == 0) ? 1 : 0;
@@ -652,7 +655,16 @@ __device__ __forceinline__ void residual_bulk(const T* __restrict__ phi, const T
         continue;
       }
     }
-    if (MODE == 0) out[p0 + k * sz] = (TO)r;
+    if (MODE == 0) {
+      const int iz = iz0 + k;
+      if (wtz && (iz < 0 || iz >= nz)) continue;
+      const int p = p0 + k * sz;
+      out[p] = (TO)r;
+      if (wtz) {
+        if (iz <= 1) out[p + nz * sz] = (TO)r;
+        if (iz == nz - 1) out[p - nz * sz] = (TO)r;
+      }
+    }
     if (MODE == 2) out[q0 + k * rz] = (TO)r;
   }
 }
@@ -661,11 +673,11 @@ template <typename T, int MODE, typename TO, int ZPT>
 __global__ void __launch_bounds__(256, 6) k_residual(const T* __restrict__ phi, const T* __restrict__ rhs,
                                                   TO* __restrict__ out, int nx, int ny, int nz, int ixmin,
                                                   int ixmax, int iymin, int iymax, int izmin, int izmax, T cx, T cy,
-                                                  T cz, T mgparam, unsigned long long* maxout) {
+                                                  T cz, T mgparam, unsigned long long* maxout, int wtz) {
   pdl_entry();
   T m = (T)0.;
   residual_bulk<T, MODE, TO, ZPT>(phi, rhs, out, nx, ny, nz, ixmin, ixmax, iymin, iymax, izmin, izmax, cx, cy, cz,
-                                  mgparam, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, false, m);
+                                  mgparam, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, false, m, wtz);
   if (maxout) block_max_to(maxout, (double)m);
 }
 
@@ -675,10 +687,20 @@ template <typename T, int MODE, typename TO>
 __device__ __forceinline__ double special_res_point(const T* __restrict__ phi, TO* __restrict__ out, int nx, int ny,
                                                     int nz, const CondArgs<T>& C, const Bnd& B, double dxsqi,
                                                     double dysqi, double dzsqi, double mgparam_d, int voltfac_on,
-                                                    int mgform2init, int lcndbndy, int i) {
+                                                    int mgform2init, int lcndbndy, int i, int wtz = 0) {
   double m = 0.;
   auto store = [&](int ix, int iy, int iz, T v) {
-    if (MODE == 0) out[pix(nx, ny, ix, iy, iz)] = (TO)v;
+    if (MODE == 0) {
+      // wtz: as in residual_bulk, image planes only through their sources
+      if (wtz && (iz < 0 || iz >= nz)) return;
+      const size_t q = pix(nx, ny, ix, iy, iz);
+      out[q] = (TO)v;
+      if (wtz) {
+        const size_t nxy = (size_t)(nx + 3) * (ny + 3);
+        if (iz <= 1) out[q + (size_t)nz * nxy] = (TO)v;
+        if (iz == nz - 1) out[q - (size_t)nz * nxy] = (TO)v;
+      }
+    }
     if (MODE == 2 && ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz)
       out[rix(nx, ny, ix, iy, iz)] = (TO)v;
   };
@@ -750,11 +772,11 @@ __device__ __forceinline__ double special_res_point(const T* __restrict__ phi, T
 template <typename T, int MODE, typename TO>
 __global__ void k_special_res(const T* __restrict__ phi, TO* __restrict__ out, int nx, int ny, int nz, CondArgs<T> C,
                               Bnd B, double dxsqi, double dysqi, double dzsqi, double mgparam_d, int voltfac_on,
-                              int mgform2init, int lcndbndy, unsigned long long* maxout) {
+                              int mgform2init, int lcndbndy, unsigned long long* maxout, int wtz) {
   pdl_entry();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const double m = special_res_point<T, MODE, TO>(phi, out, nx, ny, nz, C, B, dxsqi, dysqi, dzsqi, mgparam_d,
-                                                  voltfac_on, mgform2init, lcndbndy, i);
+                                                  voltfac_on, mgform2init, lcndbndy, i, wtz);
   if (maxout) block_max_to(maxout, m);
 }
 
@@ -768,7 +790,7 @@ __global__ void __launch_bounds__(256) k_residual_sp(const T* __restrict__ phi, 
                                                      T cy, T cz, T mgparam, int nbz, CondArgs<T> C, Bnd B,
                                                      double dxsqi, double dysqi, double dzsqi, double mgparam_d,
                                                      int voltfac_on, int mgform2init, int lcndbndy,
-                                                     unsigned long long* maxout) {
+                                                     unsigned long long* maxout, int wtz) {
   pdl_entry();
   const int nspz = (int)gridDim.z - nbz;
   double md;
@@ -777,11 +799,12 @@ __global__ void __launch_bounds__(256) k_residual_sp(const T* __restrict__ phi, 
                       (int)(blockDim.x * blockDim.y) +
                   (int)(threadIdx.y * blockDim.x + threadIdx.x);
     md = special_res_point<T, MODE, TO>(phi, out, nx, ny, nz, C, B, dxsqi, dysqi, dzsqi, mgparam_d, voltfac_on,
-                                        mgform2init, lcndbndy, i);
+                                        mgform2init, lcndbndy, i, wtz);
   } else {
     T m = (T)0.;
     residual_bulk<T, MODE, TO, ZPT>(phi, rhs, out, nx, ny, nz, ixmin, ixmax, iymin, iymax, izmin, izmax, cx, cy,
-                                    cz, mgparam, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z - nspz, true, m);
+                                    cz, mgparam, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z - nspz, true, m,
+                                    wtz);
     md = (double)m;
   }
   if (maxout) block_max_to(maxout, md);
@@ -934,11 +957,14 @@ __global__ void __launch_bounds__(256) k_restrict_xy(const T* __restrict__ res, 
   }
 }
 
+// wtz: periodic z with Dirichlet x and y; the range stops at plane nz-1 and
+// planes 0, 1 and nz-1 are also written to their images nz, nz+1 and -1 (the
+// boundary copy that would follow).
 template <typename T, int ZPT, bool ZC>
 __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __restrict__ pc, int nx, int ny,
                                                 int nxc, int nyc, int ixmin, int ixmax, int iymin, int iymax,
                                                 int izmin, int izmax, const int32_t* __restrict__ ej,
-                                                const double* __restrict__ ew) {
+                                                const double* __restrict__ ew, int nz, int wtz) {
   pdl_entry();
   const int ix = ixmin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = iymin + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -982,11 +1008,19 @@ __global__ void __launch_bounds__(256) k_expand(T* __restrict__ phi, const T* __
   for (int k = 0; k < ZPT; ++k) {
     if (!ok[k]) continue;
     const T z = wz[k], z1 = one - z;
+    T v;
     if (ZC)
-      phi[f0 + k * sz] = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3] +
-                         a00 * z * q[k][4] + a10 * z * q[k][5] + a01 * z * q[k][6] + a11 * z * q[k][7];
+      v = f[k] + a00 * z1 * q[k][0] + a10 * z1 * q[k][1] + a01 * z1 * q[k][2] + a11 * z1 * q[k][3] +
+          a00 * z * q[k][4] + a10 * z * q[k][5] + a01 * z * q[k][6] + a11 * z * q[k][7];
     else  // z not coarsened: wz = 0 and z1 = 1 exactly, the z+1 terms add zeros
-      phi[f0 + k * sz] = f[k] + a00 * q[k][0] + a10 * q[k][1] + a01 * q[k][2] + a11 * q[k][3];
+      v = f[k] + a00 * q[k][0] + a10 * q[k][1] + a01 * q[k][2] + a11 * q[k][3];
+    const int p = f0 + k * sz;
+    phi[p] = v;
+    if (wtz) {
+      const int iz = iz0 + k;
+      if (iz <= 1) phi[p + nz * sz] = v;
+      if (iz == nz - 1) phi[p - nz * sz] = v;
+    }
   }
 }
 
@@ -1227,6 +1261,15 @@ struct Solver {
     return !L.has_neumann_sub && xy_dir && (zdir || (zper && L.d.nz % 2 == 0)) && L.d.nz >= 2;
   }
 
+  // Whether the boundary copy after a residual or a prolongation on level L
+  // is only the periodic-z copy (Dirichlet x and y, periodic z, nz >= 2),
+  // which those kernels then do themselves by writing planes 0, 1 and nz-1
+  // through to their images.
+  bool zper_wt(const Level& L) const {
+    const int* b = B.b;
+    return b[0] == 0 && b[1] == 0 && b[2] == 0 && b[3] == 0 && b[4] == 2 && b[5] == 2 && L.d.nz >= 2;
+  }
+
   // Whether the first red half sweep of level l can start from an
   // unzeroed phi and write all of it (k_sor_from_zero).
   bool from_zero_ok(int l) const { return o->downpasses >= 1 && merged_ok(c->lv[l]); }
@@ -1309,6 +1352,7 @@ struct Solver {
     CondArgs<T> ca = cond_args<T>(L);
     ca.nint = 0;
     int n = L.sub[0].n + L.sub[1].n;
+    const int wt = (MODE == 0 && zper_wt(L)) ? 1 : 0;
     if (sizeof(T) == 4 && l > 0 && MODE == 0 && n && !L.has_neumann_sub) {
       // FP32, below the finest level: bulk and subgrid points in one launch
       // (the FP64 form of the merged kernel needs 76 registers and is slower)
@@ -1317,8 +1361,8 @@ struct Solver {
       launch(k_residual_sp<T, MODE, TO, zpt>, dim3(grd.x, grd.y, nbz + nspz), blk, 0, phi, rhs, out, L.d.nx, L.d.ny,
              L.d.nz, R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
              (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst), (T)o->mgparam, nbz, ca, B, dxsqi, dysqi,
-             dzsqi, o->mgparam, (int)voltfac_on, (int)mgform2init, o->lcndbndy, maxout);
-      bc<TO>(L, (TO*)out, false);
+             dzsqi, o->mgparam, (int)voltfac_on, (int)mgform2init, o->lcndbndy, maxout, wt);
+      if (!wt) bc<TO>(L, (TO*)out, false);
       return;
     }
     {
@@ -1326,15 +1370,15 @@ struct Solver {
       launch(k_residual<T, MODE, TO, zpt>, grd, blk, 0, phi, rhs, out, L.d.nx, L.d.ny, L.d.nz, R.ixmin, R.ixmax, R.iymin,
                                                   R.iymax, R.izmin, R.izmax, (T)(dxsqi * o->mgparam * cst),
                                                   (T)(dysqi * o->mgparam * cst), (T)(dzsqi * o->mgparam * cst),
-                                                  (T)o->mgparam, maxout);
+                                                  (T)o->mgparam, maxout, wt);
       c->prof_end(pe);
     }
     if (n) {
       launch(k_special_res<T, MODE, TO>, cdiv(n, 128), 128, 0, phi, out, L.d.nx, L.d.ny, L.d.nz, ca, B,
                                                               dxsqi, dysqi, dzsqi, o->mgparam, (int)voltfac_on,
-                                                              (int)mgform2init, o->lcndbndy, maxout);
+                                                              (int)mgform2init, o->lcndbndy, maxout, wt);
     }
-    if (MODE == 0) bc<TO>(L, (TO*)out, false);
+    if (MODE == 0 && !wt) bc<TO>(L, (TO*)out, false);
   }
 
   // Everything vcycle(l) does below level l: the conductor marks of level
@@ -1439,7 +1483,7 @@ struct Solver {
         coarse_region<T>(l);
       c->prof_end(pc);
       expand<T>(l);
-      bc<T>(L, Arr<T>::phi(L), false);
+      if (!zper_wt(L)) bc<T>(L, Arr<T>::phi(L), false);
     }
     for (int i = 0; i < o->uppasses; ++i) sorpass<T>(l, usev);
   }
@@ -1453,6 +1497,10 @@ struct Solver {
     const LevelDims& d = L.d;
     const LevelDims& dc = Lc.d;
     Ranges R = ranges(d, B.b, false);
+    // periodic images written by the kernel (zper_wt): plane nz is the
+    // image of plane 0, not a node of its own
+    const int wt = zper_wt(L) ? 1 : 0;
+    if (wt) R.izmax = std::min(R.izmax, d.nz - 1);
     constexpr int zpt = ZPlanes<T>::value;
     dim3 blk(32, 8);
     dim3 grd2(cdiv(R.ixmax - R.ixmin + 1, 32), cdiv(R.iymax - R.iymin + 1, 8), cdiv(R.izmax - R.izmin + 1, zpt));
@@ -1460,10 +1508,12 @@ struct Solver {
       int pe = prof_begin(l, WG_PROF_EXPAND0, (double)L.nr);
       if (dc.nz == d.nz)
         launch(k_expand<T, zpt, false>, grd2, blk, 0, Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
-                                                     R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
+                                                     R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew,
+                                                     d.nz, wt);
       else
         launch(k_expand<T, zpt, true>, grd2, blk, 0, Arr<T>::phi(L), Arr<T>::phi(Lc), d.nx, d.ny, dc.nx, dc.ny,
-                                                    R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew);
+                                                    R.ixmin, R.ixmax, R.iymin, R.iymax, R.izmin, R.izmax, L.ej, L.ew,
+                                                    d.nz, wt);
       c->prof_end(pe);
     }
   }

@@ -322,17 +322,18 @@ __device__ inline void gather_e(const double* __restrict__ phi, const GridP& g, 
 // (x, y, z, unused). gather_e's trilinear sum of node differences is the
 // trilinear sum of these node fields, so the FP32 advance reads 8 vector
 // loads a particle instead of 24 FP64 ones and interpolates in FP32.
-__global__ void k_enode(const double* __restrict__ phi, GridP g, float4* __restrict__ en) {
-  const int nx1 = g.nx + 1, ny1 = g.ny + 1;
-  const int64_t n = (int64_t)nx1 * ny1 * (g.nz + 1);
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int i = (int)(t % nx1), j = (int)((t / nx1) % ny1), k = (int)(t / ((int64_t)nx1 * ny1));
+// One thread per node: 32 x 8 blocks over (x, y), one z plane per
+// blockIdx.z, so no index is divided.
+__global__ void __launch_bounds__(256) k_enode(const double* __restrict__ phi, GridP g, float4* __restrict__ en) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x), j = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int k = (int)blockIdx.z;
+  if (i > g.nx || j > g.ny) return;
   const int sy = g.nx + 3, sz = sy * (g.ny + 3);
   const double* c = phi + ((i + 1) + sy * (j + 1) + (size_t)sz * (k + 1));
   const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
-  en[t] = make_float4((float)(tdxi * (__ldg(c - 1) - __ldg(c + 1))), (float)(tdyi * (__ldg(c - sy) - __ldg(c + sy))),
-                      (float)(tdzi * (__ldg(c - sz) - __ldg(c + sz))), 0.f);
+  en[(size_t)i + (size_t)(g.nx + 1) * (j + (size_t)(g.ny + 1) * k)] =
+      make_float4((float)(tdxi * (__ldg(c - 1) - __ldg(c + 1))), (float)(tdyi * (__ldg(c - sy) - __ldg(c + sy))),
+                  (float)(tdzi * (__ldg(c - sz) - __ldg(c + sz))), 0.f);
 }
 
 // gather_e from the node fields of k_enode, in FP32 (the cell and its
@@ -1320,6 +1321,10 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = 
   // phi on every call (k_enode)
   const bool nodes = sizeof(T) == 4 && !c->correctede;
   const size_t nn = (size_t)(c->grid.nx + 1) * (c->grid.ny + 1) * (c->grid.nz + 1);
+  if (nodes && c->grid.nz + 1 > 65535) {
+    set_error("wg_advance_f32: nz must be below 65535 (one launch slice per z plane)");
+    return WG_ETOOLARGE;
+  }
   if (nodes && c->enode_n < nn) {
     if (c->enode) cudaFree(c->enode);
     c->enode = nullptr;
@@ -1345,7 +1350,9 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = 
     int pe = c->prof_begin(WG_PROF_ADVANCE, (double)p->np);
     if (nodes) {
       ++c->nlaunch;
-      k_enode<<<cdiv64((int64_t)nn, 256), 256, 0, c->stream>>>(c->lv[0].phi, gridp(c), c->enode);
+      const dim3 eg((unsigned)((c->grid.nx + 1 + 31) / 32), (unsigned)((c->grid.ny + 1 + 7) / 8),
+                    (unsigned)(c->grid.nz + 1));
+      k_enode<<<eg, dim3(32, 8), 0, c->stream>>>(c->lv[0].phi, gridp(c), c->enode);
     }
     ++c->nlaunch;
     kern<<<cdiv64(p->np, 256), 256, 0, c->stream>>>(c->lv[0].phi, nodes ? c->enode : nullptr, gridp(c), P, ce, p->x,

@@ -396,3 +396,42 @@ class WarmStart:
                  out_margin=state.get("out_margin", 6))
         ws.train_factor = tf
         return ws
+
+
+def _bench_main():
+    """python -m warp_b200.unet [--cin C --cout C --dhw D H W --reps N]:
+    times wg_conv3_fwd (forward, bias, ReLU) on random bf16 data with CUDA
+    events and prints the dense TFLOP/s (2*27*cin*cout per voxel)."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cin", type=int, default=64)
+    ap.add_argument("--cout", type=int, default=64)
+    ap.add_argument("--dhw", type=int, nargs=3, default=[128, 128, 128])
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args()
+    D, H, W = a.dhw
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((D, H, W, a.cin), generator=g, device="cuda").to(torch.bfloat16)
+    w = (torch.randn((27, a.cout, a.cin), generator=g, device="cuda") * 0.05).to(torch.bfloat16)
+    b = torch.zeros(a.cout, device="cuda")
+    y = conv3_fwd(x, w, b, relu=True)  # warm-up
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(a.reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        conv3_fwd(x, w, b, relu=True, out=y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    check_errors(x.device)
+    flop = 2.0 * 27 * a.cin * a.cout * D * H * W
+    best = min(ms)
+    print(json.dumps({"kernel": "k_conv3_tile", "cin": a.cin, "cout": a.cout, "dhw": [D, H, W],
+                      "ms": ms, "tflops_best": flop / (best * 1e-3) / 1e12,
+                      "tflops_median": flop / (sorted(ms)[len(ms) // 2] * 1e-3) / 1e12}))
+
+
+if __name__ == "__main__":
+    _bench_main()
