@@ -57,8 +57,8 @@ def test_committed_weights_on_a_heldout_beam():
       change on the unmasked nodes (farther than the margin from every
       conductor): its mean squared error is below 10 % of the zero guess's
       (the plain warm start phi^(n-1)).
-    - The guarded guess never leaves the solve a larger starting residual
-      than phi^(n-1): a rejected guess restores phi^(n-1) bit for bit.
+    - The guard keeps a guess only when it starts MIN_GAIN times lower than
+      phi^(n-1); a rejected guess restores phi^(n-1) bit for bit.
     - Every solve from the guess reaches the 1e-6 relative residual.
     - Over the steps after the first, the solves from the guess take fewer
       V-cycles in total than those from phi^(n-1) (the plain warm start,
@@ -71,6 +71,7 @@ def test_committed_weights_on_a_heldout_beam():
     torch.cuda.set_device(0)
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     ws = WarmStart.load(os.path.join(root, "warp_b200", "weights", "warmstart_D.pt"), device="cuda")
+    ws.backoff = 1  # the network on every step, whatever the guard decided before
     rng = np.random.default_rng(4242)
     gen = torch.Generator(device="cuda").manual_seed(4242)
     run, _ = wt.beam_run("D", rng, gen, "cuda")
@@ -91,7 +92,7 @@ def test_committed_weights_on_a_heldout_beam():
         s.phi.copy_(phi_prev)
         r_plain, r_guess, kept = ws.guess(s)
         if kept:
-            assert r_guess < r_plain
+            assert r_guess * ws.MIN_GAIN <= r_plain
         else:
             assert torch.equal(s.phi, phi_prev)
         s.solve()

@@ -322,18 +322,39 @@ __device__ inline void gather_e(const double* __restrict__ phi, const GridP& g, 
 // (x, y, z, unused). gather_e's trilinear sum of node differences is the
 // trilinear sum of these node fields, so the FP32 advance reads 8 vector
 // loads a particle instead of 24 FP64 ones and interpolates in FP32.
-// One thread per node: 32 x 8 blocks over (x, y), one z plane per
-// blockIdx.z, so no index is divided.
+// 32 x 8 blocks over (x, y); each thread takes ENODE_Z consecutive z planes
+// of its (x, y) column, issuing all of its loads before the first store
+// (the column's phi at k-1 .. k+ENODE_Z serves every plane's z difference).
+// No index is divided.
+constexpr int ENODE_Z = 4;
 __global__ void __launch_bounds__(256) k_enode(const double* __restrict__ phi, GridP g, float4* __restrict__ en) {
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x), j = (int)(blockIdx.y * blockDim.y + threadIdx.y);
-  const int k = (int)blockIdx.z;
+  const int k0 = (int)blockIdx.z * ENODE_Z;
   if (i > g.nx || j > g.ny) return;
   const int sy = g.nx + 3, sz = sy * (g.ny + 3);
-  const double* c = phi + ((i + 1) + sy * (j + 1) + (size_t)sz * (k + 1));
+  const double* c = phi + ((i + 1) + sy * (j + 1) + (size_t)sz * (k0 + 1));
   const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
-  en[(size_t)i + (size_t)(g.nx + 1) * (j + (size_t)(g.ny + 1) * k)] =
-      make_float4((float)(tdxi * (__ldg(c - 1) - __ldg(c + 1))), (float)(tdyi * (__ldg(c - sy) - __ldg(c + sy))),
-                  (float)(tdzi * (__ldg(c - sz) - __ldg(c + sz))), 0.f);
+  double col[ENODE_Z + 2], xm[ENODE_Z], xp[ENODE_Z], ym[ENODE_Z], yp[ENODE_Z];
+  const int nk = min(ENODE_Z, g.nz + 1 - k0);  // planes of this thread (k0 + nk - 1 <= nz)
+#pragma unroll
+  for (int q = 0; q < ENODE_Z + 2; ++q)
+    if (q <= nk + 1) col[q] = __ldg(c + (ptrdiff_t)(q - 1) * sz);  // planes k0-1 .. k0+nk, inside -1..nz+1
+#pragma unroll
+  for (int q = 0; q < ENODE_Z; ++q)
+    if (q < nk) {
+      const double* cq = c + (ptrdiff_t)q * sz;
+      xm[q] = __ldg(cq - 1);
+      xp[q] = __ldg(cq + 1);
+      ym[q] = __ldg(cq - sy);
+      yp[q] = __ldg(cq + sy);
+    }
+  const size_t o = (size_t)i + (size_t)(g.nx + 1) * (j + (size_t)(g.ny + 1) * k0);
+  const size_t so = (size_t)(g.nx + 1) * (g.ny + 1);
+#pragma unroll
+  for (int q = 0; q < ENODE_Z; ++q)
+    if (q < nk)
+      en[o + q * so] = make_float4((float)(tdxi * (xm[q] - xp[q])), (float)(tdyi * (ym[q] - yp[q])),
+                                   (float)(tdzi * (col[q] - col[q + 2])), 0.f);
 }
 
 // gather_e from the node fields of k_enode, in FP32 (the cell and its
@@ -1321,8 +1342,8 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = 
   // phi on every call (k_enode)
   const bool nodes = sizeof(T) == 4 && !c->correctede;
   const size_t nn = (size_t)(c->grid.nx + 1) * (c->grid.ny + 1) * (c->grid.nz + 1);
-  if (nodes && c->grid.nz + 1 > 65535) {
-    set_error("wg_advance_f32: nz must be below 65535 (one launch slice per z plane)");
+  if (nodes && (c->grid.nz + 1 + ENODE_Z - 1) / ENODE_Z > 65535) {
+    set_error("wg_advance_f32: nz too large for the node-field launch (65535 slices of 4 planes)");
     return WG_ETOOLARGE;
   }
   if (nodes && c->enode_n < nn) {
@@ -1351,7 +1372,7 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = 
     if (nodes) {
       ++c->nlaunch;
       const dim3 eg((unsigned)((c->grid.nx + 1 + 31) / 32), (unsigned)((c->grid.ny + 1 + 7) / 8),
-                    (unsigned)(c->grid.nz + 1));
+                    (unsigned)((c->grid.nz + 1 + ENODE_Z - 1) / ENODE_Z));
       k_enode<<<eg, dim3(32, 8), 0, c->stream>>>(c->lv[0].phi, gridp(c), c->enode);
     }
     ++c->nlaunch;
