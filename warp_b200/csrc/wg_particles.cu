@@ -25,7 +25,16 @@ constexpr double kFixInv = 1.0 / 70368744177664.0;
 struct GridP {
   int nx, ny, nz;
   double dx, dy, dz, xmmin, ymmin, zmmin, zgrid;
+  // 1/dx and 1/(2 dx) per axis, formed once on the host (IEEE divisions,
+  // the same bits as the device's)
+  double dxi, dyi, dzi, tdxi, tdyi, tdzi;
 };
+
+inline GridP make_gridp(int nx, int ny, int nz, double dx, double dy, double dz, double xmmin, double ymmin,
+                        double zmmin, double zgrid) {
+  return GridP{nx, ny, nz, dx, dy, dz, xmmin, ymmin, zmmin, zgrid,
+               1. / dx, 1. / dy, 1. / dz, 1. / (2. * dx), 1. / (2. * dy), 1. / (2. * dz)};
+}
 
 namespace {
 
@@ -78,9 +87,9 @@ template <typename T>
 __device__ inline bool dep_cell(const T* xp, const T* yp, const T* zp, const T* gaminv, int64_t i, int64_t np,
                                 const GridP& g, int& ii, int& jj, int& kk, double& u1, double& v1, double& w1) {
   if (i >= np || gaminv[i] == (T)0) return false;
-  cellfrac(((double)xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, u1);
-  cellfrac(((double)yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, v1);
-  cellfrac(((double)zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, w1);
+  cellfrac(((double)xp[i] - g.xmmin) * g.dxi, g.nx, ii, u1);
+  cellfrac(((double)yp[i] - g.ymmin) * g.dyi, g.ny, jj, v1);
+  cellfrac(((double)zp[i] - g.zgrid - g.zmmin) * g.dzi, g.nz, kk, w1);
   return true;
 }
 
@@ -283,8 +292,8 @@ __global__ void k_rhobc(double* __restrict__ rho, int nx, int ny, int nz, int ax
 // differences of phi at the 8 cell nodes, trilinearly weighted.
 __device__ inline void gather_e(const double* __restrict__ phi, const GridP& g, double x, double y, double z,
                                 double& ext, double& eyt, double& ezt) {
-  const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
-  const double dxi = 1. / g.dx, dyi = 1. / g.dy, dzi = 1. / g.dz;
+  const double tdxi = g.tdxi, tdyi = g.tdyi, tdzi = g.tdzi;
+  const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
   int i, j, k;
   double u1, v1, w1;
   cellfrac((x - g.xmmin) * dxi, g.nx, i, u1);
@@ -333,7 +342,7 @@ __global__ void __launch_bounds__(256) k_enode(const double* __restrict__ phi, G
   if (i > g.nx || j > g.ny) return;
   const int sy = g.nx + 3, sz = sy * (g.ny + 3);
   const double* c = phi + ((i + 1) + sy * (j + 1) + (size_t)sz * (k0 + 1));
-  const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
+  const double tdxi = g.tdxi, tdyi = g.tdyi, tdzi = g.tdzi;
   double col[ENODE_Z + 2], xm[ENODE_Z], xp[ENODE_Z], ym[ENODE_Z], yp[ENODE_Z];
   const int nk = min(ENODE_Z, g.nz + 1 - k0);  // planes of this thread (k0 + nk - 1 <= nz)
 #pragma unroll
@@ -363,9 +372,9 @@ __device__ inline void gather_e_nodes(const float4* __restrict__ en, const GridP
                                       float& ext, float& eyt, float& ezt) {
   int i, j, k;
   double u1d, v1d, w1d;
-  cellfrac((x - g.xmmin) * (1. / g.dx), g.nx, i, u1d);
-  cellfrac((y - g.ymmin) * (1. / g.dy), g.ny, j, v1d);
-  cellfrac((z - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, k, w1d);
+  cellfrac((x - g.xmmin) * g.dxi, g.nx, i, u1d);
+  cellfrac((y - g.ymmin) * g.dyi, g.ny, j, v1d);
+  cellfrac((z - g.zgrid - g.zmmin) * g.dzi, g.nz, k, w1d);
   const float u1 = (float)u1d, v1 = (float)v1d, w1 = (float)w1d;
   const float u0 = 1.f - u1, v0 = 1.f - v1, w0 = 1.f - w1;
   const int sy = g.nx + 1, sz = sy * (g.ny + 1);
@@ -428,7 +437,7 @@ __global__ void k_efield_sub(const double* __restrict__ phi, GridP g, const int3
     const int co = id == 0 ? 1 : id == 1 ? cy : cz;
     const int coord = id == 0 ? ix : id == 1 ? iy : iz;
     const int nmaxc = id == 0 ? g.nx : id == 1 ? g.ny : g.nz;
-    const double di = id == 0 ? 1. / g.dx : id == 1 ? 1. / g.dy : 1. / g.dz;
+    const double di = id == 0 ? g.dxi : id == 1 ? g.dyi : g.dzi;
     const double dm = dels[6 * t + 2 * id], dp = dels[6 * t + 2 * id + 1];
     double vv0, dd0, vv1, dd1;
     if (0. < dm && dm <= 1.) {
@@ -498,8 +507,8 @@ __device__ __forceinline__ void cond_edge(const double* __restrict__ pa, int ps,
 // cell with fraction 1.
 __device__ inline bool gather_e_cond(const double* __restrict__ phi, const GridP& g, const CondE& ce, double x,
                                      double y, double z, double& ext, double& eyt, double& ezt) {
-  const double tdxi = 1. / (2. * g.dx), tdyi = 1. / (2. * g.dy), tdzi = 1. / (2. * g.dz);
-  const double dxi = 1. / g.dx, dyi = 1. / g.dy, dzi = 1. / g.dz;
+  const double tdxi = g.tdxi, tdyi = g.tdyi, tdzi = g.tdzi;
+  const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
   const double xi = (x - g.xmmin) * dxi, yj = (y - g.ymmin) * dyi, zk = (z - g.zgrid - g.zmmin) * dzi;
   if (xi < 0. || xi > g.nx || yj < 0. || yj > g.ny || zk < 0. || zk > g.nz) return false;
   int i, j, k;
@@ -591,7 +600,35 @@ struct PushP {
   const double* cdb;
   int nzl;
   double zlmin, dzl;
+  // formed once on the host (set_push_constants), in the expressions and
+  // operand order of the push, so with the same bits as per particle:
+  // q (dt/2) / m; the Boris factors q dt / 2 / m (fullv) and q (dt/2) / 2 / m
+  // (halfv, synchv); 1/dzl; zmmax - zmmin and its inverse; zmmin and zmmax
+  // rounded to FP32 towards the inside of the interval
+  double cst, cbf, cbh, dzli, syslen, sysleni;
+  float zminf, zmaxf;
 };
+
+// The FP32 image of a z bound of the periodic wrap, rounded towards the
+// inside of [zmmin, zmmax] (a float rounded outward would let a wrapped
+// particle sit just past the grid, where its CIC weights leave [0, 1]).
+inline float inner_bound_f(double v, bool lower) {
+  float f = (float)v;
+  if (lower && (double)f < v) f = std::nextafter(f, INFINITY);
+  if (!lower && (double)f > v) f = std::nextafter(f, -INFINITY);
+  return f;
+}
+
+inline void set_push_constants(PushP& P) {
+  P.cst = P.q * (0.5 * P.dt) / P.m;
+  P.cbf = P.q * P.dt * 0.5 / P.m;
+  P.cbh = P.q * (0.5 * P.dt) * 0.5 / P.m;
+  P.dzli = 1. / P.dzl;
+  P.syslen = P.zmmax - P.zmmin;
+  P.sysleni = 1. / (P.zmmax - P.zmmin);
+  P.zminf = inner_bound_f(P.zmmin, true);
+  P.zmaxf = inner_bound_f(P.zmmax, false);
+}
 
 // The deposit of one advanced particle per thread (the CTA's 256 particles)
 // into the fixed-point accumulator: the same cells, weights and integer
@@ -627,9 +664,9 @@ __device__ inline void block_deposit(bool live, double x, double y, double z, co
   int ii = 0, jj = 0, kk = 0;
   double u1 = 0., v1 = 0., w1 = 0.;
   if (live) {
-    cellfrac((x - g.xmmin) * (1. / g.dx), g.nx, ii, u1);
-    cellfrac((y - g.ymmin) * (1. / g.dy), g.ny, jj, v1);
-    cellfrac((z - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, w1);
+    cellfrac((x - g.xmmin) * g.dxi, g.nx, ii, u1);
+    cellfrac((y - g.ymmin) * g.dyi, g.ny, jj, v1);
+    cellfrac((z - g.zgrid - g.zmmin) * g.dzi, g.nz, kk, w1);
   }
   int lo[3] = {live ? ii : 0x7fffffff, live ? jj : 0x7fffffff, live ? kk : 0x7fffffff};
   int hi[3] = {live ? ii : -1, live ? jj : -1, live ? kk : -1};
@@ -712,19 +749,14 @@ __device__ inline void block_deposit(bool live, double x, double y, double z, co
 // (with lcorrectede: gathered in FP64 at the FP32 positions and rounded).
 // The push constants (q dt / 2m, the lattice tables, the pipe radius) are
 // formed in FP64 and rounded once.
-// A z bound of the periodic wrap in the particle type: FP64 as given; in FP32
-// rounded towards the inside of [zmmin, zmmax] (a float rounded outward would
-// let a wrapped particle sit just past the grid, where its CIC weights leave
-// [0, 1]).
+// The z bounds of the periodic wrap in the particle type: FP64 as given; in
+// FP32 rounded towards the inside of [zmmin, zmmax] (inner_bound_f).
 template <typename T>
-__device__ __forceinline__ T inner_bound(double v, bool lower) {
+__device__ __forceinline__ T zbound(const PushP& P, bool lower) {
   if constexpr (sizeof(T) == 8) {
-    return v;
+    return lower ? P.zmmin : P.zmmax;
   } else {
-    float f = (float)v;
-    if (lower && (double)f < v) f = nextafterf(f, INFINITY);
-    if (!lower && (double)f > v) f = nextafterf(f, -INFINITY);
-    return f;
+    return lower ? P.zminf : P.zmaxf;
   }
 }
 
@@ -769,7 +801,7 @@ __device__ __forceinline__ bool advance_one(const double* __restrict__ phi, cons
     const T vz = uz * gi;
     const T a = vz * (dtr - dtl);
     const T dzi = fabs((T)1 / copysign(fabs(a) + (T)1.0e-36, a));
-    int iz = (int)fmax((T)0, (z - (T)P.zlmin) * (T)(1. / P.dzl) + (T)0.5);
+    int iz = (int)fmax((T)0, (z - (T)P.zlmin) * (T)P.dzli + (T)0.5);
     if (iz > P.nzl) iz = P.nzl;
     const T zs = (T)__ldg(P.czs + iz), ze = (T)__ldg(P.cze + iz);
     const T z1 = z + vz * dtl, z2 = z + vz * dtr;
@@ -787,13 +819,13 @@ __device__ __forceinline__ bool advance_one(const double* __restrict__ phi, cons
     }
   }
   // epush3d (half step), bpush3d (ibpush = 1), epush3d (half step)
-  const T cst = (T)(P.q * (0.5 * P.dt) / P.m);
+  const T cst = (T)P.cst;
   if (CENTER != 1) {
     ux = ux + ex * cst;
     uy = uy + ey * cst;
     uz = uz + ez * cst;
   }
-  const T cb = (T)(P.q * (CENTER == 0 ? P.dt : 0.5 * P.dt) * 0.5 / P.m);
+  const T cb = (T)(CENTER == 0 ? P.cbf : P.cbh);
   const T tx = gi * bx * cb, ty = gi * by * cb, tz = gi * bz * cb;
   const T tsqi = (T)2 / ((T)1 + tx * tx + ty * ty + tz * tz);
   const T sx = tx * tsqi, sy = ty * tsqi, sz = tz * tsqi;
@@ -817,8 +849,8 @@ __device__ __forceinline__ bool advance_one(const double* __restrict__ phi, cons
   y = y + uy * gi * dt;
   z = z + uz * gi * dt;
   // periz (top.F:4015-4035)
-  const T zmmin = inner_bound<T>(P.zmmin, true), zmmax = inner_bound<T>(P.zmmax, false);
-  const T syslen = (T)(P.zmmax - P.zmmin), sysleni = (T)(1. / (P.zmmax - P.zmmin));
+  const T zmmin = zbound<T>(P, true), zmmax = zbound<T>(P, false);
+  const T syslen = (T)P.syslen, sysleni = (T)P.sysleni;
   if (z < zmmin) z = z + syslen * (T)(int)((zmmax - z) * sysleni);
   if (z > zmmax) z = z - syslen * (T)(int)((z - zmmin) * sysleni);
   if constexpr (sizeof(T) == 4) {
@@ -883,9 +915,9 @@ __global__ void k_cell_keys(const T* __restrict__ xp, const T* __restrict__ yp, 
   }
   int ii, jj, kk;
   double f;
-  cellfrac(((double)xp[i] - g.xmmin) * (1. / g.dx), g.nx, ii, f);
-  cellfrac(((double)yp[i] - g.ymmin) * (1. / g.dy), g.ny, jj, f);
-  cellfrac(((double)zp[i] - g.zgrid - g.zmmin) * (1. / g.dz), g.nz, kk, f);
+  cellfrac(((double)xp[i] - g.xmmin) * g.dxi, g.nx, ii, f);
+  cellfrac(((double)yp[i] - g.ymmin) * g.dyi, g.ny, jj, f);
+  cellfrac(((double)zp[i] - g.zgrid - g.zmmin) * g.dzi, g.nz, kk, f);
   key[i] = (int64_t)ii + (int64_t)(g.nx + 1) * ((int64_t)jj + (int64_t)(g.ny + 1) * kk);
 }
 
@@ -1108,8 +1140,8 @@ __global__ void k_moments_final(const double* __restrict__ part, int nb, double*
 inline unsigned cdiv64(int64_t a, unsigned b) { return (unsigned)((a + b - 1) / b); }
 
 GridP gridp(const wg_ctx* c) {
-  return GridP{c->grid.nx, c->grid.ny, c->grid.nz, c->dx, c->dy, c->dz, c->grid.xmmin, c->grid.ymmin,
-               c->grid.zmmin, 0.};
+  return make_gridp(c->grid.nx, c->grid.ny, c->grid.nz, c->dx, c->dy, c->dz, c->grid.xmmin, c->grid.ymmin,
+                    c->grid.zmmin, 0.);
 }
 
 // Element type of a particle struct.
@@ -1336,6 +1368,7 @@ int advance_t(wg_ctx* c, const PS* p, const wg_push_params* prm, bool deposit = 
   if (cdiv64(p->np, 256) > 2147483647LL) { set_error("wg_advance: too many particles"); return WG_ETOOLARGE; }
   PushP P{p->q, p->m, prm->dt, c->grid.zmmin, c->grid.zmmax, prm->prwall, prm->prwallx, prm->prwally,
           prm->use_lattice ? c->czs : nullptr, c->cze, c->cdb, c->nzl, c->zlmin, c->dzl};
+  set_push_constants(P);
   CondE ce{};
   if (c->correctede) WG_TRY(prepare_correctede(c, &ce));
   // the FP32 push without lcorrectede gathers from node fields formed from
@@ -1574,7 +1607,7 @@ int deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int
   k_zero_u64<<<(unsigned)std::min<int64_t>((nr + 255) / 256, 148 * 16), 256, 0, s>>>(acc, (size_t)nr);
   k_zero_u64<<<1, 32, 0, s>>>(flag, 1);
   const double dx = (G.xmmax - G.xmmin) / G.nx, dy = (G.ymmax - G.ymmin) / G.ny, dz = (G.zmmax - G.zmmin) / G.nz;
-  GridP g{G.nx, G.ny, G.nz, dx, dy, dz, G.xmmin, G.ymmin, G.zmmin, 0.};
+  GridP g = make_gridp(G.nx, G.ny, G.nz, dx, dy, dz, G.xmmin, G.ymmin, G.zmmin, 0.);
   if (p->np > 0) k_deposit<double><<<cdiv64(p->np, DEP_NT * DEP_PPT), DEP_NT, 0, s>>>(p->x, p->y, p->z, p->gaminv, p->np, g, acc);
   double gg = p->w * p->q;
   gg = gg / dx;
