@@ -93,6 +93,14 @@ __device__ inline bool dep_cell(const T* xp, const T* yp, const T* zp, const T* 
   return true;
 }
 
+// The sum over the 32 lanes of a warp of v < 2^51, exact, as two 32-bit
+// warp reductions of its bits 0-24 and 25 up (each sums below 2^31).
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+  const unsigned lo = __reduce_add_sync(0xffffffffu, (unsigned)(v & 0x1FFFFFFull));
+  const unsigned hi = __reduce_add_sync(0xffffffffu, (unsigned)(v >> 25));
+  return ((unsigned long long)hi << 25) + lo;
+}
+
 // Adds v to node (i, j, k) of the box or of the global accumulator.
 template <int NB>
 __device__ inline void dep_add(DepBoxN<NB>& box, bool use_box, int ox, int oy, int oz, int bx, int by,
@@ -158,12 +166,7 @@ __global__ void __launch_bounds__(DEP_NT, 4) k_deposit(const T* __restrict__ xp,
     auto flush = [&]() {
       if (ci < 0) return;
 #pragma unroll
-      for (int n = 0; n < 8; ++n) {
-        unsigned long long v = s[n];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        s[n] = v;
-      }
+      for (int n = 0; n < 8; ++n) s[n] = warp_sum_u64(s[n]);
       // lane n < 8 adds node n
       unsigned long long mine = 0ull;
 #pragma unroll
@@ -701,9 +704,7 @@ __device__ inline void block_deposit(bool live, double x, double y, double z, co
       for (int n = 0; n < 8; ++n) {
         const int dx = n & 1, dy = (n >> 1) & 1, dz = n >> 2;
         const double wgt = (dx ? u1 : u0) * (dy ? v1 : v0) * (dz ? w1 : w0);
-        unsigned long long v = (unsigned long long)llrint(wgt * kFixScale);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        const unsigned long long v = warp_sum_u64((unsigned long long)llrint(wgt * kFixScale));
         if (lane == n) mine = v;
       }
       if (lane < 8 && mine)
