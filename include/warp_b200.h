@@ -194,10 +194,11 @@ int wg_deposit_end(wg_ctx* ctx, int zero_first);
  * accumulator is a fixed array inside the library, so the grid is limited to
  * (nx+1)(ny+1)(nz+1) <= 1048576 nodes (8 MiB); larger grids get WG_ETOOLARGE.
  * Call with the device that holds rho and the particles current. The first
- * call on each device looks up that array's device address. Work is queued
- * on `stream` (a cudaStream_t, NULL = legacy default stream), which is
- * synchronized before return. Calls that overlap on one device (other
- * streams or threads) share the accumulator and race: serialize them. */
+ * call on each device looks up that array's device address; make that first
+ * call before any stream capture. Work is queued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream), which is synchronized before
+ * return. Calls that overlap on one device (other streams or threads) share
+ * the accumulator and race: serialize them. */
 int wg_deposit_noalloc(const wg_grid* grid, const wg_particles* p, double* rho, int zero_first, void* stream);
 /* applyrhoboundaryconditions3d (w3d.F:2660-2750) on rho. */
 int wg_finalize_rho(wg_ctx* ctx);

@@ -1557,7 +1557,7 @@ constexpr int64_t kNoAllocMaxNodes = 1 << 20;  // (nx+1)(ny+1)(nz+1) limit: 8 Mi
 constexpr int kNoAllocMaxDevices = 64;
 
 // accumulator nodes [0, kNoAllocMaxNodes), then the overflow flag
-__device__ __align__(256) unsigned long long g_noalloc_acc[kNoAllocMaxNodes + 32];
+static __device__ __align__(256) unsigned long long g_noalloc_acc[kNoAllocMaxNodes + 32];
 
 std::mutex g_noalloc_mu;
 unsigned long long* g_noalloc_ptr[kNoAllocMaxDevices] = {};
